@@ -1,0 +1,412 @@
+"""felis_b200 — B200-native FELIS slice loop behind a C ABI.
+
+Python view of include/felis_b200.h (ctypes over the in-tree
+libfelis_b200.so).  The library is the product: every compute call here goes
+to CUDA kernels; nothing falls back to the CPU.  Importing the package fails
+loudly when the shared library has not been built.
+"""
+from __future__ import annotations
+
+import ctypes as C
+import os
+
+import numpy as np
+
+_HERE = os.path.dirname(os.path.abspath(__file__))
+LIB_PATH = os.path.join(_HERE, "_lib", "libfelis_b200.so")
+
+if not os.path.exists(LIB_PATH):
+    raise ImportError(
+        f"felis_b200: {LIB_PATH} is missing; build it with `python -m felis_b200._build` "
+        "(the CUDA extension is required, there is no CPU fallback)")
+
+_lib = C.CDLL(LIB_PATH)
+
+MAX_HARMONY = 8
+MAX_SPECIES = 8
+ABI_VERSION = 1
+
+OK, BAD_ARG, CUDA_ERROR, THETA_OVERFLOW, OUT_OF_RANGE, NAN, TIMEOUT, UNSUPPORTED, NO_DEVICE, IO, NOT_FOUND = range(11)
+STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA_ERROR", 3: "THETA_OVERFLOW", 4: "OUT_OF_RANGE", 5: "NAN",
+                6: "TIMEOUT", 7: "UNSUPPORTED", 8: "NO_DEVICE", 9: "IO", 10: "NOT_FOUND"}
+STATIC, TIME_DEPENDENT = 1, 2
+BIPOLAR, QUADPOLAR = 1, 2
+FP64, MIXED = 0, 1
+
+_dp = C.POINTER(C.c_double)
+_i64p = C.POINTER(C.c_int64)
+_i32p = C.POINTER(C.c_int32)
+
+
+class Undulator(C.Structure):
+    _fields_ = [("type", C.c_int32), ("K0_alpha", C.c_int32), ("numbers", C.c_int32), ("air", C.c_int32),
+                ("lambdaU", C.c_double), ("slopeK", C.c_double), ("ue", C.c_double),
+                ("unit_start", _dp), ("unit_end", _dp), ("und_start", _dp), ("und_end", _dp), ("K0", _dp)]
+
+
+class Quad(C.Structure):
+    _fields_ = [("numbers", C.c_int32), ("pad_", C.c_int32), ("unit_start", _dp), ("unit_end", _dp),
+                ("qd_start", _dp), ("qd_end", _dp), ("g", _dp)]
+
+
+class Params(C.Structure):
+    _fields_ = [
+        ("abi_version", C.c_int32), ("precision", C.c_int32), ("dimension", C.c_int32), ("mode", C.c_int32),
+        ("num_harmony", C.c_int32), ("harmony", C.c_int32 * MAX_HARMONY),
+        ("slice_n", C.c_int32), ("min_i", C.c_int32), ("global_slice_n", C.c_int32),
+        ("nx", C.c_int32), ("ny", C.c_int32), ("num_slice", C.c_int32), ("num_lambda_u", C.c_int32),
+        ("num_species", C.c_int32), ("scl_mode", C.c_int32), ("scf_mode", C.c_int32), ("nr", C.c_int32),
+        ("bessel_rows", C.c_int32), ("bessel_cols", C.c_int32), ("abc_n", C.c_int32), ("wake_on", C.c_int32),
+        ("max_step", C.c_int32), ("num_undulators", C.c_int32), ("num_quads", C.c_int32),
+        ("ks", C.c_double), ("lambda0", C.c_double), ("dz", C.c_double), ("dx", C.c_double), ("dy", C.c_double),
+        ("dr", C.c_double), ("min_x", C.c_double), ("max_x", C.c_double), ("min_y", C.c_double),
+        ("max_y", C.c_double), ("min_z", C.c_double), ("max_z", C.c_double),
+        ("gamma0", C.c_double), ("gam_r", C.c_double), ("d_bessel", C.c_double), ("abc_sig", C.c_double),
+        ("spot_sig_r", C.c_double),
+        ("K0_init", C.c_double), ("ue_init", C.c_double), ("lambdaU_init", C.c_double),
+        ("K0_alpha_init", C.c_int32), ("und_type_init", C.c_int32),
+        ("abc_alpha", _dp), ("abc_alpha_p", _dp), ("abc_beta", _dp), ("abc_beta_p", _dp),
+        ("bessel", _dp), ("wake_e", _dp),
+        ("undulators", C.POINTER(Undulator)), ("quads", C.POINTER(Quad)),
+    ]
+
+
+class Lattice(C.Structure):
+    _fields_ = [("K0", C.c_double), ("ue", C.c_double), ("lambdaU", C.c_double), ("ku", C.c_double),
+                ("g", C.c_double), ("K0_alpha", C.c_int32), ("und_type", C.c_int32),
+                ("current_flag", C.c_int32), ("drift_flag", C.c_int32)]
+
+
+def _sig(name, res, *args):
+    f = getattr(_lib, name)
+    f.restype = res
+    f.argtypes = list(args)
+    return f
+
+
+_vp = C.c_void_p
+_sig("felis_create", C.c_int, C.POINTER(Params), C.POINTER(_vp))
+_sig("felis_destroy", None, _vp)
+_sig("felis_last_error", C.c_char_p, _vp)
+_sig("felis_device_info", C.c_int, C.c_char_p, C.c_size_t, _i32p)
+_sig("felis_upload_particles", C.c_int, _vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _dp)
+_sig("felis_download_particles", C.c_int, _vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp)
+_sig("felis_upload_field", C.c_int, _vp, C.c_int32, C.c_int32, _dp)
+_sig("felis_download_field", C.c_int, _vp, C.c_int32, C.c_int32, _dp)
+_sig("felis_download_source", C.c_int, _vp, C.c_int32, C.c_int32, _dp)
+_sig("felis_download_ez", C.c_int, _vp, _dp)
+_sig("felis_update_lattice", C.c_int, _vp, C.c_int32, C.c_double)
+_sig("felis_get_lattice", C.c_int, _vp, C.POINTER(Lattice))
+_sig("felis_set_lattice", C.c_int, _vp, C.POINTER(Lattice))
+for _n in ("felis_update_total_energy", "felis_twiss", "felis_bfactor"):
+    _sig(_n, C.c_int, _vp, C.c_int32, _dp)
+for _n in ("felis_solve_field", "felis_transverse_push", "felis_push_theta_gamma", "felis_drift_theta_gamma",
+           "felis_periodic_particles", "felis_shift_field", "felis_step"):
+    _sig(_n, C.c_int, _vp, C.c_int32)
+_sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, _dp, _dp, _dp)
+_sig("felis_edge_deposit_count", C.c_int, _vp, _i64p)
+_sig("felis_sort_by_slice", C.c_int, _i32p, C.c_int64, _i64p)
+_sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
+_sig("felis_config_free", None, _vp)
+_sig("felis_config_params", C.POINTER(Params), _vp)
+_sig("felis_config_error", C.c_char_p)
+_sig("felis_config_load_beam", C.c_int, _vp, C.c_int32, C.c_uint64, _i64p, _dp, _dp, _dp, _dp, _dp, _dp, _dp)
+_sig("felis_config_load_seed", C.c_int, _vp, C.c_int32, _dp, _dp)
+_sig("felis_config_wake", C.c_int, _vp, _dp, _dp)
+_sig("felis_detmath_sincos", None, C.c_double, _dp, _dp)
+_sig("felis_detmath_atan", C.c_double, C.c_double)
+_sig("felis_detmath_atan2", C.c_double, C.c_double, C.c_double)
+
+
+class FelisError(RuntimeError):
+    def __init__(self, status: int, msg: str):
+        super().__init__(f"{STATUS_NAMES.get(status, status)}: {msg}")
+        self.status = status
+
+
+def _p(a: np.ndarray):
+    return a.ctypes.data_as(_dp) if a is not None else None
+
+
+def _f64(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float64)
+
+
+class Config:
+    """A parsed FELIS input file (felis_config_load) and its setup tables."""
+
+    def __init__(self, path: str, num_ranks: int = 1, rank: int = 0):
+        h = _vp()
+        st = _lib.felis_config_load(os.fsencode(path), num_ranks, rank, C.byref(h))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        self._h = h
+        self.params = _lib.felis_config_params(h).contents
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.felis_config_free(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    @property
+    def N(self) -> int:
+        return self.params.nx * self.params.ny
+
+    def harmonics(self) -> list[int]:
+        return [self.params.harmony[i] for i in range(self.params.num_harmony)]
+
+    def bessel(self) -> np.ndarray:
+        p = self.params
+        return np.ctypeslib.as_array(p.bessel, shape=(p.bessel_rows * p.bessel_cols,)).reshape(p.bessel_rows, p.bessel_cols).copy()
+
+    def abc(self) -> tuple[np.ndarray, ...]:
+        p = self.params
+        out = []
+        for name, n in (("abc_alpha", p.nx), ("abc_alpha_p", p.nx), ("abc_beta", p.ny), ("abc_beta_p", p.ny)):
+            a = np.ctypeslib.as_array(getattr(p, name), shape=(2 * n,)).copy()
+            out.append(a[0::2] + 1j * a[1::2])
+        return tuple(out)
+
+    def load_beam(self, species: int = 0, seed: int = 0) -> dict:
+        """Initial particles of one species (loadBeam.cpp:28-269)."""
+        S = self.params.slice_n
+        counts = np.zeros(S, dtype=np.int64)
+        st = _lib.felis_config_load_beam(self._h, species, seed, counts.ctypes.data_as(_i64p), *([None] * 7))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        n = int(counts.sum())
+        arrs = {k: np.zeros(n) for k in ("x", "y", "px", "py", "theta", "gamma")}
+        w = np.zeros(S)
+        st = _lib.felis_config_load_beam(self._h, species, seed, counts.ctypes.data_as(_i64p),
+                                         *(_p(arrs[k]) for k in ("x", "y", "px", "py", "theta", "gamma")), _p(w))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        off = np.zeros(S + 1, dtype=np.int64)
+        off[1:] = np.cumsum(counts)
+        arrs["offsets"] = off
+        arrs["weights"] = w
+        return arrs
+
+    def load_seed(self, hidx: int) -> tuple[np.ndarray, np.ndarray]:
+        """Seed field of harmonic index hidx, reference layout (S+2, ny, nx) complex."""
+        p = self.params
+        n = (p.slice_n + 2) * p.nx * p.ny
+        ux = np.zeros(2 * n)
+        uy = np.zeros(2 * n)
+        st = _lib.felis_config_load_seed(self._h, hidx, _p(ux), _p(uy))
+        if st != OK:
+            raise FelisError(st, "load_seed")
+        shp = (p.slice_n + 2, p.ny, p.nx)
+        return (ux[0::2] + 1j * ux[1::2]).reshape(shp), (uy[0::2] + 1j * uy[1::2]).reshape(shp)
+
+    def wake(self, den: np.ndarray) -> np.ndarray:
+        """Wake energy loss per global slice from the slice charge (wakeField.cpp:9-50)."""
+        den = _f64(den)
+        out = np.zeros(self.params.global_slice_n)
+        st = _lib.felis_config_wake(self._h, _p(den), _p(out))
+        if st != OK:
+            raise FelisError(st, "wake")
+        return out
+
+
+def _cplx_to_interleaved(a: np.ndarray) -> np.ndarray:
+    a = np.ascontiguousarray(a, dtype=np.complex128).ravel()
+    return a.view(np.float64)
+
+
+class Handle:
+    """One felis_handle: the device-resident slice loop of one GPU."""
+
+    def __init__(self, params: Params):
+        h = _vp()
+        st = _lib.felis_create(C.byref(params), C.byref(h))
+        if st != OK:
+            raise FelisError(st, "felis_create failed (see stderr)")
+        self._h = h
+        self.S = params.slice_n
+        self.nx, self.ny = params.nx, params.ny
+        self.H = params.num_harmony
+        self.species = params.num_species
+        self.L, self.F, self.nr = params.scl_mode, params.scf_mode, params.nr
+        self.mode = params.mode
+        self._counts = [0] * self.species
+
+    def close(self):
+        if getattr(self, "_h", None):
+            _lib.felis_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, st: int):
+        if st != OK:
+            raise FelisError(st, _lib.felis_last_error(self._h).decode())
+
+    # ---- data in / out ----
+    def upload_particles(self, species: int, x, y, px, py, theta, gamma, offsets, weights):
+        arrs = [_f64(a) for a in (x, y, px, py, theta, gamma)]
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        w = _f64(weights)
+        self._ck(_lib.felis_upload_particles(self._h, species, *(_p(a) for a in arrs), off.ctypes.data_as(_i64p), _p(w)))
+        self._counts[species] = int(off[-1])
+
+    def download_particles(self, species: int = 0) -> dict:
+        n = self._counts[species]
+        out = {k: np.zeros(n) for k in ("x", "y", "px", "py", "theta", "gamma")}
+        self._ck(_lib.felis_download_particles(self._h, species, *(_p(out[k]) for k in ("x", "y", "px", "py", "theta", "gamma"))))
+        return out
+
+    def upload_field(self, hidx: int, pol: int, data: np.ndarray):
+        buf = _cplx_to_interleaved(data)
+        self._ck(_lib.felis_upload_field(self._h, hidx, pol, _p(buf)))
+
+    def _dl(self, fn, hidx, pol) -> np.ndarray:
+        n = (self.S + 2) * self.nx * self.ny
+        buf = np.zeros(2 * n)
+        self._ck(fn(self._h, hidx, pol, _p(buf)))
+        return (buf[0::2] + 1j * buf[1::2]).reshape(self.S + 2, self.ny, self.nx)
+
+    def download_field(self, hidx: int, pol: int) -> np.ndarray:
+        return self._dl(_lib.felis_download_field, hidx, pol)
+
+    def download_source(self, hidx: int, pol: int) -> np.ndarray:
+        return self._dl(_lib.felis_download_source, hidx, pol)
+
+    def download_ez(self) -> np.ndarray:
+        n = self.L * (self.S + 2) * self.F * self.nr
+        buf = np.zeros(2 * n)
+        self._ck(_lib.felis_download_ez(self._h, _p(buf)))
+        return (buf[0::2] + 1j * buf[1::2]).reshape(self.L, self.S + 2, self.F, self.nr)
+
+    # ---- lattice ----
+    def update_lattice(self, it: int, half: float):
+        self._ck(_lib.felis_update_lattice(self._h, it, half))
+
+    def lattice(self) -> Lattice:
+        l = Lattice()
+        self._ck(_lib.felis_get_lattice(self._h, C.byref(l)))
+        return l
+
+    def set_lattice(self, l: Lattice):
+        self._ck(_lib.felis_set_lattice(self._h, C.byref(l)))
+
+    # ---- per-step functions (main.cpp:117-149) ----
+    def total_energy(self, it: int = 0) -> np.ndarray:
+        out = np.zeros(2 * self.H)
+        self._ck(_lib.felis_update_total_energy(self._h, it, _p(out)))
+        return out
+
+    def twiss(self, it: int = 0) -> np.ndarray:
+        out = np.zeros(6 * self.species)
+        self._ck(_lib.felis_twiss(self._h, it, _p(out)))
+        return out
+
+    def bfactor(self, it: int = 0) -> np.ndarray:
+        out = np.zeros(2 * self.H)
+        self._ck(_lib.felis_bfactor(self._h, it, _p(out)))
+        return out
+
+    def solve_field(self, it: int = 0):
+        self._ck(_lib.felis_solve_field(self._h, it))
+
+    def transverse_push(self, it: int = 0):
+        self._ck(_lib.felis_transverse_push(self._h, it))
+
+    def push_theta_gamma(self, it: int = 0):
+        self._ck(_lib.felis_push_theta_gamma(self._h, it))
+
+    def drift_theta_gamma(self, it: int = 0):
+        self._ck(_lib.felis_drift_theta_gamma(self._h, it))
+
+    def periodic_particles(self, it: int = 0):
+        self._ck(_lib.felis_periodic_particles(self._h, it))
+
+    def shift_field(self, it: int = 0):
+        self._ck(_lib.felis_shift_field(self._h, it))
+
+    def step(self, it: int):
+        self._ck(_lib.felis_step(self._h, it))
+
+    def run(self, it0: int, it1: int):
+        self._ck(_lib.felis_run(self._h, it0, it1))
+
+    def diagnostics(self, it0: int, it1: int):
+        n = it1 - it0
+        e = np.zeros(n * 2 * self.H)
+        t = np.zeros(n * 6 * self.species)
+        b = np.zeros(n * 2 * self.H)
+        self._ck(_lib.felis_get_diagnostics(self._h, it0, it1, _p(e), _p(t), _p(b)))
+        return e.reshape(n, 2 * self.H), t.reshape(n, 6 * self.species), b.reshape(n, 2 * self.H)
+
+    def edge_deposit_count(self) -> int:
+        c = C.c_int64(0)
+        self._ck(_lib.felis_edge_deposit_count(self._h, C.byref(c)))
+        return c.value
+
+    def run_loop(self, it0: int, it1: int):
+        """The drop-in sequence of main.cpp:117-155 through the per-function calls."""
+        for it in range(it0, it1):
+            self.total_energy(it)
+            self.twiss(it)
+            self.bfactor(it)
+            self.solve_field(it)
+            self.update_lattice(it, 0.0)
+            self.transverse_push(it)
+            self.update_lattice(it, 0.5)
+            self.transverse_push(it)
+            lat = self.lattice()
+            if not lat.drift_flag:
+                self.push_theta_gamma(it)
+            else:
+                self.drift_theta_gamma(it)
+            self.periodic_particles(it)
+            if not lat.drift_flag and self.mode == TIME_DEPENDENT:
+                self.shift_field(it)
+
+
+def device_info() -> tuple[str, int]:
+    name = C.create_string_buffer(256)
+    sm = C.c_int32(0)
+    st = _lib.felis_device_info(name, 256, C.byref(sm))
+    if st != OK:
+        raise FelisError(st, "no CUDA device")
+    return name.value.decode(), sm.value
+
+
+def sort_by_slice(keys: np.ndarray) -> np.ndarray:
+    """Stable GPU sort of slice keys; returns the permutation (felis_sort_by_slice)."""
+    k = np.ascontiguousarray(keys, dtype=np.int32)
+    perm = np.zeros(len(k), dtype=np.int64)
+    st = _lib.felis_sort_by_slice(k.ctypes.data_as(_i32p), len(k), perm.ctypes.data_as(_i64p))
+    if st != OK:
+        raise FelisError(st, "felis_sort_by_slice")
+    return perm
+
+
+def detmath_sincos(x: float) -> tuple[float, float]:
+    s, c = C.c_double(), C.c_double()
+    _lib.felis_detmath_sincos(x, C.byref(s), C.byref(c))
+    return s.value, c.value
+
+
+def detmath_atan(x: float) -> float:
+    return _lib.felis_detmath_atan(x)
+
+
+def detmath_atan2(y: float, x: float) -> float:
+    return _lib.felis_detmath_atan2(y, x)
+
+
+def library_symbols() -> list[str]:
+    """Names of every entry point declared in include/felis_b200.h."""
+    import re
+
+    hdr = os.path.join(os.path.dirname(_HERE), "include", "felis_b200.h")
+    with open(hdr) as f:
+        text = f.read()
+    return sorted(set(re.findall(r"\b(felis_[a-z0-9_]+)\s*\(", text)))

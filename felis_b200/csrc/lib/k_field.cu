@@ -1,0 +1,455 @@
+// Field kernels of the FELIS slice loop, FP64 plain path (--fmad=false).
+//
+//  * Ordered source deposit (solveField.cpp:233-312).  The reference adds
+//    each particle's bilinear current into ScUx/ScUy one particle after the
+//    other, so every cell is a sequential sum in particle order.  Here one
+//    CTA owns one slice: it sorts the slice's (cell, particle) keys in shared
+//    memory (bitonic, 32-bit composite keys), then one thread per target cell
+//    merges the four source buckets (cells t, t-1, t-nx, t-nx-1) by particle
+//    index and accumulates in exactly that order.  No float atomics; the
+//    result equals the sequential CPU sum bit for bit.
+//  * Ez space charge (solveField.cpp:315-399) the same way over radial bins,
+//    followed by the per-slice Thomas solve in r.
+//  * ADI (solveField.cpp:80-185).  One CTA owns one (slice, harmonic,
+//    polarisation) plane.  The x sweep runs one thread per row with the
+//    forward elimination stored in a shared-memory plane, the back
+//    substitution overwrites it with Uc; the y sweep runs one thread per
+//    column on that plane and writes U back to HBM coalesced.  The
+//    data-independent recurrence coefficients (CC) are host tables.
+#include "field.cuh"
+
+namespace felis {
+
+namespace {
+
+__device__ __forceinline__ double block_sum(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t += red[k];
+  return t;
+}
+
+__device__ __forceinline__ void bitonic_sort(uint32_t* s, int n2) {
+  for (int k = 2; k <= n2; k <<= 1) {
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < n2; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const uint32_t a = s[i], b = s[ixj];
+          const bool up = ((i & k) == 0);
+          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  }
+}
+
+// First index in s[0, n) with s[idx] >= v (s sorted ascending).
+__device__ __forceinline__ int lower_bound_u32(const uint32_t* s, int n, uint32_t v) {
+  int lo = 0, hi = n;
+  while (lo < hi) {
+    const int mid = (lo + hi) >> 1;
+    if (s[mid] < v) lo = mid + 1;
+    else hi = mid;
+  }
+  return lo;
+}
+
+// Maps a slice-local deposit index q (species-major) to the global particle index.
+__device__ __forceinline__ int64_t q_to_n(const DepositLaunch& a, int s, uint32_t q) {
+  const int S = a.G.S;
+  for (int sp = 0; sp < a.G.nspecies; ++sp) {
+    const int64_t b = a.soff[(size_t)sp * (S + 1) + s], e = a.soff[(size_t)sp * (S + 1) + s + 1];
+    if ((int64_t)q < e - b) return b + q;
+    q -= (uint32_t)(e - b);
+  }
+  return -1;
+}
+
+__global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
+  extern __shared__ __align__(16) unsigned char dsm[];
+  uint32_t* keys = reinterpret_cast<uint32_t*>(dsm);
+  __shared__ int red_i[4][16];
+  const DevGeom& G = a.G;
+  const int s = blockIdx.x;
+  const int S = G.S, nx = G.nx, ny = G.ny, N = G.N;
+  const uint32_t qmask = (1u << a.qbits) - 1u;
+  // ---- slice particle count (all species) and capacity check ----
+  int64_t Pt = 0, Plast0 = 0, Plast = 0;
+  for (int sp = 0; sp < G.nspecies; ++sp) {
+    const int64_t b = a.soff[(size_t)sp * (S + 1) + s], e = a.soff[(size_t)sp * (S + 1) + s + 1];
+    if (sp == G.nspecies - 1) { Plast0 = Pt; Plast = e - b; }
+    Pt += e - b;
+  }
+  if (Pt > a.cap) {
+    if (threadIdx.x == 0) {
+      set_flag(a.err, ERR_DEPOSIT_CAPACITY);
+      a.box[s] = make_int4(1, 0, 1, 0);
+    }
+    return;
+  }
+  int n2 = 1;
+  while (n2 < Pt) n2 <<= 1;
+  // ---- phase A: 2-D source ----
+  int cmin_i = 1 << 30, cmax_i = -1, cmin_j = 1 << 30, cmax_j = -1;
+  for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+    uint32_t v = 0xFFFFFFFFu;
+    if (q < Pt) {
+      const int64_t n = q_to_n(a, s, (uint32_t)q);
+      const int k = a.dep.key[n];
+      if (k >= 0) {
+        v = ((uint32_t)k << a.qbits) | (uint32_t)q;
+        const int ki = k % nx, kj = k / nx;
+        cmin_i = min(cmin_i, ki); cmax_i = max(cmax_i, ki);
+        cmin_j = min(cmin_j, kj); cmax_j = max(cmax_j, kj);
+      }
+    }
+    keys[q] = v;
+  }
+  // block min/max of the occupied cells
+  for (int o = 16; o > 0; o >>= 1) {
+    cmin_i = min(cmin_i, __shfl_down_sync(0xffffffffu, cmin_i, o));
+    cmax_i = max(cmax_i, __shfl_down_sync(0xffffffffu, cmax_i, o));
+    cmin_j = min(cmin_j, __shfl_down_sync(0xffffffffu, cmin_j, o));
+    cmax_j = max(cmax_j, __shfl_down_sync(0xffffffffu, cmax_j, o));
+  }
+  if ((threadIdx.x & 31) == 0) {
+    const int w = threadIdx.x >> 5;
+    red_i[0][w] = cmin_i; red_i[1][w] = cmax_i; red_i[2][w] = cmin_j; red_i[3][w] = cmax_j;
+  }
+  __syncthreads();
+  bitonic_sort(keys, n2);
+  int i0 = 1 << 30, i1 = -1, j0 = 1 << 30, j1 = -1;
+  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+    i0 = min(i0, red_i[0][w]); i1 = max(i1, red_i[1][w]);
+    j0 = min(j0, red_i[2][w]); j1 = max(j1, red_i[3][w]);
+  }
+  // valid entries precede the 0xFFFFFFFF padding
+  const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
+  // targets: interior cells a key can reach
+  const int ti0 = max(1, i0), ti1 = min(nx - 2, i1 + 1);
+  const int tj0 = max(1, j0), tj1 = min(ny - 2, j1 + 1);
+  if (threadIdx.x == 0) a.box[s] = (V > 0 && ti0 <= ti1 && tj0 <= tj1) ? make_int4(ti0, ti1, tj0, tj1) : make_int4(1, 0, 1, 0);
+  if (V > 0 && ti0 <= ti1 && tj0 <= tj1) {
+    const int bw = ti1 - ti0 + 1, bh = tj1 - tj0 + 1;
+    const size_t tot = (size_t)a.total;
+    for (int c = threadIdx.x; c < bw * bh; c += blockDim.x) {
+      const int ti = ti0 + c % bw, tj = tj0 + c / bw;
+      const int t = tj * nx + ti;
+      // source buckets: corner (ii, jj) of key t - jj*nx - ii
+      int lo[4], hi[4];
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const int ii = cb & 1, jj = cb >> 1;
+        const int k = t - jj * nx - ii;
+        lo[cb] = lower_bound_u32(keys, V, (uint32_t)k << a.qbits);
+        hi[cb] = lower_bound_u32(keys, V, (uint32_t)(k + 1) << a.qbits);
+      }
+      cd accx[FELIS_MAX_HARMONY], accy[FELIS_MAX_HARMONY];
+      for (int h = 0; h < G.H; ++h) { accx[h] = C(0, 0); accy[h] = C(0, 0); }
+      while (true) {
+        int best = -1;
+        uint32_t bq = 0xFFFFFFFFu;
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb)
+          if (lo[cb] < hi[cb]) {
+            const uint32_t q = keys[lo[cb]] & qmask;
+            if (q < bq) { bq = q; best = cb; }
+          }
+        if (best < 0) break;
+        ++lo[best];
+        const int ii = best & 1, jj = best >> 1;
+        const int64_t n = q_to_n(a, s, bq);
+        const double wx1 = a.dep.wx1[n], wy1 = a.dep.wy1[n];
+        const double wxv = ii ? wx1 : 1.0 - wx1;
+        const double wyv = jj ? wy1 : 1.0 - wy1;
+        const cd ex = cscale(cscale(a.etaX, wxv), wyv);
+        const cd ey = cscale(cscale(a.etaY, wxv), wyv);
+        for (int h = 0; h < G.H; ++h) {
+          const double2 mc2 = a.dep.coef[(size_t)h * tot + n];
+          const cd mc = C(mc2.x, mc2.y);
+          cd fx, fy;
+          if (G.harmony[h] % 2 == 1) {
+            fx = C(a.fconst[h][0].x, a.fconst[h][0].y);
+            fy = C(a.fconst[h][1].x, a.fconst[h][1].y);
+          } else {
+            const double2 v1 = a.dep.fx[(size_t)h * tot + n], v2 = a.dep.fy[(size_t)h * tot + n];
+            fx = C(v1.x, v1.y);
+            fy = C(v2.x, v2.y);
+          }
+          accx[h] = csub(accx[h], cmul(cmul(ex, fx), mc));
+          accy[h] = csub(accy[h], cmul(cmul(ey, fy), mc));
+        }
+      }
+      for (int h = 0; h < G.H; ++h) {
+        a.Sc[(((size_t)h * 2 + 0) * S + s) * N + t] = make_double2(accx[h].re, accx[h].im);
+        a.Sc[(((size_t)h * 2 + 1) * S + s) * N + t] = make_double2(accy[h].re, accy[h].im);
+      }
+    }
+  }
+  __syncthreads();
+  // ---- phase B: Ez of the last species (solveField.cpp:315-399) ----
+  const int nr = G.nr, L = G.L, F = G.F;
+  int m2 = 1;
+  while (m2 < Plast) m2 <<= 1;
+  for (int q = threadIdx.x; q < m2; q += blockDim.x) {
+    uint32_t v = 0xFFFFFFFFu;
+    if (q < Plast) {
+      const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + q));
+      const int rk = a.dep.rkey[n];
+      if (rk >= 0) v = ((uint32_t)rk << a.qbits) | (uint32_t)q;
+    }
+    keys[q] = v;
+  }
+  __syncthreads();
+  bitonic_sort(keys, m2);
+  const int VR = lower_bound_u32(keys, m2, 0xFFFFFFFFu);
+  const size_t tot = (size_t)a.total;
+  // d[j] = accumulated radial source of bin j (j < nr-1; bin nr-1 is not
+  // used).  dbin and the modified diagonal live after the key area.
+  double2* dbin = reinterpret_cast<double2*>(dsm + (((size_t)a.cap * sizeof(uint32_t) + 15) & ~(size_t)15));
+  double* bmod = reinterpret_cast<double*>(dbin + (size_t)L * F * nr);
+  for (int idx = threadIdx.x; idx < L * F * nr; idx += blockDim.x) {
+    const int lf = idx / nr, b = idx % nr;
+    const int f = lf % F;
+    cd acc = C(0, 0);
+    if (b < nr - 1 && !(f > 0 && b == 0)) {
+      int lo0, hi0, lo1 = 0, hi1 = 0;
+      lo0 = lower_bound_u32(keys, VR, (uint32_t)b << a.qbits);
+      hi0 = lower_bound_u32(keys, VR, (uint32_t)(b + 1) << a.qbits);
+      if (b >= 2) {
+        lo1 = lower_bound_u32(keys, VR, (uint32_t)(b - 1) << a.qbits);
+        hi1 = lo0;
+      }
+      while (lo0 < hi0 || lo1 < hi1) {
+        const uint32_t q0 = lo0 < hi0 ? (keys[lo0] & qmask) : 0xFFFFFFFFu;
+        const uint32_t q1 = lo1 < hi1 ? (keys[lo1] & qmask) : 0xFFFFFFFFu;
+        const bool take0 = q0 < q1;
+        const uint32_t q = take0 ? q0 : q1;
+        if (take0) ++lo0; else ++lo1;
+        const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + q));
+        const double2 v = a.dep.ez[(size_t)lf * tot + n];
+        const cd cc = C(v.x, v.y);
+        if (b == 0) {
+          acc = cadd(acc, cc);  // idxR == 0 branch: no radial weight
+        } else {
+          const double wr1 = a.dep.wr1[n];
+          const double wr = take0 ? 1.0 - wr1 : wr1;
+          acc = cadd(acc, cscale(cc, wr));
+        }
+      }
+    }
+    dbin[idx] = make_double2(acc.re, acc.im);
+  }
+  __syncthreads();
+  // Thomas solve in r, one thread per (l, f)
+  if ((int)threadIdx.x < L * F) {
+    const int lf = threadIdx.x, l = lf / F, f = lf % F;
+    const double A = a.A;
+    double2* d = dbin + lf * nr;
+    auto acoef = [&](int j) -> double { return (j == 0) ? (f == 0 ? 1.0 : 0.0) : (j == nr - 1 ? 0.0 : j + 0.5); };
+    auto ccoef = [&](int j) -> double { return (j == 0 || j == nr - 1) ? 0.0 : j - 0.5; };
+    double* bm = bmod + (size_t)lf * nr;
+    double bprev;
+    if (f == 0) bprev = -(1.0 + (l + 1.0) * (l + 1.0) * A / 8.0);
+    else { bprev = 1.0; d[0] = make_double2(0.0, 0.0); }
+    bm[0] = bprev;
+    for (int j = 1; j < nr; ++j) {
+      double bj = (j == nr - 1) ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * A * j - f * f * G.logtab[j];
+      const double ww = ccoef(j) / bprev;
+      bj -= ww * acoef(j - 1);
+      cd dj = (j == nr - 1) ? C(0, 0) : C(d[j].x, d[j].y);
+      const cd dp = C(d[j - 1].x, d[j - 1].y);
+      dj = csub(dj, cscale(dp, ww));
+      d[j] = make_double2(dj.re, dj.im);
+      bm[j] = bj;
+      bprev = bj;
+    }
+    const size_t ezs = (size_t)(S + 2) * nr * F;
+    const int sliceI = s + 1;
+    for (int j = nr - 2; j >= 0; --j) {
+      const cd dj = C(d[j].x, d[j].y);
+      const cd r = cdivr(csub(dj, cscale(C(0.0, 0.0), acoef(j))), bm[j]);
+      a.Ez[(size_t)l * ezs + (size_t)sliceI * F * nr + (size_t)f * nr + j] = make_double2(r.re, r.im);
+    }
+  }
+}
+
+// ---- ADI -------------------------------------------------------------------
+__global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
+  extern __shared__ double2 Apl[];  // ny rows of nxp complex
+  __shared__ double red[8];
+  const DevGeom& G = a.G;
+  const int S = G.S, nx = G.nx, ny = G.ny, N = G.N, nxp = a.nxp;
+  const int s = blockIdx.x % S;
+  const int hp = blockIdx.x / S;  // h*2 + pol
+  const int h = hp >> 1, pol = hp & 1;
+  const AdiTab T = a.tab[h];
+  double2* U = a.U + field_plane(S, h, pol, s, a.ring_base) * N;
+  const double2* Sc = a.Sc + ((size_t)hp * S + s) * N;
+  const int4 bx = a.box[s];
+  const bool src = a.use_source != 0;
+  const int tid = threadIdx.x;
+  // ---- x sweep: thread per row j ----
+  {
+    const int j = tid;
+    if (j >= 1 && j <= ny - 2) {
+      const cd rm = T.rx_m[j], r0 = T.rx_0[j], rp = T.rx_p[j];
+      const bool rowin = src && j >= bx.z && j <= bx.w;
+      cd DD = C(0, 0);
+      for (int i = 1; i <= nx - 2; ++i) {
+        const double2 up = U[(j + 1) * nx + i], u0 = U[j * nx + i], um = U[(j - 1) * nx + i];
+        cd t = cmul(rm, C(up.x, up.y));
+        t = cadd(t, cmul(r0, C(u0.x, u0.y)));
+        t = csub(t, cmul(rp, C(um.x, um.y)));
+        if (rowin && i >= bx.x && i <= bx.y) {
+          const double2 sv = Sc[j * nx + i];
+          t = cadd(t, C(sv.x, sv.y));
+        }
+        if (i == 1) {
+          DD = cdiv_inv(t, T.ax_p[1], T.ax_pinv[1]);
+        } else if (i < nx - 2) {
+          DD = csub(cdiv_inv(t, T.ax_p[i], T.ax_pinv[i]), cdiv_inv(cmul(T.ax_a[i], DD), T.ax_q[i], T.ax_qinv[i]));
+        } else {
+          DD = csub(t, cdiv_inv(DD, T.ax_cc[nx - 3], T.ax_ccinv[nx - 3]));
+        }
+        Apl[j * nxp + i] = make_double2(DD.re, DD.im);
+      }
+      cd Uc = cdiv_inv(DD, T.ax_cc[nx - 2], T.ax_ccinv[nx - 2]);
+      Apl[j * nxp + nx - 2] = make_double2(Uc.re, Uc.im);
+      for (int i = nx - 3; i > 0; --i) {
+        const double2 d = Apl[j * nxp + i];
+        Uc = cdiv_inv(csub(C(d.x, d.y), Uc), T.ax_cc[i], T.ax_ccinv[i]);
+        Apl[j * nxp + i] = make_double2(Uc.re, Uc.im);
+      }
+      Apl[j * nxp + 0] = make_double2(0.0, 0.0);
+      Apl[j * nxp + nx - 1] = make_double2(0.0, 0.0);
+    }
+  }
+  __syncthreads();
+  // ---- y sweep: thread per column i, one barrier per row ----
+  const int i = tid;
+  const bool col = i >= 1 && i <= nx - 2;
+  cd rm = C(0, 0), r0 = C(0, 0), rp = C(0, 0);
+  if (col) { rm = T.ry_m[i]; r0 = T.ry_0[i]; rp = T.ry_p[i]; }
+  const bool colin = src && i >= bx.x && i <= bx.y;
+  cd DD = C(0, 0);
+  for (int j = 1; j <= ny - 2; ++j) {
+    double2 up = make_double2(0, 0), u0 = up, um = up;
+    if (col) { up = Apl[j * nxp + i + 1]; u0 = Apl[j * nxp + i]; um = Apl[j * nxp + i - 1]; }
+    __syncthreads();
+    if (col) {
+      cd t = cmul(rm, C(up.x, up.y));
+      t = cadd(t, cmul(r0, C(u0.x, u0.y)));
+      t = csub(t, cmul(rp, C(um.x, um.y)));
+      if (colin && j >= bx.z && j <= bx.w) {
+        const double2 sv = Sc[j * nx + i];
+        t = cadd(t, C(sv.x, sv.y));
+      }
+      if (j == 1) {
+        DD = cdiv_inv(t, T.ay_p[1], T.ay_pinv[1]);
+      } else if (j < ny - 2) {
+        DD = csub(cdiv_inv(t, T.ay_p[j], T.ay_pinv[j]), cdiv_inv(cmul(T.ay_a[j], DD), T.ay_q[j], T.ay_qinv[j]));
+      } else {
+        DD = csub(t, cdiv_inv(DD, T.ay_cc[ny - 3], T.ay_ccinv[ny - 3]));
+      }
+      Apl[j * nxp + i] = make_double2(DD.re, DD.im);
+    }
+  }
+  double e = 0.0;
+  if (col) {
+    cd Un = cdiv_inv(DD, T.ay_cc[ny - 2], T.ay_ccinv[ny - 2]);
+    U[(ny - 2) * nx + i] = make_double2(Un.re, Un.im);
+    double en[1] = {cnorm(Un)};
+    for (int j = ny - 3; j > 0; --j) {
+      const double2 d = Apl[j * nxp + i];
+      Un = cdiv_inv(csub(C(d.x, d.y), Un), T.ay_cc[j], T.ay_ccinv[j]);
+      U[j * nx + i] = make_double2(Un.re, Un.im);
+      en[0] += cnorm(Un);
+    }
+    e = en[0];
+  }
+  if (a.energy) {
+    // boundary cells keep their values (the ADI never writes them)
+    if (tid < nx) {
+      const double2 b0 = U[tid], b1 = U[(ny - 1) * nx + tid];
+      e += b0.x * b0.x + b0.y * b0.y + b1.x * b1.x + b1.y * b1.y;
+      if (tid == 0 || tid == nx - 1)
+        for (int j = 1; j <= ny - 2; ++j) {
+          const double2 b = U[j * nx + tid];
+          e += b.x * b.x + b.y * b.y;
+        }
+    }
+    const double t = block_sum(e, red);
+    if (tid == 0) a.energy[(size_t)hp * S + s] = t;
+  }
+}
+
+// Plane sums of |U|^2 (updateTotalEnergy.cpp:25-33), one block per plane.
+__global__ void __launch_bounds__(256) k_energy(DevGeom G, const double2* U, int ring_base, double* out) {
+  __shared__ double red[8];
+  const int S = G.S;
+  const int s = blockIdx.x % S, hp = blockIdx.x / S;
+  const double2* P = U + field_plane(S, hp >> 1, hp & 1, s, ring_base) * G.N;
+  double e = 0.0;
+  for (int k = threadIdx.x; k < G.N; k += blockDim.x) {
+    const double2 v = P[k];
+    e += v.x * v.x + v.y * v.y;
+  }
+  const double t = block_sum(e, red);
+  if (threadIdx.x == 0) out[(size_t)hp * S + s] = t;
+}
+
+// out[hp] = sum over planes s of planes[hp][s], s < S - skip_last (fixed order).
+__global__ void __launch_bounds__(256) k_sum_planes(const double* planes, int S, int skip_last, double* out) {
+  __shared__ double red[8];
+  const int hp = blockIdx.x;
+  double e = 0.0;
+  for (int s = threadIdx.x; s < S - skip_last; s += blockDim.x) e += planes[(size_t)hp * S + s];
+  const double t = block_sum(e, red);
+  if (threadIdx.x == 0) out[hp] = t;
+}
+
+}  // namespace
+
+size_t deposit_smem_bytes(int cap, int L, int F, int nr) {
+  // sort keys, then the radial bins and the modified Thomas diagonal
+  return (((size_t)cap * sizeof(uint32_t) + 15) & ~(size_t)15) + (size_t)L * F * nr * (sizeof(double2) + sizeof(double));
+}
+
+void launch_deposit(const DepositLaunch& a, cudaStream_t st) {
+  const size_t smem = deposit_smem_bytes(a.cap, a.G.L, a.G.F, a.G.nr);
+  k_deposit<<<a.G.S, 512, smem, st>>>(a);
+}
+
+void deposit_set_smem(size_t bytes) {
+  cudaFuncSetAttribute(k_deposit, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+void adi_set_smem(size_t bytes) {
+  cudaFuncSetAttribute(k_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
+}
+
+size_t adi_smem_bytes(int nx, int ny, int nxp) { return (size_t)ny * nxp * sizeof(double2); }
+
+void launch_adi(const AdiLaunch& a, cudaStream_t st) {
+  const int mx = a.G.nx > a.G.ny ? a.G.nx : a.G.ny;
+  const int threads = ((mx + 31) / 32) * 32;
+  k_adi<<<a.G.S * a.G.H * 2, threads, adi_smem_bytes(a.G.nx, a.G.ny, a.nxp), st>>>(a);
+}
+
+void launch_energy(const DevGeom& G, const double2* U, int ring_base, double* out_planes, cudaStream_t st) {
+  k_energy<<<G.S * G.H * 2, 256, 0, st>>>(G, U, ring_base, out_planes);
+}
+
+void launch_sum_planes(const double* planes, int H, int S, int skip_last, double* out, cudaStream_t st) {
+  k_sum_planes<<<H * 2, 256, 0, st>>>(planes, S, skip_last, out);
+}
+
+}  // namespace felis

@@ -1,0 +1,179 @@
+"""Input files (FELIS .inp format) for the workloads this library is measured on.
+
+The reference publishes no benchmark inputs; these are the synthetic beams
+of the project's workload table, written in the reference's own input format
+(README.md:51-187; keys as parsed by parameterSetting.cpp):
+
+  static   Plain FP64 steady-state single slice: 8 GeV, relative energy
+           spread 1e-4, normalised emittance 0.4 um, beta 20 m, 3 kA;
+           2048 beamlets x 4 quiet-start particles; BiPolar undulator
+           lambda_u 2.6 cm, K0 2.6, 10 units of 3.4 m with 0.6 m in-air gaps;
+           1 MW Gaussian seed, waist 30 um; 102 x 102 grid over +-300 um,
+           ABC_N 10; 40 m (1539 steps of one period).
+  sase     Plain FP64 time-dependent SASE: the same beam and undulator,
+           flat-top 3 kA over 1024 slices, 8192 particles per slice with
+           shot-noise phases, no seed.
+
+The seed is put into the x polarisation (laser_alpha = 1), the one a
+K0_alpha = 1 planar undulator couples to; with the reference's default
+laser_alpha = -1 it would land in Uy and never interact.
+"""
+from __future__ import annotations
+
+import os
+import tempfile
+
+PLANCK_H = 4.135667696e-15  # [eV s], constants.h
+C_LIGHT = 299792458.0
+MC2 = 0.510998918
+
+
+def resonant_photon_energy(energy_mev: float, lambda_u_cm: float, K0: float) -> float:
+    gamma = energy_mev / MC2 + 1.0
+    lam_u = lambda_u_cm * 0.01
+    lam0 = lam_u / (2.0 * gamma * gamma) * (1.0 + 0.5 * K0 * K0)
+    return PLANCK_H * C_LIGHT / lam0
+
+
+def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, per_beamlet: int = 4,
+               nx: int = 101, window_um: float = 300.0, total_length: float = 40.0, harmonics=(1,),
+               energy_mev: float = 8000.0, spread_pct: float = 0.01, emit_um: float = 0.4, beta: float = 20.0,
+               current: float = 3000.0, K0: float = 2.6, lambda_u_cm: float = 2.6, units: int = 10,
+               unit_len: float = 4.0, und_len: float = 3.4, seed_power: float = 1e6, seed_sigma_um: float = 30.0,
+               noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
+               linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
+               in_air: bool = True) -> str:
+    static = kind == "static"
+    if noise is None:
+        noise = not static
+    photon = resonant_photon_energy(energy_mev, lambda_u_cm, K0)
+    lam0_um = PLANCK_H * C_LIGHT / photon * 1e6
+    minZ, maxZ = 0.0, (slices + 0.5) * lam0_um
+    harm = "\n".join(f" harmony{i} = {h}" for i, h in enumerate(harmonics))
+    zspan = 1.0e-3
+    quad_block = ""
+    if quads:
+        quad_block = """
+[Quad]
+ numbers=10
+ unit_start = 3.6
+ unit_end = 7.6
+ quad_start = 3.6
+ quad_end = 3.7
+ g = 10
+
+[Quad]
+ numbers=10
+ unit_start = 5.6
+ unit_end = 9.6
+ quad_start = 5.6
+ quad_end = 5.7
+ g = -10
+"""
+    return f"""// generated by felis_b200.workloads ({kind})
+[Save]
+ field_save=OFF
+ particle_save=OFF
+ total_length={total_length}
+ save_step=1000000
+ save_start=1000000
+
+[Domain]
+ dimension=3
+ mode={'Static' if static else 'Time_Dependent'}
+ minZ={minZ!r}
+ maxZ={maxZ!r}
+ minX={-window_um}
+ maxX={window_um}
+ minY={-window_um}
+ maxY={window_um}
+ nx={nx}
+ ny={nx}
+ photon_energy={photon!r}
+ num_harmony={len(harmonics)}
+{harm}
+ slices_in_bucket=1
+ lambdaUs_in_iteration=1
+ ABC_N={abc_n}
+ ABC_coef=1
+
+[Seed]
+ power={seed_power}
+ rms_duration=1e9
+ spot_sigma_R={seed_sigma_um}
+ focus=0
+ laser_alpha=1
+
+[Undulator]
+ undulator_type={undulator}
+ polarity={polarity}
+ K0_alpha=1
+ numbers={units}
+ in_air={'ON' if in_air else 'OFF'}
+ linear_taper={linear_taper}
+ lambdaU={lambda_u_cm}
+ unit_start=0.0
+ unit_end={unit_len}
+ undulator_start=0.0
+ undulator_end={und_len}
+ K0={K0}
+
+[Wake_field]
+ activate={'ON' if wake else 'OFF'}
+ shape=Circular
+ ac_dc=AC
+ radius=5e-3
+ conductivity=5.8e7
+ ctau=8.1e-6
+{quad_block}
+[EBeam]
+ load_type=Polygon
+ noise_ONOFF={'ON' if noise else 'OFF'}
+ beam_energy={energy_mev}
+ energy_spread={spread_pct}
+ peak_current={current}
+ norm_emittance_x={emit_um}
+ norm_emittance_y={emit_um}
+ beta_x={beta}
+ beta_y={beta}
+ alpha_x=0
+ alpha_y=0
+ beamlets_in_bucket={beamlets}
+ number_in_beamlet={per_beamlet}
+ z_nodes=2
+ z0={-zspan}
+ z1={zspan}
+ z_n0=1
+ z_n1=1
+ energy_nodes=2
+ energy_z0={-zspan}
+ energy_z1={zspan}
+ energy_n0=1
+ energy_n1=1
+ energySpread_nodes=2
+ energySpread_z0={-zspan}
+ energySpread_z1={zspan}
+ energySpread_n0=1
+ energySpread_n1=1
+ emit_nodes=2
+ emit_z0={-zspan}
+ emit_z1={zspan}
+ emit_n0=1
+ emit_n1=1
+"""
+
+
+def write_input(path: str | None = None, kind: str = "sase", **kw) -> str:
+    text = input_text(kind, **kw)
+    if path is None:
+        fd, path = tempfile.mkstemp(prefix=f"felis_{kind}_", suffix=".inp")
+        os.close(fd)
+    with open(path, "w") as f:
+        f.write(text)
+    return path
+
+
+WORKLOADS = {
+    "static": dict(kind="static"),
+    "sase": dict(kind="sase"),
+}

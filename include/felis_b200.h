@@ -1,0 +1,255 @@
+/* felis_b200.h — C ABI of the B200-native FELIS slice loop.
+ *
+ * The reference (scienter/felis) has no plugin API: its per-step loop
+ * (main.cpp:92-156) calls plain C++ functions that mutate one shared Domain
+ * (mesh.h:150-178), and its errors end the process (exit / MPI_Abort).
+ * This header replaces those functions one for one with entry points that
+ * take an opaque handle, keep every array resident in HBM, and return a
+ * status instead of exiting.  Each declaration cites the reference function
+ * it stands in for.
+ *
+ * Conventions
+ *   - Every function returns felis_status; felis_last_error() gives text.
+ *     The library never calls exit().
+ *   - The library owns device memory.  Callers own host buffers; copies are
+ *     synchronous (the call returns when the host buffer may be reused).
+ *   - One handle per host thread; one CUDA stream per handle.
+ *   - Complex numbers are interleaved (re, im) FP64, the memory layout of
+ *     std::complex<double>.
+ *   - Field arrays use the reference layout: per harmonic and polarisation
+ *     (slice_n + 2) planes of ny rows by nx points, ghost planes 0 and
+ *     slice_n + 1 included (boundary.cpp:49-53).
+ *   - Particles are structure-of-arrays, concatenated slice by slice in
+ *     slice order, with slice_offsets[slice_n + 1] giving each slice's range
+ *     (the per-slice ptclList of particle.h:24-35, flattened).
+ */
+#ifndef FELIS_B200_H
+#define FELIS_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#define FELIS_ABI_VERSION 1
+#define FELIS_MAX_HARMONY 8
+#define FELIS_MAX_SPECIES 8
+
+typedef enum felis_status {
+  FELIS_OK = 0,
+  FELIS_BAD_ARG = 1,        /* invalid argument or size */
+  FELIS_CUDA_ERROR = 2,     /* a CUDA runtime call failed */
+  FELIS_THETA_OVERFLOW = 3, /* |dtheta| > 2 pi numSlice in the push (particlePush.cpp:371-374) */
+  FELIS_OUT_OF_RANGE = 4,   /* theta outside [0, dTh] after the wrap (rearrangeParticles.cpp:105-108) */
+  FELIS_NAN = 5,            /* non-finite value found in the particle state */
+  FELIS_TIMEOUT = 6,        /* a bounded device wait gave up */
+  FELIS_UNSUPPORTED = 7,    /* configuration this build does not implement */
+  FELIS_NO_DEVICE = 8,      /* no CUDA device */
+  FELIS_IO = 9,             /* input file could not be read or parsed */
+  FELIS_NOT_FOUND = 10      /* a key or block is missing from the input file */
+} felis_status;
+
+typedef enum felis_mode { FELIS_STATIC = 1, FELIS_TIME_DEPENDENT = 2 } felis_mode;
+typedef enum felis_und_type { FELIS_BIPOLAR = 1, FELIS_QUADPOLAR = 2 } felis_und_type;
+typedef enum felis_precision {
+  FELIS_FP64 = 0,  /* plain path: FP64 everywhere, bit-exact with the CPU restatement */
+  FELIS_MIXED = 1  /* FP32 push and ADI; FP64 theta, reductions and lattice */
+} felis_precision;
+
+/* One [Undulator] block after parameterSetting.cpp:345-429 (UndList, mesh.h:44-56). */
+typedef struct felis_undulator {
+  int32_t type;     /* felis_und_type */
+  int32_t K0_alpha; /* +1: By major, -1: Bx major */
+  int32_t numbers;  /* units in this block */
+  int32_t air;      /* in_air */
+  double lambdaU;   /* [m] */
+  double slopeK;    /* slope_K / sqrt(2) [1/m] */
+  double ue;        /* polarity */
+  const double* unit_start; /* [numbers] each, [m] */
+  const double* unit_end;
+  const double* und_start;
+  const double* und_end;
+  const double* K0;
+} felis_undulator;
+
+/* One [Quad] block after parameterSetting.cpp:287-338 (QuadList, mesh.h:58-63). */
+typedef struct felis_quad {
+  int32_t numbers;
+  int32_t pad_;
+  const double* unit_start;
+  const double* unit_end;
+  const double* qd_start;
+  const double* qd_end;
+  const double* g; /* [T/m] */
+} felis_quad;
+
+/* Domain scalars and tables after parameterSetting() + boundary()
+ * (parameterSetting.cpp:42-285, boundary.cpp:20-124).  Arrays are read
+ * during felis_create() only. */
+typedef struct felis_params {
+  int32_t abi_version; /* FELIS_ABI_VERSION */
+  int32_t precision;   /* felis_precision */
+  int32_t dimension;   /* 3 (the 1D model is not implemented on the GPU) */
+  int32_t mode;        /* felis_mode */
+  int32_t num_harmony;
+  int32_t harmony[FELIS_MAX_HARMONY];
+  int32_t slice_n;        /* slices held by this handle (subSliceN) */
+  int32_t min_i;          /* global index of the first slice (D->minI) */
+  int32_t global_slice_n; /* D->sliceN; length of wake_e */
+  int32_t nx, ny;         /* grid points (input key + 1, parameterSetting.cpp:108-111) */
+  int32_t num_slice;      /* slices_in_bucket */
+  int32_t num_lambda_u;   /* lambdaUs_in_iteration */
+  int32_t num_species;
+  int32_t scl_mode, scf_mode, nr; /* L, F, radial grid of the Ez solve */
+  int32_t bessel_rows, bessel_cols; /* bn, BesselMaxOrder */
+  int32_t abc_n;
+  int32_t wake_on;
+  int32_t max_step;
+  int32_t num_undulators, num_quads;
+  double ks, lambda0, dz, dx, dy, dr;
+  double min_x, max_x, min_y, max_y, min_z, max_z;
+  double gamma0, gam_r, d_bessel, abc_sig, spot_sig_r;
+  /* lattice state after parameterSetting (D->K0, ue, K0_alpha, lambdaU, undType) */
+  double K0_init, ue_init, lambdaU_init;
+  int32_t K0_alpha_init, und_type_init;
+  /* tables from boundary(): ABC coefficients (complex, nx or ny entries),
+   * Bessel table (bessel_rows x bessel_cols, row-major), wake energy loss per
+   * global slice (wakeField.cpp:9-50; may be NULL when wake_on == 0). */
+  const double* abc_alpha;
+  const double* abc_alpha_p;
+  const double* abc_beta;
+  const double* abc_beta_p;
+  const double* bessel;
+  const double* wake_e;
+  const felis_undulator* undulators;
+  const felis_quad* quads;
+} felis_params;
+
+/* Lattice state that updateK_quadG() leaves in Domain (updateK_quadG.cpp:8-94). */
+typedef struct felis_lattice {
+  double K0, ue, lambdaU, ku, g;
+  int32_t K0_alpha, und_type, current_flag, drift_flag;
+} felis_lattice;
+
+typedef struct felis_handle felis_handle;
+
+/* ---- lifecycle (boundary.cpp:20-71 allocation) ------------------------- */
+felis_status felis_create(const felis_params* params, felis_handle** out);
+void felis_destroy(felis_handle* h);
+const char* felis_last_error(const felis_handle* h);
+felis_status felis_device_info(char* name, size_t name_len, int32_t* sm_count);
+
+/* ---- data in / out ------------------------------------------------------
+ * Particles of one species (loadBeam.cpp:158-246 / restoreParticleHDF.cpp:166-214
+ * fill the same per-slice arrays).  slice_offsets has slice_n + 1 entries,
+ * weights has slice_n entries (ptclList::weight). */
+felis_status felis_upload_particles(felis_handle* h, int32_t species,
+                                    const double* x, const double* y,
+                                    const double* px, const double* py,
+                                    const double* theta, const double* gamma,
+                                    const int64_t* slice_offsets,
+                                    const double* weights);
+felis_status felis_download_particles(felis_handle* h, int32_t species,
+                                      double* x, double* y, double* px,
+                                      double* py, double* theta, double* gamma);
+/* Field of one harmonic index and polarisation (0: Ux, 1: Uy), reference
+ * layout with ghost planes (loadSeed.cpp:74-75 writes it). */
+felis_status felis_upload_field(felis_handle* h, int32_t harmonic_index,
+                                int32_t pol, const double* data);
+felis_status felis_download_field(felis_handle* h, int32_t harmonic_index,
+                                  int32_t pol, double* data);
+/* Source term ScUx/ScUy of the last solve (solveField.cpp:233-312), same
+ * layout; cells the ADI never reads (grid edges) are returned as zero. */
+felis_status felis_download_source(felis_handle* h, int32_t harmonic_index,
+                                   int32_t pol, double* data);
+/* Ez[l][(slice_n+2) * F * nr] of the last space-charge solve. */
+felis_status felis_download_ez(felis_handle* h, double* data);
+
+/* ---- lattice (updateK_quadG.cpp:8-94, evaluated on the host in FP64) ---- */
+felis_status felis_update_lattice(felis_handle* h, int32_t iteration, double half);
+felis_status felis_get_lattice(felis_handle* h, felis_lattice* out);
+felis_status felis_set_lattice(felis_handle* h, const felis_lattice* in);
+
+/* ---- per-step functions (main.cpp:117-149) ------------------------------ */
+/* updateTotalEnergy.cpp:7-45: out[2*h] = sum |Ux_h|^2, out[2*h+1] = sum |Uy_h|^2
+ * over slices 1..slice_n (unscaled, as stored in totalEnergyX/Y). */
+felis_status felis_update_total_energy(felis_handle* h, int32_t iteration, double* out);
+/* twiss.cpp:7-99: per species {emitX, betaX, alphaX, emitY, betaY, alphaY}
+ * (emittance unnormalised, as computed before the file write). */
+felis_status felis_twiss(felis_handle* h, int32_t iteration, double* out);
+/* saveFile.cpp:109-172: per harmonic {Re b, Im b} of sum w e^{iH theta} / sum w. */
+felis_status felis_bfactor(felis_handle* h, int32_t iteration, double* out);
+/* solveField.cpp:49-78: source deposit + Ez (if the lattice's current flag is
+ * set) and the ADI solve of Ux then Uy, every slice and harmonic. */
+felis_status felis_solve_field(felis_handle* h, int32_t iteration);
+/* particlePush.cpp:32-117 (one dz/2 RK4 call with the current lattice). */
+felis_status felis_transverse_push(felis_handle* h, int32_t iteration);
+/* particlePush.cpp:198-386 (push_theta_gamma_3D). */
+felis_status felis_push_theta_gamma(felis_handle* h, int32_t iteration);
+/* particlePush.cpp:119-195 (drift_theta_gamma). */
+felis_status felis_drift_theta_gamma(felis_handle* h, int32_t iteration);
+/* rearrangeParticles.cpp:77-114 (periodicParticles). */
+felis_status felis_periodic_particles(felis_handle* h, int32_t iteration);
+/* solveField.cpp:19-47 + fieldShareZ.cpp:39-78 at one rank (shiftField). */
+felis_status felis_shift_field(felis_handle* h, int32_t iteration);
+
+/* ---- fused helpers ----------------------------------------------------- */
+/* One whole iteration of main.cpp:117-155 (diagnostics recorded on the
+ * device, lattice updated on the host), using the fused kernels. */
+felis_status felis_step(felis_handle* h, int32_t iteration);
+/* Iterations [it0, it1) replayed from one captured CUDA graph. */
+felis_status felis_run(felis_handle* h, int32_t it0, int32_t it1);
+/* Diagnostics recorded by felis_step / felis_run for iterations [it0, it1):
+ * energy[(it-it0)*2H + ...] as felis_update_total_energy, twiss
+ * [(it-it0)*6*num_species + ...] as felis_twiss, bfactor [(it-it0)*2H + ...]
+ * as felis_bfactor.  Any pointer may be NULL. */
+felis_status felis_get_diagnostics(felis_handle* h, int32_t it0, int32_t it1,
+                                   double* energy, double* twiss, double* bfactor);
+/* Count of deposit particles that hit the q6 edge case (cell index nx-1 or
+ * ny-1 accepted by solveField.cpp:273), accumulated since creation. */
+felis_status felis_edge_deposit_count(felis_handle* h, int64_t* count);
+
+/* ---- slice sort (the slice binning of restoreParticleHDF.cpp:166-214 and
+ * the slice-major write order of saveParticleHDF.cpp:95-109) -------------
+ * Stable sort of n particles by integer slice key on the GPU: perm[k] is the
+ * input row that lands at position k; equal keys keep input order.  Keys
+ * must lie in [0, 2^30). */
+felis_status felis_sort_by_slice(const int32_t* keys, int64_t n, int64_t* perm);
+
+/* ---- host-side setup of the reference's input format -------------------- */
+/* Parses a FELIS input file ([Domain], [Save], [Seed], [Undulator], [Quad],
+ * [EBeam], [Wake_field], [Bessel_table], [Phase_shifter] blocks;
+ * findparam.cpp:30-116, parameterSetting.cpp:42-627) and builds the tables
+ * of boundary.cpp:73-124.  The returned object owns every array that
+ * felis_params points to. */
+typedef struct felis_config felis_config;
+felis_status felis_config_load(const char* path, int32_t num_ranks, int32_t rank,
+                               felis_config** out);
+void felis_config_free(felis_config* c);
+const felis_params* felis_config_params(const felis_config* c);
+const char* felis_config_error(void);
+/* Initial particles of one species (loadBeam.cpp:28-269): writes counts per
+ * slice (slice_n entries) when the arrays are NULL; fills them otherwise.
+ * `seed` plays the role of GSL_RNG_SEED. */
+felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t seed,
+                                    int64_t* counts, double* x, double* y,
+                                    double* px, double* py, double* theta,
+                                    double* gamma, double* weights);
+/* Initial seed field (loadSeed.cpp:25-80), reference layout, both pols. */
+felis_status felis_config_load_seed(felis_config* c, int32_t harmonic_index,
+                                    double* ux, double* uy);
+/* Wake energy loss per slice (wakeField.cpp:9-50,53-159,161-223) from the
+ * per-slice charge (den[s] = weight * count, summed over species). */
+felis_status felis_config_wake(felis_config* c, const double* den, double* wake_e);
+
+/* ---- deterministic elementary functions (host versions, for tests) ------ */
+void felis_detmath_sincos(double x, double* s, double* c);
+double felis_detmath_atan(double x);
+double felis_detmath_atan2(double y, double x);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* FELIS_B200_H */
