@@ -1,0 +1,365 @@
+"""Throughput of the FELIS slice loop on B200.
+
+Workload (default `sase`): plain FP64 time-dependent SASE, 8 GeV beam,
+flat-top 3 kA over 1024 slices of 8192 particles (8,388,608 in all) with
+shot-noise phases, BiPolar undulator lambda_u = 2.6 cm, K0 = 2.6,
+102 x 102 grid over +-300 um, one step per undulator period.  A "step" is
+one iteration of the reference loop (main.cpp:117-155) over every slice.
+
+  python bench.py [--gpus N] [--steps K] [--warmup W] [--impl felis|reference]
+
+--impl felis      the GPU library: W untimed iterations, then K iterations
+                  replayed from one CUDA graph, timed with CUDA events on the
+                  library's stream (inputs resident in HBM); also the same
+                  loop end to end through the C ABI with host buffers, and the
+                  CPU restatement on a bounded sample as a reported baseline.
+--impl reference  the reference's CPU path (the oracle port: the reference
+                  does not build here, it needs MPI/HDF5/GSL) on the host's
+                  cores, on a bounded sample of the same workload.
+Under torchrun (N > 1) every rank runs its own copy of the workload on its
+GPU (weak scaling); time is the max over ranks.
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "particle-steps/s + ADI cells/s vs FP64 plain GPU path at <=1% power error"
+UNIT = "particle-steps/s"
+BYTES_PARTICLE_STEP = 96   # FP64: read + write 6 x 8 B of state
+BYTES_ADI_CELL = 32        # FP64: read + write one complex cell
+
+
+def peaks() -> tuple[float, str]:
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["hbm_gbs"]), "measured"
+    except Exception:
+        return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    def __init__(self, index: int = 0):
+        self.path = tempfile.mktemp(prefix="felis_clocks_", suffix=".csv")
+        q = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+             "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+             "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+        try:
+            self.proc = subprocess.Popen(["nvidia-smi", f"--id={index}", f"--query-gpu={q}", "--format=csv,noheader,nounits",
+                                          "-lms", "200"], stdout=open(self.path, "w"), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self) -> dict:
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        time.sleep(0.25)
+        self.proc.terminate()
+        self.proc.wait()
+        sm, smax, reasons = [], [], set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        with open(self.path) as f:
+            for line in f:
+                parts = [x.strip() for x in line.split(",")]
+                if len(parts) < 9:
+                    continue
+                try:
+                    sm.append(float(parts[1]))
+                    smax.append(float(parts[2]))
+                except ValueError:
+                    continue
+                for n, v in zip(names, parts[5:9]):
+                    if v.lower() == "active":
+                        reasons.add(n)
+        os.unlink(self.path)
+        return {"sm_mhz": statistics.median(sm) if sm else None, "sm_max_mhz": max(smax) if smax else None,
+                "reasons": sorted(reasons), "samples": len(sm)}
+
+
+def make_workload(name: str, rank: int = 0, slices: int | None = None):
+    import felis_b200 as fb
+    from felis_b200 import workloads
+
+    d = tempfile.mkdtemp(prefix="felis_bench_")
+    kw = dict(workloads.WORKLOADS[name])
+    if slices and name == "sase":
+        kw["slices"] = slices
+    path = workloads.write_input(os.path.join(d, f"{name}.inp"), **kw)
+    cfg = fb.Config(path)
+    beam = cfg.load_beam(0, seed=2 if name == "sase" else 1)
+    fields = [cfg.load_seed(h) for h in range(cfg.params.num_harmony)]
+    return cfg, beam, fields
+
+
+def dist_init():
+    world = int(os.environ.get("WORLD_SIZE", "1"))
+    if world <= 1:
+        return None, 0, 1
+    import datetime
+
+    import torch
+    import torch.distributed as dist
+
+    rank = int(os.environ["RANK"])
+    local = int(os.environ.get("LOCAL_RANK", rank))
+    torch.cuda.set_device(local)
+    dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=300))
+    return dist, rank, world
+
+
+def max_over_ranks(dist, v: float) -> float:
+    if dist is None:
+        return v
+    import torch
+
+    t = torch.tensor([v], dtype=torch.float64, device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+def barrier(dist):
+    if dist is not None:
+        dist.barrier()
+
+
+def cpu_sample(name: str, steps: int, warmup: int, target_s: float, threads: int):
+    """Oracle (reference CPU path restated, reference compiler flags) on a slice
+    subset of the workload; returns particle-steps/s and a description."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import oracle
+
+    import felis_b200 as fb
+    from felis_b200 import workloads
+
+    out_dir = tempfile.mkdtemp(prefix="felis_oracle_")
+    variant = "fast"
+    try:
+        oracle.build("fast", out_dir)
+    except Exception:
+        variant, out_dir = "strict", None
+    base = dict(workloads.WORKLOADS[name])
+    total_slices = 1024 if name == "sase" else 1
+
+    def run(slices: int, nsteps: int):
+        kw = dict(base)
+        if name == "sase":
+            kw["slices"] = slices
+        d = tempfile.mkdtemp(prefix="felis_cpu_")
+        cfg = fb.Config(workloads.write_input(os.path.join(d, "s.inp"), **kw))
+        b = cfg.load_beam(0, seed=2 if name == "sase" else 1)
+        o = oracle.Oracle(cfg.params, threads=threads, variant=variant, out_dir=out_dir)
+        o.set_particles(0, b["x"], b["y"], b["px"], b["py"], b["theta"], b["gamma"], b["offsets"], b["weights"])
+        for hh in range(cfg.params.num_harmony):
+            ux, uy = cfg.load_seed(hh)
+            o.set_field(hh, 0, ux)
+            o.set_field(hh, 1, uy)
+        o.run(0, warmup, diagnostics=True)
+        t0 = time.perf_counter()
+        o.run(warmup, warmup + nsteps, diagnostics=True)
+        dt = time.perf_counter() - t0
+        return int(b["offsets"][-1]), dt, cfg.params
+
+    # calibrate on one slice per thread for one iteration, then size the
+    # sample so the timed part takes about target_s seconds
+    probe = min(total_slices, threads)
+    n, dt, p = run(probe, 1)
+    rate = n / max(dt, 1e-6)
+    per_slice = max(n // probe, 1)
+    nsteps = max(1, min(steps, 3))
+    slices = total_slices if name != "sase" else int(min(total_slices, max(probe, target_s * rate / (per_slice * nsteps))))
+    n, dt, p = run(slices, nsteps)
+    value = n * nsteps / dt
+    sample = (f"{slices} of {total_slices} slices x {n // max(slices, 1)} particles, iterations "
+              f"{warmup}..{warmup + nsteps - 1} after {warmup} untimed, {dt:.1f} s timed on {threads} threads")
+    return value, sample, variant
+
+
+def run_felis(args, dist, rank, world):
+    import numpy as np
+
+    import felis_b200 as fb
+
+    cfg, beam, fields = make_workload(args.workload, rank, args.slices)
+    p = cfg.params
+    P = int(beam["offsets"][-1])
+    cells = p.slice_n * p.nx * p.ny * 2 * p.num_harmony
+    h = fb.Handle(p)
+    h.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
+                       beam["offsets"], beam["weights"])
+    for hh, (ux, uy) in enumerate(fields):
+        h.upload_field(hh, 0, ux)
+        h.upload_field(hh, 1, uy)
+    W, K = args.warmup, args.steps
+    h.run(0, W)
+    h.sync()
+    # ---- timed region: K iterations from one graph, events on the library stream ----
+    h.profile(True, max_launches=16 * K + 64)
+    barrier(dist)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    time.sleep(0.3)
+    h.run(W, W + K)
+    h.sync()
+    ms = h.last_run_ms()
+    clk = clocks.stop()
+    barrier(dist)
+    ms = max_over_ranks(dist, ms)
+    sec = ms / 1e3
+    kinds = {}
+    for name, k in fb.KERNEL_KINDS.items():
+        n, t = h.kernel_stats(k)
+        kinds[name] = {"launches": n, "ms": t}
+    launches, _ = h.kernel_stats(-1)
+    e, tw, bf = h.diagnostics(W, W + K)
+    value = P * K * world / sec
+    adi_cells = cells * K * world / sec
+    # dominant kernel roofline (HBM): algorithmic bytes per launch / mean launch time
+    dom = max(kinds, key=lambda k: kinds[k]["ms"])
+    bytes_per_launch = {"particles": P * BYTES_PARTICLE_STEP, "adi": cells * BYTES_ADI_CELL,
+                        "deposit": P * 4 + p.slice_n * p.nx * p.ny * 2 * p.num_harmony * 16,
+                        "reduce": 0, "shift": 0}
+    peak, peak_kind = peaks()
+    kd = kinds[dom]
+    avg_ms = kd["ms"] / max(kd["launches"], 1)
+    achieved = bytes_per_launch[dom] / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    step_bytes = P * BYTES_PARTICLE_STEP + cells * BYTES_ADI_CELL
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_path):
+        try:
+            with open(prof_path) as f:
+                traffic = json.load(f).get(args.workload, {}).get(dom)
+        except Exception:
+            traffic = None
+    # ---- end to end through the C ABI with host buffers ----
+    e2e = run_e2e(args, cfg, beam, fields, dist)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded beam loader of the reference input format)",
+        "config": {"workload": f"{args.workload}: FP64 time-dependent SASE, {p.slice_n} slices x "
+                               f"{P // p.slice_n} particles, {p.nx}x{p.ny} grid, H={p.num_harmony}"
+                   if args.workload == "sase" else f"{args.workload}: FP64 static, {P} particles, {p.nx}x{p.ny} grid",
+                   "slices": p.slice_n, "particles": P, "grid": [p.nx, p.ny], "harmonics": p.num_harmony,
+                   "iterations": [W, W + K], "l2": "inputs larger than L2 (particles 403 MB, field 171 MB per pol)",
+                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "adi_cells_per_s": adi_cells,
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_per_launch": bytes_per_launch[dom], "mean_launch_ms": avg_ms},
+        "step_roofline": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (ms / K / 1e3) / 1e9,
+                          "frac": step_bytes / (ms / K / 1e3) / 1e9 / peak},
+        "kernels": kinds,
+        "gpu_launches": launches,
+        "clocks": clk,
+        "e2e": e2e,
+        "final_power_units": float(e[-1, 0]),
+    }
+    return line
+
+
+def run_e2e(args, cfg, beam, fields, dist):
+    """Upload from pinned host memory, K iterations through felis_step with
+    each iteration's diagnostics read back, final particles downloaded."""
+    import numpy as np
+
+    import felis_b200 as fb
+
+    try:
+        import torch
+
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.complex128, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+    except Exception:
+        def pinned(a):
+            return np.array(a)
+
+    p = cfg.params
+    host = {k: pinned(np.asarray(beam[k])) for k in ("x", "y", "px", "py", "theta", "gamma")}
+    hf = [(pinned(ux), pinned(uy)) for ux, uy in fields]
+    K = max(1, min(args.steps, args.e2e_steps))
+    P = int(beam["offsets"][-1])
+    h = fb.Handle(p)
+    barrier(dist)
+    t0 = time.perf_counter()
+    h.upload_particles(0, host["x"], host["y"], host["px"], host["py"], host["theta"], host["gamma"],
+                       beam["offsets"], beam["weights"])
+    for hh, (ux, uy) in enumerate(hf):
+        h.upload_field(hh, 0, ux)
+        h.upload_field(hh, 1, uy)
+    for it in range(K):
+        h.step(it)
+        h.diagnostics(it, it + 1)
+    out = h.download_particles(0)
+    dt = time.perf_counter() - t0
+    barrier(dist)
+    dt = max_over_ranks(dist, dt)
+    world = 1 if dist is None else dist.get_world_size()
+    h2d = 6 * P * 8 + sum(2 * a.nbytes for a, _ in hf)
+    d2h = K * (2 * p.num_harmony + 6 * p.num_species + 2 * p.num_harmony) * 8 + 6 * P * 8
+    h.close()
+    return {"value": P * K * world / dt, "unit": UNIT, "steps": K, "seconds": dt,
+            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+            "api": "felis_upload_* + felis_step + felis_get_diagnostics per iteration + felis_download_particles"}
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=200)
+    ap.add_argument("--warmup", type=int, default=5)
+    ap.add_argument("--impl", choices=["felis", "reference"], default="felis")
+    ap.add_argument("--workload", choices=["sase", "static"], default="sase")
+    ap.add_argument("--cpu-seconds", type=float, default=15.0)
+    ap.add_argument("--e2e-steps", type=int, default=100)
+    ap.add_argument("--no-cpu-baseline", action="store_true")
+    ap.add_argument("--slices", type=int, default=None, help="smaller sase bunch (profiling captures)")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        ap.error("--warmup must be >= 3")
+    threads = os.cpu_count() or 1
+
+    if args.impl == "reference":
+        rank = int(os.environ.get("RANK", "0"))
+        if rank != 0:
+            return
+        value, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, 20.0, threads)
+        print(json.dumps({
+            "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "higher_is_better": True,
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
+            "config": {"workload": args.workload},
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
+                             "sample": sample + f"; oracle build '{variant}' (reference compiler flags)"},
+            "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+        }), flush=True)
+        return
+
+    dist, rank, world = dist_init()
+    line = run_felis(args, dist, rank, world)
+    if rank == 0:
+        if args.no_cpu_baseline:
+            line["cpu_baseline"] = None
+        else:
+            v, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, args.cpu_seconds, threads)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
+                                    "sample": sample + f"; oracle build '{variant}' (reference compiler flags)"}
+        print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.destroy_process_group()
+
+
+if __name__ == "__main__":
+    main()

@@ -30,6 +30,7 @@ OK, BAD_ARG, CUDA_ERROR, THETA_OVERFLOW, OUT_OF_RANGE, NAN, TIMEOUT, UNSUPPORTED
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA_ERROR", 3: "THETA_OVERFLOW", 4: "OUT_OF_RANGE", 5: "NAN",
                 6: "TIMEOUT", 7: "UNSUPPORTED", 8: "NO_DEVICE", 9: "IO", 10: "NOT_FOUND"}
 STATIC, TIME_DEPENDENT = 1, 2
+KERNEL_KINDS = {"particles": 0, "deposit": 1, "adi": 2, "reduce": 3, "shift": 4}
 BIPOLAR, QUADPOLAR = 1, 2
 FP64, MIXED = 0, 1
 
@@ -107,6 +108,10 @@ _sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, _dp, _dp, _dp)
 _sig("felis_edge_deposit_count", C.c_int, _vp, _i64p)
 _sig("felis_sort_by_slice", C.c_int, _i32p, C.c_int64, _i64p)
+_sig("felis_sync", C.c_int, _vp)
+_sig("felis_profile", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_kernel_stats", C.c_int, _vp, C.c_int32, _i64p, _dp)
+_sig("felis_last_run_ms", C.c_int, _vp, _dp)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
 _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
@@ -347,6 +352,23 @@ class Handle:
         c = C.c_int64(0)
         self._ck(_lib.felis_edge_deposit_count(self._h, C.byref(c)))
         return c.value
+
+    def sync(self):
+        self._ck(_lib.felis_sync(self._h))
+
+    def profile(self, enable: bool, max_launches: int = 0):
+        self._ck(_lib.felis_profile(self._h, 1 if enable else 0, max_launches))
+
+    def kernel_stats(self, kind: int = -1) -> tuple[int, float]:
+        n = C.c_int64(0)
+        ms = C.c_double(0)
+        self._ck(_lib.felis_kernel_stats(self._h, kind, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
+
+    def last_run_ms(self) -> float:
+        ms = C.c_double(0)
+        self._ck(_lib.felis_last_run_ms(self._h, C.byref(ms)))
+        return ms.value
 
     def run_loop(self, it0: int, it1: int):
         """The drop-in sequence of main.cpp:117-155 through the per-function calls."""

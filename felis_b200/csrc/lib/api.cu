@@ -97,9 +97,18 @@ struct felis_handle {
   double* d_hist_b = nullptr;     // [max_step+1][2H]
   int hist_n = 0;
   double* d_tmp = nullptr;        // small scratch for per-call outputs
+  double* d_l1 = nullptr;         // level-1 rows of the diagnostic reduction
+  int l1_blocks = 148;
   int* d_err = nullptr;
   int* h_err = nullptr;           // pinned
   int64_t edge_total = 0;
+  // measurement: per-kernel CUDA events on the handle's stream and launch counts
+  bool prof = false;
+  std::vector<cudaEvent_t> ev;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, size_t>> marks;
+  int64_t launches[FELIS_KERNEL_KINDS] = {0};
+  double last_run_ms = 0.0;
   // fused-step state
   bool prep_valid = false;        // deposit records match particles + lattice
   bool diag_valid = false;        // hist row for the next iteration already written
@@ -108,6 +117,28 @@ struct felis_handle {
 };
 
 namespace {
+
+// Brackets one kernel launch: counts it and, when profiling, records CUDA
+// events around it on the handle's stream (event nodes when captured).
+struct KernelScope {
+  felis_handle* h;
+  int kind;
+  size_t slot = (size_t)-1;
+  KernelScope(felis_handle* hh, int k) : h(hh), kind(k) {
+    h->launches[k] += 1;
+    if (h->prof && h->ev_used + 2 <= h->ev.size()) {
+      slot = h->ev_used;
+      h->ev_used += 2;
+      cudaEventRecordWithFlags(h->ev[slot], h->st, h->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
+  }
+  ~KernelScope() {
+    if (slot != (size_t)-1) {
+      cudaEventRecordWithFlags(h->ev[slot + 1], h->st, h->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+      h->marks.emplace_back(kind, slot);
+    }
+  }
+};
 
 #define CK(call)                                                                     \
   do {                                                                               \
@@ -373,7 +404,10 @@ felis_status run_particles(felis_handle* h, unsigned ops, const felis_lattice* l
     if (!push_coef(h, *l1, &a.pc)) return fail(h, FELIS_BAD_ARG, "invalid K0_alpha");
   if (ops & OP_PREP)
     if (!prep_coef(h, *l1, &a.prep)) return fail(h, FELIS_BAD_ARG, "invalid K0_alpha");
-  launch_particles(a, h->st);
+  {
+    KernelScope ks(h, FELIS_KERNEL_PARTICLES);
+    launch_particles(a, h->st);
+  }
   CK(cudaGetLastError());
   return FELIS_OK;
 }
@@ -419,9 +453,13 @@ felis_status run_deposit(felis_handle* h, const felis_lattice& L) {
   const double ks = h->p.ks, ue = L.ue, K0 = L.K0, gamR = h->p.gam_r, dr = h->p.dr;
   d.A = ks * ks * (1.0 + 0.5 * (1.0 + ue * ue) * K0 * K0) / (gamR * gamR) * dr * dr;
   d.cap = h->dep_pcap;
-  d.qbits = h->dep_qbits;
+  d.neven = 0;
+  for (int k = 0; k < h->p.num_harmony; ++k) d.neven += (h->p.harmony[k] % 2 == 0);
   d.err = h->d_err;
-  launch_deposit(d, h->st);
+  {
+    KernelScope ks(h, FELIS_KERNEL_DEPOSIT);
+    launch_deposit(d, h->st);
+  }
   CK(cudaGetLastError());
   return FELIS_OK;
 }
@@ -437,7 +475,10 @@ felis_status run_adi(felis_handle* h, int use_source) {
   a.tab = h->d_adi;
   a.energy = h->d_planes;
   a.nxp = h->nxp;
-  launch_adi(a, h->st);
+  {
+    KernelScope ks(h, FELIS_KERNEL_ADI);
+    launch_adi(a, h->st);
+  }
   CK(cudaGetLastError());
   return FELIS_OK;
 }
@@ -446,6 +487,7 @@ felis_status do_shift(felis_handle* h) {
   const int S = h->p.slice_n;
   h->ring_base = ((h->ring_base - 1) % S + S) % S;
   const size_t N = (size_t)h->p.nx * h->p.ny;
+  KernelScope ks(h, FELIS_KERNEL_SHIFT);
   for (int hh = 0; hh < h->p.num_harmony; ++hh)
     for (int pol = 0; pol < 2; ++pol)
       CK(cudaMemsetAsync(h->U + field_plane(S, hh, pol, 0, h->ring_base) * N, 0, N * sizeof(double2), h->st));
@@ -525,19 +567,25 @@ felis_status relayout(felis_handle* h, const std::vector<int64_t>& new_counts_pe
     CK(cudaMalloc(&h->dep.ez, n * LF * sizeof(double2)));
     h->dep_cap = n;
   }
-  // deposit sort capacity: next power of two >= largest slice
-  int cap = 1, qbits = 0;
-  while (cap < maxslice) { cap <<= 1; ++qbits; }
-  if (qbits == 0) { cap = 2; qbits = 1; }
-  const int64_t N = (int64_t)h->p.nx * h->p.ny;
-  if (qbits > 31 || ((N + 2) >> (32 - qbits)) != 0) return fail(h, FELIS_UNSUPPORTED, "grid x particles-per-slice too large for 32-bit deposit keys");
-  const size_t smem = deposit_smem_bytes(cap, h->p.scl_mode, h->p.scf_mode, h->p.nr);
+  // deposit chunk: the largest power of two (<= 4096) whose sorted keys and
+  // particle records fit in ~100 KB of shared memory (two CTAs per SM)
+  int neven = 0;
+  for (int k = 0; k < h->p.num_harmony; ++k) neven += (h->p.harmony[k] % 2 == 0);
   int dev_smem = 0;
   cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-  if ((int)smem > dev_smem) return fail(h, FELIS_UNSUPPORTED, "slice too large for the shared-memory deposit sort");
+  const size_t budget = std::min<size_t>(100 * 1024, (size_t)dev_smem);
+  int cap = 4096;
+  while (cap > 64 && deposit_smem_bytes(cap, h->p.num_harmony, neven, h->p.scl_mode, h->p.scf_mode, h->p.nr) > budget) cap >>= 1;
+  const size_t smem = deposit_smem_bytes(cap, h->p.num_harmony, neven, h->p.scl_mode, h->p.scf_mode, h->p.nr);
+  if ((int)smem > dev_smem) return fail(h, FELIS_UNSUPPORTED, "deposit records do not fit in shared memory");
+  int qbits = 0;
+  while ((1 << qbits) < cap) ++qbits;
+  const int64_t N = (int64_t)h->p.nx * h->p.ny;
+  if (((N + 2) >> (32 - qbits)) != 0) return fail(h, FELIS_UNSUPPORTED, "grid too large for 32-bit deposit keys");
   deposit_set_smem(smem);
   h->dep_pcap = cap;
   h->dep_qbits = qbits;
+  (void)maxslice;
   invalidate_particles(h);
   return FELIS_OK;
 }
@@ -649,6 +697,7 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
   if (ce == cudaSuccess) ce = cudaMalloc(&h->d_hist_t, (size_t)h->hist_n * 6 * p->num_species * sizeof(double));
   if (ce == cudaSuccess) ce = cudaMalloc(&h->d_hist_b, (size_t)h->hist_n * 2 * H * sizeof(double));
   if (ce == cudaSuccess) ce = cudaMalloc(&h->d_tmp, (size_t)(6 * FELIS_MAX_SPECIES + 4 * FELIS_MAX_HARMONY) * sizeof(double));
+  if (ce == cudaSuccess) ce = cudaMalloc(&h->d_l1, (size_t)h->l1_blocks * (7 * FELIS_MAX_SPECIES + 2 * FELIS_MAX_HARMONY + 1) * sizeof(double));
   if (ce == cudaSuccess) ce = cudaMalloc(&h->d_err, ERR_SLOTS * sizeof(int));
   if (ce == cudaSuccess) ce = cudaMemsetAsync(h->d_err, 0, ERR_SLOTS * sizeof(int), h->st);
   if (ce == cudaSuccess) ce = cudaMallocHost(&h->h_err, ERR_SLOTS * sizeof(int));
@@ -723,11 +772,12 @@ void felis_destroy(felis_handle* h) {
   if (h->st) cudaStreamSynchronize(h->st);
   void* ptrs[] = {h->x, h->y, h->px, h->py, h->th, h->ga, h->d_soff, h->d_weight, h->d_tiles, h->U, h->Sc, h->box,
                   h->Ez, h->d_bessel, h->d_wake, h->d_log, h->d_adi, h->d_part, h->d_planes, h->d_planes2,
-                  h->d_hist_e, h->d_hist_t, h->d_hist_b, h->d_tmp, h->d_err,
+                  h->d_hist_e, h->d_hist_t, h->d_hist_b, h->d_tmp, h->d_l1, h->d_err,
                   h->dep.key, h->dep.rkey, h->dep.wx1, h->dep.wy1, h->dep.wr1, h->dep.coef, h->dep.fx, h->dep.fy, h->dep.ez};
   for (void* q : ptrs) if (q) cudaFree(q);
   for (void* q : h->adi_dev) if (q) cudaFree(q);
   if (h->h_err) cudaFreeHost(h->h_err);
+  for (cudaEvent_t e : h->ev) cudaEventDestroy(e);
   if (h->st) cudaStreamDestroy(h->st);
   delete h;
 }
@@ -878,8 +928,12 @@ felis_status felis_set_lattice(felis_handle* h, const felis_lattice* in) {
 felis_status felis_update_total_energy(felis_handle* h, int32_t it, double* out) {
   if (!h || !out) return FELIS_BAD_ARG;
   (void)it;
-  launch_energy(h->G, h->U, h->ring_base, h->d_planes2, h->st);
-  launch_sum_planes(h->d_planes2, h->p.num_harmony, h->p.slice_n, 0, h->d_tmp, h->st);
+  {
+    KernelScope ks(h, FELIS_KERNEL_REDUCE);
+    launch_energy(h->G, h->U, h->ring_base, h->d_planes2, h->st);
+    launch_sum_planes(h->d_planes2, h->p.num_harmony, h->p.slice_n, 0, h->d_tmp, h->st);
+    h->launches[FELIS_KERNEL_REDUCE] += 1;
+  }
   CK(cudaGetLastError());
   CK(cudaMemcpyAsync(out, h->d_tmp, 2 * h->p.num_harmony * sizeof(double), cudaMemcpyDeviceToHost, h->st));
   CK(cudaStreamSynchronize(h->st));
@@ -891,8 +945,11 @@ static felis_status diag_now(felis_handle* h, double* twiss_dev, double* bf_dev)
   if (s != FELIS_OK) return s;
   s = run_particles(h, OP_DIAG, nullptr, nullptr);
   if (s != FELIS_OK) return s;
-  launch_diag_finalize(h->d_part, (int)h->tiles.size(), h->diag_stride, h->p.num_species, h->p.num_harmony, h->d_tiles,
-                       twiss_dev, bf_dev, h->st);
+  {
+    KernelScope ks(h, FELIS_KERNEL_REDUCE);
+    launch_diag_finalize(h->d_part, (int)h->tiles.size(), h->diag_stride, h->p.num_species, h->p.num_harmony,
+                         h->d_tiles, h->d_l1, h->l1_blocks, twiss_dev, bf_dev, h->st);
+  }
   CK(cudaGetLastError());
   return FELIS_OK;
 }
@@ -1001,8 +1058,12 @@ static felis_status step_impl(felis_handle* h, int it) {
   // diagnostics of this iteration (state before the step)
   if (!(h->diag_valid && h->diag_iter == it)) {
     if (rec) {
-      launch_energy(h->G, h->U, h->ring_base, h->d_planes2, h->st);
-      launch_sum_planes(h->d_planes2, H, h->p.slice_n, 0, h->d_hist_e + (size_t)it * 2 * H, h->st);
+      {
+        KernelScope ks(h, FELIS_KERNEL_REDUCE);
+        launch_energy(h->G, h->U, h->ring_base, h->d_planes2, h->st);
+        launch_sum_planes(h->d_planes2, H, h->p.slice_n, 0, h->d_hist_e + (size_t)it * 2 * H, h->st);
+        h->launches[FELIS_KERNEL_REDUCE] += 1;
+      }
       felis_status s = diag_now(h, h->d_hist_t + (size_t)it * 6 * ns, h->d_hist_b + (size_t)it * 2 * H);
       if (s != FELIS_OK) return s;
     }
@@ -1028,9 +1089,13 @@ static felis_status step_impl(felis_handle* h, int it) {
   }
   // diagnostics of the next iteration from the fused partials and the ADI planes
   if (it + 1 < h->hist_n) {
-    launch_diag_finalize(h->d_part, (int)h->tiles.size(), h->diag_stride, ns, H, h->d_tiles,
-                         h->d_hist_t + (size_t)(it + 1) * 6 * ns, h->d_hist_b + (size_t)(it + 1) * 2 * H, h->st);
-    launch_sum_planes(h->d_planes, H, h->p.slice_n, shift ? 1 : 0, h->d_hist_e + (size_t)(it + 1) * 2 * H, h->st);
+    {
+      KernelScope ks(h, FELIS_KERNEL_REDUCE);
+      launch_diag_finalize(h->d_part, (int)h->tiles.size(), h->diag_stride, ns, H, h->d_tiles, h->d_l1, h->l1_blocks,
+                           h->d_hist_t + (size_t)(it + 1) * 6 * ns, h->d_hist_b + (size_t)(it + 1) * 2 * H, h->st);
+      launch_sum_planes(h->d_planes, H, h->p.slice_n, shift ? 1 : 0, h->d_hist_e + (size_t)(it + 1) * 2 * H, h->st);
+      h->launches[FELIS_KERNEL_REDUCE] += 1;
+    }
     CK(cudaGetLastError());
     h->diag_valid = true;
     h->diag_iter = it + 1;
@@ -1066,8 +1131,20 @@ felis_status felis_run(felis_handle* h, int32_t it0, int32_t it1) {
   }
   if (ce != cudaSuccess) return fail(h, FELIS_CUDA_ERROR, std::string("graph capture: ") + cudaGetErrorString(ce));
   ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e0, h->st);
   if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, h->st);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e1, h->st);
   if (ce == cudaSuccess) ce = cudaStreamSynchronize(h->st);
+  if (ce == cudaSuccess) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    h->last_run_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
   if (exec) cudaGraphExecDestroy(exec);
   cudaGraphDestroy(graph);
   if (ce != cudaSuccess) return fail(h, FELIS_CUDA_ERROR, std::string("graph run: ") + cudaGetErrorString(ce));
@@ -1090,6 +1167,50 @@ felis_status felis_edge_deposit_count(felis_handle* h, int64_t* count) {
   felis_status s = check_err(h);
   *count = h->edge_total;
   return s;
+}
+
+felis_status felis_sync(felis_handle* h) {
+  if (!h) return FELIS_BAD_ARG;
+  return check_err(h);
+}
+
+felis_status felis_profile(felis_handle* h, int32_t enable, int32_t max_launches) {
+  if (!h || max_launches < 0) return FELIS_BAD_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  h->prof = enable != 0;
+  h->marks.clear();
+  h->ev_used = 0;
+  for (int k = 0; k < FELIS_KERNEL_KINDS; ++k) h->launches[k] = 0;
+  const size_t want = 2 * (size_t)max_launches;
+  while (h->prof && h->ev.size() < want) {
+    cudaEvent_t e;
+    CK(cudaEventCreate(&e));
+    h->ev.push_back(e);
+  }
+  return FELIS_OK;
+}
+
+felis_status felis_kernel_stats(felis_handle* h, int32_t kind, int64_t* launches, double* total_ms) {
+  if (!h || kind < -1 || kind >= FELIS_KERNEL_KINDS) return FELIS_BAD_ARG;
+  CK(cudaStreamSynchronize(h->st));
+  int64_t n = 0;
+  if (kind < 0) for (int k = 0; k < FELIS_KERNEL_KINDS; ++k) n += h->launches[k];
+  else n = h->launches[kind];
+  double ms = 0.0;
+  for (const auto& m : h->marks) {
+    if (kind >= 0 && m.first != kind) continue;
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, h->ev[m.second], h->ev[m.second + 1]) == cudaSuccess) ms += t;
+  }
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
+  return FELIS_OK;
+}
+
+felis_status felis_last_run_ms(felis_handle* h, double* ms) {
+  if (!h || !ms) return FELIS_BAD_ARG;
+  *ms = h->last_run_ms;
+  return FELIS_OK;
 }
 
 void felis_detmath_sincos(double x, double* s, double* c) { fm::sincos(x, s, c); }

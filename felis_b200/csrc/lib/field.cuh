@@ -45,12 +45,13 @@ struct DepositLaunch {
   double2 fconst[FELIS_MAX_HARMONY][2];  // odd-harmonic fx, fy (per call constants)
   cd etaX, etaY;
   double A;             // Ez Thomas coefficient (solveField.cpp:320)
-  int cap, qbits;       // particles per slice the shared-memory sort holds
+  int cap;              // particles per chunk (power of two) staged in shared memory
+  int neven;            // number of even harmonics
   int* err;
 };
 
 void launch_deposit(const DepositLaunch& a, cudaStream_t st);
-size_t deposit_smem_bytes(int cap, int L, int F, int nr);
+size_t deposit_smem_bytes(int chunk, int H, int neven, int L, int F, int nr);
 void deposit_set_smem(size_t bytes);
 void adi_set_smem(size_t bytes);
 void launch_adi(const AdiLaunch& a, cudaStream_t st);

@@ -72,185 +72,276 @@ __device__ __forceinline__ int64_t q_to_n(const DepositLaunch& a, int s, uint32_
   return -1;
 }
 
+// Shared-memory layout of one deposit CTA (chunk of C particles):
+//   keys[C] u32 | wx1[C] | wy1[C] | coef[H][C] double2 | fx,fy[neven][C] |
+//   radial bins d[L*F*nr] double2 | modified diagonal [L*F*nr] double
+// The radial pass reuses the 2-D record area for {wr1[C], ez[L*F][C]}.
+struct DepLayout {
+  int C, qb;
+  size_t keys, wx, wy, coef, fx, fy, wr, ez, bins, bmod, total;
+};
+
+__host__ __device__ inline DepLayout dep_layout(int C, int H, int neven, int LF, int nr) {
+  DepLayout L;
+  L.C = C;
+  int qb = 0;
+  while ((1 << qb) < C) ++qb;
+  L.qb = qb;
+  size_t o = 0;
+  auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~(size_t)15; return r; };
+  L.keys = take((size_t)C * 4);
+  const size_t rec0 = o;
+  L.wx = take((size_t)C * 8);
+  L.wy = take((size_t)C * 8);
+  L.coef = take((size_t)C * 16 * H);
+  L.fx = take((size_t)C * 16 * neven);
+  L.fy = take((size_t)C * 16 * neven);
+  const size_t rec2d_end = o;
+  o = rec0;
+  L.wr = take((size_t)C * 8);
+  L.ez = take((size_t)C * 16 * LF);
+  if (o < rec2d_end) o = rec2d_end;
+  L.bins = take((size_t)LF * nr * 16);
+  L.bmod = take((size_t)LF * nr * 8);
+  L.total = o;
+  return L;
+}
+
 __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
   extern __shared__ __align__(16) unsigned char dsm[];
-  uint32_t* keys = reinterpret_cast<uint32_t*>(dsm);
   __shared__ int red_i[4][16];
+  __shared__ int sbox[4];
   const DevGeom& G = a.G;
   const int s = blockIdx.x;
-  const int S = G.S, nx = G.nx, ny = G.ny, N = G.N;
-  const uint32_t qmask = (1u << a.qbits) - 1u;
-  // ---- slice particle count (all species) and capacity check ----
+  const int S = G.S, nx = G.nx, ny = G.ny, N = G.N, H = G.H;
+  const int nr = G.nr, LFn = G.L * G.F;
+  const DepLayout Ly = dep_layout(a.cap, H, a.neven, LFn, nr);
+  const int CH = Ly.C, qb = Ly.qb;
+  const uint32_t qmask = (1u << qb) - 1u;
+  uint32_t* keys = reinterpret_cast<uint32_t*>(dsm + Ly.keys);
+  double* rwx = reinterpret_cast<double*>(dsm + Ly.wx);
+  double* rwy = reinterpret_cast<double*>(dsm + Ly.wy);
+  double2* rcoef = reinterpret_cast<double2*>(dsm + Ly.coef);
+  double2* rfx = reinterpret_cast<double2*>(dsm + Ly.fx);
+  double2* rfy = reinterpret_cast<double2*>(dsm + Ly.fy);
+  double* rwr = reinterpret_cast<double*>(dsm + Ly.wr);
+  double2* rez = reinterpret_cast<double2*>(dsm + Ly.ez);
+  double2* dbin = reinterpret_cast<double2*>(dsm + Ly.bins);
+  double* bmod = reinterpret_cast<double*>(dsm + Ly.bmod);
+  const size_t tot = (size_t)a.total;
+  // ---- slice particle count (all species) ----
   int64_t Pt = 0, Plast0 = 0, Plast = 0;
   for (int sp = 0; sp < G.nspecies; ++sp) {
     const int64_t b = a.soff[(size_t)sp * (S + 1) + s], e = a.soff[(size_t)sp * (S + 1) + s + 1];
     if (sp == G.nspecies - 1) { Plast0 = Pt; Plast = e - b; }
     Pt += e - b;
   }
-  if (Pt > a.cap) {
-    if (threadIdx.x == 0) {
-      set_flag(a.err, ERR_DEPOSIT_CAPACITY);
-      a.box[s] = make_int4(1, 0, 1, 0);
-    }
-    return;
-  }
-  int n2 = 1;
-  while (n2 < Pt) n2 <<= 1;
-  // ---- phase A: 2-D source ----
-  int cmin_i = 1 << 30, cmax_i = -1, cmin_j = 1 << 30, cmax_j = -1;
-  for (int q = threadIdx.x; q < n2; q += blockDim.x) {
-    uint32_t v = 0xFFFFFFFFu;
-    if (q < Pt) {
-      const int64_t n = q_to_n(a, s, (uint32_t)q);
-      const int k = a.dep.key[n];
+  // ---- box of occupied 2-D cells over the whole slice ----
+  {
+    int cmin_i = 1 << 30, cmax_i = -1, cmin_j = 1 << 30, cmax_j = -1;
+    for (int64_t q = threadIdx.x; q < Pt; q += blockDim.x) {
+      const int k = a.dep.key[q_to_n(a, s, (uint32_t)q)];
       if (k >= 0) {
-        v = ((uint32_t)k << a.qbits) | (uint32_t)q;
         const int ki = k % nx, kj = k / nx;
         cmin_i = min(cmin_i, ki); cmax_i = max(cmax_i, ki);
         cmin_j = min(cmin_j, kj); cmax_j = max(cmax_j, kj);
       }
     }
-    keys[q] = v;
-  }
-  // block min/max of the occupied cells
-  for (int o = 16; o > 0; o >>= 1) {
-    cmin_i = min(cmin_i, __shfl_down_sync(0xffffffffu, cmin_i, o));
-    cmax_i = max(cmax_i, __shfl_down_sync(0xffffffffu, cmax_i, o));
-    cmin_j = min(cmin_j, __shfl_down_sync(0xffffffffu, cmin_j, o));
-    cmax_j = max(cmax_j, __shfl_down_sync(0xffffffffu, cmax_j, o));
-  }
-  if ((threadIdx.x & 31) == 0) {
-    const int w = threadIdx.x >> 5;
-    red_i[0][w] = cmin_i; red_i[1][w] = cmax_i; red_i[2][w] = cmin_j; red_i[3][w] = cmax_j;
-  }
-  __syncthreads();
-  bitonic_sort(keys, n2);
-  int i0 = 1 << 30, i1 = -1, j0 = 1 << 30, j1 = -1;
-  for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
-    i0 = min(i0, red_i[0][w]); i1 = max(i1, red_i[1][w]);
-    j0 = min(j0, red_i[2][w]); j1 = max(j1, red_i[3][w]);
-  }
-  // valid entries precede the 0xFFFFFFFF padding
-  const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
-  // targets: interior cells a key can reach
-  const int ti0 = max(1, i0), ti1 = min(nx - 2, i1 + 1);
-  const int tj0 = max(1, j0), tj1 = min(ny - 2, j1 + 1);
-  if (threadIdx.x == 0) a.box[s] = (V > 0 && ti0 <= ti1 && tj0 <= tj1) ? make_int4(ti0, ti1, tj0, tj1) : make_int4(1, 0, 1, 0);
-  if (V > 0 && ti0 <= ti1 && tj0 <= tj1) {
-    const int bw = ti1 - ti0 + 1, bh = tj1 - tj0 + 1;
-    const size_t tot = (size_t)a.total;
-    for (int c = threadIdx.x; c < bw * bh; c += blockDim.x) {
-      const int ti = ti0 + c % bw, tj = tj0 + c / bw;
-      const int t = tj * nx + ti;
-      // source buckets: corner (ii, jj) of key t - jj*nx - ii
-      int lo[4], hi[4];
-#pragma unroll
-      for (int cb = 0; cb < 4; ++cb) {
-        const int ii = cb & 1, jj = cb >> 1;
-        const int k = t - jj * nx - ii;
-        lo[cb] = lower_bound_u32(keys, V, (uint32_t)k << a.qbits);
-        hi[cb] = lower_bound_u32(keys, V, (uint32_t)(k + 1) << a.qbits);
+    for (int o = 16; o > 0; o >>= 1) {
+      cmin_i = min(cmin_i, __shfl_down_sync(0xffffffffu, cmin_i, o));
+      cmax_i = max(cmax_i, __shfl_down_sync(0xffffffffu, cmax_i, o));
+      cmin_j = min(cmin_j, __shfl_down_sync(0xffffffffu, cmin_j, o));
+      cmax_j = max(cmax_j, __shfl_down_sync(0xffffffffu, cmax_j, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+      const int w = threadIdx.x >> 5;
+      red_i[0][w] = cmin_i; red_i[1][w] = cmax_i; red_i[2][w] = cmin_j; red_i[3][w] = cmax_j;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int i0 = 1 << 30, i1 = -1, j0 = 1 << 30, j1 = -1;
+      for (int w = 0; w < (int)(blockDim.x >> 5); ++w) {
+        i0 = min(i0, red_i[0][w]); i1 = max(i1, red_i[1][w]);
+        j0 = min(j0, red_i[2][w]); j1 = max(j1, red_i[3][w]);
       }
-      cd accx[FELIS_MAX_HARMONY], accy[FELIS_MAX_HARMONY];
-      for (int h = 0; h < G.H; ++h) { accx[h] = C(0, 0); accy[h] = C(0, 0); }
-      while (true) {
-        int best = -1;
-        uint32_t bq = 0xFFFFFFFFu;
-#pragma unroll
-        for (int cb = 0; cb < 4; ++cb)
-          if (lo[cb] < hi[cb]) {
-            const uint32_t q = keys[lo[cb]] & qmask;
-            if (q < bq) { bq = q; best = cb; }
-          }
-        if (best < 0) break;
-        ++lo[best];
-        const int ii = best & 1, jj = best >> 1;
-        const int64_t n = q_to_n(a, s, bq);
-        const double wx1 = a.dep.wx1[n], wy1 = a.dep.wy1[n];
-        const double wxv = ii ? wx1 : 1.0 - wx1;
-        const double wyv = jj ? wy1 : 1.0 - wy1;
-        const cd ex = cscale(cscale(a.etaX, wxv), wyv);
-        const cd ey = cscale(cscale(a.etaY, wxv), wyv);
-        for (int h = 0; h < G.H; ++h) {
-          const double2 mc2 = a.dep.coef[(size_t)h * tot + n];
-          const cd mc = C(mc2.x, mc2.y);
-          cd fx, fy;
-          if (G.harmony[h] % 2 == 1) {
-            fx = C(a.fconst[h][0].x, a.fconst[h][0].y);
-            fy = C(a.fconst[h][1].x, a.fconst[h][1].y);
-          } else {
-            const double2 v1 = a.dep.fx[(size_t)h * tot + n], v2 = a.dep.fy[(size_t)h * tot + n];
-            fx = C(v1.x, v1.y);
-            fy = C(v2.x, v2.y);
-          }
-          accx[h] = csub(accx[h], cmul(cmul(ex, fx), mc));
-          accy[h] = csub(accy[h], cmul(cmul(ey, fy), mc));
+      // interior cells a key can reach
+      const int ti0 = max(1, i0), ti1 = min(nx - 2, i1 + 1), tj0 = max(1, j0), tj1 = min(ny - 2, j1 + 1);
+      const bool any = i1 >= 0 && ti0 <= ti1 && tj0 <= tj1;
+      sbox[0] = any ? ti0 : 1; sbox[1] = any ? ti1 : 0; sbox[2] = any ? tj0 : 1; sbox[3] = any ? tj1 : 0;
+      a.box[s] = make_int4(sbox[0], sbox[1], sbox[2], sbox[3]);
+    }
+    __syncthreads();
+  }
+  const int bi0 = sbox[0], bi1 = sbox[1], bj0 = sbox[2], bj1 = sbox[3];
+  const int bw = bi1 - bi0 + 1, bh = bj1 - bj0 + 1;
+  // zero the box: cells no particle reaches stay exactly zero
+  if (bw > 0 && bh > 0)
+    for (int c = threadIdx.x; c < bw * bh; c += blockDim.x) {
+      const int t = (bj0 + c / bw) * nx + bi0 + c % bw;
+      for (int h = 0; h < H; ++h) {
+        a.Sc[(((size_t)h * 2 + 0) * S + s) * N + t] = make_double2(0.0, 0.0);
+        a.Sc[(((size_t)h * 2 + 1) * S + s) * N + t] = make_double2(0.0, 0.0);
+      }
+    }
+  __syncthreads();
+  // ---- phase A: 2-D source, chunk by chunk in particle order ----
+  for (int64_t c0 = 0; c0 < Pt && bw > 0 && bh > 0; c0 += CH) {
+    const int nc = (int)((Pt - c0) < CH ? (Pt - c0) : CH);
+    int n2 = 1;
+    while (n2 < nc) n2 <<= 1;
+    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+      uint32_t v = 0xFFFFFFFFu;
+      if (q < nc) {
+        const int k = a.dep.key[q_to_n(a, s, (uint32_t)(c0 + q))];
+        if (k >= 0) v = ((uint32_t)k << qb) | (uint32_t)q;
+      }
+      keys[q] = v;
+    }
+    __syncthreads();
+    bitonic_sort(keys, n2);
+    const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
+    // records of the chunk, in sorted order
+    for (int pos = threadIdx.x; pos < V; pos += blockDim.x) {
+      const int64_t n = q_to_n(a, s, (uint32_t)(c0 + (keys[pos] & qmask)));
+      rwx[pos] = a.dep.wx1[n];
+      rwy[pos] = a.dep.wy1[n];
+      int e = 0;
+      for (int h = 0; h < H; ++h) {
+        rcoef[(size_t)h * CH + pos] = a.dep.coef[(size_t)h * tot + n];
+        if (G.harmony[h] % 2 == 0) {
+          rfx[(size_t)e * CH + pos] = a.dep.fx[(size_t)h * tot + n];
+          rfy[(size_t)e * CH + pos] = a.dep.fy[(size_t)h * tot + n];
+          ++e;
         }
       }
-      for (int h = 0; h < G.H; ++h) {
-        a.Sc[(((size_t)h * 2 + 0) * S + s) * N + t] = make_double2(accx[h].re, accx[h].im);
-        a.Sc[(((size_t)h * 2 + 1) * S + s) * N + t] = make_double2(accy[h].re, accy[h].im);
+    }
+    __syncthreads();
+    if (V > 0) {
+      // the chunk's own reach (sorted keys give the row range directly)
+      const int kfirst = (int)(keys[0] >> qb), klast = (int)(keys[V - 1] >> qb);
+      const int rj0 = max(bj0, kfirst / nx), rj1 = min(bj1, klast / nx + 1);
+      const int rh = rj1 - rj0 + 1;
+      for (int c = threadIdx.x; c < bw * max(rh, 0); c += blockDim.x) {
+        const int ti = bi0 + c % bw, tj = rj0 + c / bw;
+        const int t = tj * nx + ti;
+        int lo[4], hi[4];
+        bool any = false;
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+          const int k = t - (cb >> 1) * nx - (cb & 1);
+          lo[cb] = lower_bound_u32(keys, V, (uint32_t)k << qb);
+          hi[cb] = lower_bound_u32(keys, V, (uint32_t)(k + 1) << qb);
+          any |= lo[cb] < hi[cb];
+        }
+        if (!any) continue;
+        cd accx[FELIS_MAX_HARMONY], accy[FELIS_MAX_HARMONY];
+        for (int h = 0; h < H; ++h) {
+          const double2 vx = a.Sc[(((size_t)h * 2 + 0) * S + s) * N + t];
+          const double2 vy = a.Sc[(((size_t)h * 2 + 1) * S + s) * N + t];
+          accx[h] = C(vx.x, vx.y);
+          accy[h] = C(vy.x, vy.y);
+        }
+        while (true) {
+          int best = -1;
+          uint32_t bq = 0xFFFFFFFFu;
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb)
+            if (lo[cb] < hi[cb]) {
+              const uint32_t q = keys[lo[cb]] & qmask;
+              if (q < bq) { bq = q; best = cb; }
+            }
+          if (best < 0) break;
+          const int pos = lo[best]++;
+          const int ii = best & 1, jj = best >> 1;
+          const double wx1 = rwx[pos], wy1 = rwy[pos];
+          const double wxv = ii ? wx1 : 1.0 - wx1;
+          const double wyv = jj ? wy1 : 1.0 - wy1;
+          const cd ex = cscale(cscale(a.etaX, wxv), wyv);
+          const cd ey = cscale(cscale(a.etaY, wxv), wyv);
+          int e = 0;
+          for (int h = 0; h < H; ++h) {
+            const double2 m = rcoef[(size_t)h * CH + pos];
+            const cd mc = C(m.x, m.y);
+            cd fx, fy;
+            if (G.harmony[h] % 2 == 1) {
+              fx = C(a.fconst[h][0].x, a.fconst[h][0].y);
+              fy = C(a.fconst[h][1].x, a.fconst[h][1].y);
+            } else {
+              const double2 v1 = rfx[(size_t)e * CH + pos], v2 = rfy[(size_t)e * CH + pos];
+              fx = C(v1.x, v1.y);
+              fy = C(v2.x, v2.y);
+              ++e;
+            }
+            accx[h] = csub(accx[h], cmul(cmul(ex, fx), mc));
+            accy[h] = csub(accy[h], cmul(cmul(ey, fy), mc));
+          }
+        }
+        for (int h = 0; h < H; ++h) {
+          a.Sc[(((size_t)h * 2 + 0) * S + s) * N + t] = make_double2(accx[h].re, accx[h].im);
+          a.Sc[(((size_t)h * 2 + 1) * S + s) * N + t] = make_double2(accy[h].re, accy[h].im);
+        }
       }
     }
+    __syncthreads();
   }
-  __syncthreads();
   // ---- phase B: Ez of the last species (solveField.cpp:315-399) ----
-  const int nr = G.nr, L = G.L, F = G.F;
-  int m2 = 1;
-  while (m2 < Plast) m2 <<= 1;
-  for (int q = threadIdx.x; q < m2; q += blockDim.x) {
-    uint32_t v = 0xFFFFFFFFu;
-    if (q < Plast) {
-      const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + q));
-      const int rk = a.dep.rkey[n];
-      if (rk >= 0) v = ((uint32_t)rk << a.qbits) | (uint32_t)q;
-    }
-    keys[q] = v;
-  }
+  for (int idx = threadIdx.x; idx < LFn * nr; idx += blockDim.x) dbin[idx] = make_double2(0.0, 0.0);
   __syncthreads();
-  bitonic_sort(keys, m2);
-  const int VR = lower_bound_u32(keys, m2, 0xFFFFFFFFu);
-  const size_t tot = (size_t)a.total;
-  // d[j] = accumulated radial source of bin j (j < nr-1; bin nr-1 is not
-  // used).  dbin and the modified diagonal live after the key area.
-  double2* dbin = reinterpret_cast<double2*>(dsm + (((size_t)a.cap * sizeof(uint32_t) + 15) & ~(size_t)15));
-  double* bmod = reinterpret_cast<double*>(dbin + (size_t)L * F * nr);
-  for (int idx = threadIdx.x; idx < L * F * nr; idx += blockDim.x) {
-    const int lf = idx / nr, b = idx % nr;
-    const int f = lf % F;
-    cd acc = C(0, 0);
-    if (b < nr - 1 && !(f > 0 && b == 0)) {
-      int lo0, hi0, lo1 = 0, hi1 = 0;
-      lo0 = lower_bound_u32(keys, VR, (uint32_t)b << a.qbits);
-      hi0 = lower_bound_u32(keys, VR, (uint32_t)(b + 1) << a.qbits);
+  for (int64_t c0 = 0; c0 < Plast; c0 += CH) {
+    const int nc = (int)((Plast - c0) < CH ? (Plast - c0) : CH);
+    int n2 = 1;
+    while (n2 < nc) n2 <<= 1;
+    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
+      uint32_t v = 0xFFFFFFFFu;
+      if (q < nc) {
+        const int rk = a.dep.rkey[q_to_n(a, s, (uint32_t)(Plast0 + c0 + q))];
+        if (rk >= 0) v = ((uint32_t)rk << qb) | (uint32_t)q;
+      }
+      keys[q] = v;
+    }
+    __syncthreads();
+    bitonic_sort(keys, n2);
+    const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
+    for (int pos = threadIdx.x; pos < V; pos += blockDim.x) {
+      const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + c0 + (keys[pos] & qmask)));
+      rwr[pos] = a.dep.wr1[n];
+      for (int lf = 0; lf < LFn; ++lf) rez[(size_t)lf * CH + pos] = a.dep.ez[(size_t)lf * tot + n];
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < LFn * nr; idx += blockDim.x) {
+      const int lf = idx / nr, b = idx % nr, f = lf % G.F;
+      if (b >= nr - 1 || (f > 0 && b == 0)) continue;
+      int lo0 = lower_bound_u32(keys, V, (uint32_t)b << qb);
+      const int hi0 = lower_bound_u32(keys, V, (uint32_t)(b + 1) << qb);
+      int lo1 = 0, hi1 = 0;
       if (b >= 2) {
-        lo1 = lower_bound_u32(keys, VR, (uint32_t)(b - 1) << a.qbits);
+        lo1 = lower_bound_u32(keys, V, (uint32_t)(b - 1) << qb);
         hi1 = lo0;
       }
+      if (lo0 >= hi0 && lo1 >= hi1) continue;
+      const double2 a0 = dbin[idx];
+      cd acc = C(a0.x, a0.y);
       while (lo0 < hi0 || lo1 < hi1) {
         const uint32_t q0 = lo0 < hi0 ? (keys[lo0] & qmask) : 0xFFFFFFFFu;
         const uint32_t q1 = lo1 < hi1 ? (keys[lo1] & qmask) : 0xFFFFFFFFu;
         const bool take0 = q0 < q1;
-        const uint32_t q = take0 ? q0 : q1;
-        if (take0) ++lo0; else ++lo1;
-        const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + q));
-        const double2 v = a.dep.ez[(size_t)lf * tot + n];
+        const int pos = take0 ? lo0++ : lo1++;
+        const double2 v = rez[(size_t)lf * CH + pos];
         const cd cc = C(v.x, v.y);
         if (b == 0) {
           acc = cadd(acc, cc);  // idxR == 0 branch: no radial weight
         } else {
-          const double wr1 = a.dep.wr1[n];
-          const double wr = take0 ? 1.0 - wr1 : wr1;
-          acc = cadd(acc, cscale(cc, wr));
+          const double wr1 = rwr[pos];
+          acc = cadd(acc, cscale(cc, take0 ? 1.0 - wr1 : wr1));
         }
       }
+      dbin[idx] = make_double2(acc.re, acc.im);
     }
-    dbin[idx] = make_double2(acc.re, acc.im);
+    __syncthreads();
   }
-  __syncthreads();
   // Thomas solve in r, one thread per (l, f)
-  if ((int)threadIdx.x < L * F) {
-    const int lf = threadIdx.x, l = lf / F, f = lf % F;
+  if ((int)threadIdx.x < LFn) {
+    const int lf = threadIdx.x, l = lf / G.F, f = lf % G.F;
     const double A = a.A;
     double2* d = dbin + lf * nr;
     auto acoef = [&](int j) -> double { return (j == 0) ? (f == 0 ? 1.0 : 0.0) : (j == nr - 1 ? 0.0 : j + 0.5); };
@@ -271,12 +362,12 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
       bm[j] = bj;
       bprev = bj;
     }
-    const size_t ezs = (size_t)(S + 2) * nr * F;
+    const size_t ezs = (size_t)(S + 2) * nr * G.F;
     const int sliceI = s + 1;
     for (int j = nr - 2; j >= 0; --j) {
       const cd dj = C(d[j].x, d[j].y);
       const cd r = cdivr(csub(dj, cscale(C(0.0, 0.0), acoef(j))), bm[j]);
-      a.Ez[(size_t)l * ezs + (size_t)sliceI * F * nr + (size_t)f * nr + j] = make_double2(r.re, r.im);
+      a.Ez[(size_t)l * ezs + (size_t)sliceI * G.F * nr + (size_t)f * nr + j] = make_double2(r.re, r.im);
     }
   }
 }
@@ -418,13 +509,12 @@ __global__ void __launch_bounds__(256) k_sum_planes(const double* planes, int S,
 
 }  // namespace
 
-size_t deposit_smem_bytes(int cap, int L, int F, int nr) {
-  // sort keys, then the radial bins and the modified Thomas diagonal
-  return (((size_t)cap * sizeof(uint32_t) + 15) & ~(size_t)15) + (size_t)L * F * nr * (sizeof(double2) + sizeof(double));
+size_t deposit_smem_bytes(int chunk, int H, int neven, int L, int F, int nr) {
+  return dep_layout(chunk, H, neven, L * F, nr).total;
 }
 
 void launch_deposit(const DepositLaunch& a, cudaStream_t st) {
-  const size_t smem = deposit_smem_bytes(a.cap, a.G.L, a.G.F, a.G.nr);
+  const size_t smem = deposit_smem_bytes(a.cap, a.G.H, a.neven, a.G.L, a.G.F, a.G.nr);
   k_deposit<<<a.G.S, 512, smem, st>>>(a);
 }
 

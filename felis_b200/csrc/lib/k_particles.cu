@@ -403,20 +403,47 @@ __global__ void __launch_bounds__(256) k_particles(ParticleLaunch a) {
   }
 }
 
-// Sums the per-tile partials in a fixed order and finishes twiss.cpp:177-192
-// and saveFile.cpp:166 (b / totalN).
-__global__ void __launch_bounds__(256) k_diag_finalize(const double* part, int ntiles, int stride, int nspecies,
-                                                       int H, const int4* tiles, double* twiss, double* bf) {
+// Level 1: block b sums tiles [b*per, (b+1)*per) of every quantity in a
+// fixed order: 7 twiss sums per species, then the 2H+1 bFactor sums.
+__global__ void __launch_bounds__(256) k_diag_level1(const double* part, int ntiles, int stride, int nspecies,
+                                                     int H, const int4* tiles, int per, double* out) {
   __shared__ double red[8];
-  for (int sp = 0; sp < nspecies; ++sp) {
-    double acc[7];
+  const int t0 = blockIdx.x * per, t1 = min(ntiles, t0 + per);
+  const int nq = 7 * nspecies + 2 * H + 1;
+  double* o = out + (size_t)blockIdx.x * nq;
+  for (int sp = 0; sp < nspecies; ++sp)
     for (int k = 0; k < 7; ++k) {
       double v = 0.0;
-      for (int t = threadIdx.x; t < ntiles; t += blockDim.x)
+      for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x)
         if (tiles[t].x == sp) v += part[(size_t)t * stride + k];
-      acc[k] = block_sum(v, red);
+      const double r = block_sum(v, red);
+      if (threadIdx.x == 0) o[7 * sp + k] = r;
     }
-    if (threadIdx.x == 0) {
+  for (int k = 0; k < 2 * H + 1; ++k) {
+    double v = 0.0;
+    for (int t = t0 + threadIdx.x; t < t1; t += blockDim.x) v += part[(size_t)t * stride + 7 + k];
+    const double r = block_sum(v, red);
+    if (threadIdx.x == 0) o[7 * nspecies + k] = r;
+  }
+}
+
+// Level 2: one block adds the level-1 rows in order and finishes
+// twiss.cpp:177-192 and saveFile.cpp:166 (b / totalN).
+__global__ void __launch_bounds__(256) k_diag_level2(const double* l1, int nblocks, int nspecies, int H,
+                                                     double* twiss, double* bf) {
+  __shared__ double red[8];
+  const int nq = 7 * nspecies + 2 * H + 1;
+  __shared__ double tot[7 * FELIS_MAX_SPECIES + 2 * FELIS_MAX_HARMONY + 1];
+  for (int k = 0; k < nq; ++k) {
+    double v = 0.0;
+    for (int b = threadIdx.x; b < nblocks; b += blockDim.x) v += l1[(size_t)b * nq + k];
+    const double r = block_sum(v, red);
+    if (threadIdx.x == 0) tot[k] = r;
+  }
+  __syncthreads();
+  if (threadIdx.x == 0) {
+    for (int sp = 0; sp < nspecies; ++sp) {
+      const double* acc = tot + 7 * sp;
       double* o = twiss + 6 * sp;
       for (int k = 0; k < 6; ++k) o[k] = 0.0;
       const double cnt = acc[6];
@@ -429,18 +456,8 @@ __global__ void __launch_bounds__(256) k_diag_finalize(const double* part, int n
         o[3] = ey; o[4] = avgY2 / ey; o[5] = -avgCY / ey;
       }
     }
-  }
-  double wsum = 0.0;
-  {
-    double v = 0.0;
-    for (int t = threadIdx.x; t < ntiles; t += blockDim.x) v += part[(size_t)t * stride + 7 + 2 * H];
-    wsum = block_sum(v, red);
-  }
-  for (int k = 0; k < 2 * H; ++k) {
-    double v = 0.0;
-    for (int t = threadIdx.x; t < ntiles; t += blockDim.x) v += part[(size_t)t * stride + 7 + k];
-    const double tot = block_sum(v, red);
-    if (threadIdx.x == 0) bf[k] = tot / wsum;
+    const double wsum = tot[7 * nspecies + 2 * H];
+    for (int k = 0; k < 2 * H; ++k) bf[k] = tot[7 * nspecies + k] / wsum;
   }
 }
 
@@ -452,8 +469,10 @@ void launch_particles(const ParticleLaunch& a, cudaStream_t st) {
 }
 
 void launch_diag_finalize(const double* partials, int ntiles, int stride, int nspecies, int H, const int4* tiles,
-                          double* out_twiss, double* out_bf, cudaStream_t st) {
-  k_diag_finalize<<<1, 256, 0, st>>>(partials, ntiles, stride, nspecies, H, tiles, out_twiss, out_bf);
+                          double* l1, int l1_blocks, double* out_twiss, double* out_bf, cudaStream_t st) {
+  const int per = (ntiles + l1_blocks - 1) / l1_blocks;
+  k_diag_level1<<<l1_blocks, 256, 0, st>>>(partials, ntiles, stride, nspecies, H, tiles, per, l1);
+  k_diag_level2<<<1, 256, 0, st>>>(l1, l1_blocks, nspecies, H, out_twiss, out_bf);
 }
 
 }  // namespace felis

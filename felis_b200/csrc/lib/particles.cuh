@@ -55,7 +55,10 @@ struct ParticleLaunch {
 };
 
 void launch_particles(const ParticleLaunch& a, cudaStream_t st);
+// Deterministic two-level reduction of the per-tile partial sums; l1 holds
+// l1_blocks * (7*nspecies + 2H + 1) doubles.
 void launch_diag_finalize(const double* partials, int ntiles, int stride, int nspecies, int H,
-                          const int4* tiles, double* out_twiss, double* out_bf, cudaStream_t st);
+                          const int4* tiles, double* l1, int l1_blocks, double* out_twiss, double* out_bf,
+                          cudaStream_t st);
 
 }  // namespace felis

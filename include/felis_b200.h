@@ -211,6 +211,29 @@ felis_status felis_get_diagnostics(felis_handle* h, int32_t it0, int32_t it1,
  * ny-1 accepted by solveField.cpp:273), accumulated since creation. */
 felis_status felis_edge_deposit_count(felis_handle* h, int64_t* count);
 
+/* ---- measurement ------------------------------------------------------ */
+/* Waits for the handle's stream and reports a device error raised since the
+ * last check (felis_step and felis_run return device errors the same way). */
+felis_status felis_sync(felis_handle* h);
+/* Kernel kinds counted / timed by felis_kernel_stats. */
+enum {
+  FELIS_KERNEL_PARTICLES = 0, /* push / drift / wrap / deposit records / beam partial sums */
+  FELIS_KERNEL_DEPOSIT = 1,   /* ordered source deposit + Ez solve */
+  FELIS_KERNEL_ADI = 2,       /* ADI sweeps of every plane */
+  FELIS_KERNEL_REDUCE = 3,    /* power, twiss and bFactor reductions */
+  FELIS_KERNEL_SHIFT = 4,     /* slippage shift (clears one plane per harmonic and pol) */
+  FELIS_KERNEL_KINDS = 8
+};
+/* Resets the launch counters; with enable != 0, brackets each of the next
+ * max_launches kernel launches with CUDA events on the handle's stream
+ * (recorded into the graph by felis_run). */
+felis_status felis_profile(felis_handle* h, int32_t enable, int32_t max_launches);
+/* Launches of one kind (kind -1: all kinds) since felis_profile, and the sum
+ * of their event-timed durations in milliseconds. */
+felis_status felis_kernel_stats(felis_handle* h, int32_t kind, int64_t* launches, double* total_ms);
+/* Device time of the last felis_run graph launch (CUDA events around it). */
+felis_status felis_last_run_ms(felis_handle* h, double* ms);
+
 /* ---- slice sort (the slice binning of restoreParticleHDF.cpp:166-214 and
  * the slice-major write order of saveParticleHDF.cpp:95-109) -------------
  * Stable sort of n particles by integer slice key on the GPU: perm[k] is the

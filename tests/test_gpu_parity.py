@@ -173,3 +173,22 @@ def test_slice_sort_stable(fb):
     # already slice-major input (the reference's order) is the identity
     keys = np.repeat(np.arange(300, dtype=np.int32), 97)
     assert_bits(fb.sort_by_slice(keys), np.arange(keys.size), "identity")
+
+
+@pytest.mark.parametrize("kw", [
+    dict(kind="static", beamlets=2048, nx=61, total_length=2.0),
+    dict(kind="sase", slices=3, beamlets=1536, nx=51, total_length=1.0, harmonics=(1, 2, 3),
+         undulator="QuadPolar", polarity=0.5, seed_power=5e6),
+])
+def test_multichunk_deposit_bit_exact(fb, oracle_mod, tmp_path, kw):
+    """Slices larger than one shared-memory chunk of the ordered deposit."""
+    kind = kw.pop("kind")
+    cfg, beam, fields = make_case(fb, tmp_path, kind=kind, **kw)
+    H = cfg.params.num_harmony
+    n = cfg.params.max_step
+    g, o = load_both(fb, oracle_mod, cfg, beam, fields)
+    g.run(0, n)
+    o.run(0, n)
+    _particles_equal(g, o, "multichunk")
+    _fields_equal(g, o, H, "multichunk")
+    assert_bits(g.download_ez()[:, 1:-1], o.get_ez()[:, 1:-1], "multichunk Ez")
