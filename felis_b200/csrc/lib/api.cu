@@ -71,7 +71,7 @@ struct felis_handle {
   DevDeposit dep{};
   int64_t dep_cap = 0;
   bool has_even = false;
-  int dep_pcap = 0, dep_qbits = 0;
+  int dep_pcap = 0;
   // field
   double2* U = nullptr;
   double2* Sc = nullptr;
@@ -567,24 +567,25 @@ felis_status relayout(felis_handle* h, const std::vector<int64_t>& new_counts_pe
     CK(cudaMalloc(&h->dep.ez, n * LF * sizeof(double2)));
     h->dep_cap = n;
   }
-  // deposit chunk: the largest power of two (<= 4096) whose sorted keys and
-  // particle records fit in ~100 KB of shared memory (two CTAs per SM)
-  int neven = 0;
-  for (int k = 0; k < h->p.num_harmony; ++k) neven += (h->p.harmony[k] % 2 == 0);
+  // deposit chunk: the largest power of two (<= 4096 particles) whose sort
+  // buffers and records fit in ~100 KB of shared memory (two CTAs per SM)
   int dev_smem = 0;
   cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
   const size_t budget = std::min<size_t>(100 * 1024, (size_t)dev_smem);
+  const int H = h->p.num_harmony, Lm = h->p.scl_mode, Fm = h->p.scf_mode, nr = h->p.nr;
+  int neven = 0;
+  for (int k = 0; k < H; ++k) neven += (h->p.harmony[k] % 2 == 0);
   int cap = 4096;
-  while (cap > 64 && deposit_smem_bytes(cap, h->p.num_harmony, neven, h->p.scl_mode, h->p.scf_mode, h->p.nr) > budget) cap >>= 1;
-  const size_t smem = deposit_smem_bytes(cap, h->p.num_harmony, neven, h->p.scl_mode, h->p.scf_mode, h->p.nr);
-  if ((int)smem > dev_smem) return fail(h, FELIS_UNSUPPORTED, "deposit records do not fit in shared memory");
-  int qbits = 0;
-  while ((1 << qbits) < cap) ++qbits;
-  const int64_t N = (int64_t)h->p.nx * h->p.ny;
-  if (((N + 2) >> (32 - qbits)) != 0) return fail(h, FELIS_UNSUPPORTED, "grid too large for 32-bit deposit keys");
+  while (cap > 64 && deposit_smem_bytes(cap, H, neven, Lm, Fm, nr) > budget) cap >>= 1;
+  const size_t smem = deposit_smem_bytes(cap, H, neven, Lm, Fm, nr);
+  if ((int)smem > dev_smem) return fail(h, FELIS_UNSUPPORTED, "deposit buffers do not fit in shared memory");
+  int qb = 0;
+  while ((1 << qb) < cap) ++qb;
+  int kb = 0;
+  while ((1 << kb) < h->p.nx * h->p.ny + 1) ++kb;
+  if (kb + qb > 32) return fail(h, FELIS_UNSUPPORTED, "grid too large for 32-bit deposit keys");
   deposit_set_smem(smem);
   h->dep_pcap = cap;
-  h->dep_qbits = qbits;
   (void)maxslice;
   invalidate_particles(h);
   return FELIS_OK;

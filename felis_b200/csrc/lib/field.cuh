@@ -45,7 +45,7 @@ struct DepositLaunch {
   double2 fconst[FELIS_MAX_HARMONY][2];  // odd-harmonic fx, fy (per call constants)
   cd etaX, etaY;
   double A;             // Ez Thomas coefficient (solveField.cpp:320)
-  int cap;              // particles per chunk (power of two) staged in shared memory
+  int cap;              // particles per chunk (<= 4096, the radix sort's u16 counters)
   int neven;            // number of even harmonics
   int* err;
 };

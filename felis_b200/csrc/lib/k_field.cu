@@ -34,22 +34,6 @@ __device__ __forceinline__ double block_sum(double v, double* red) {
   return t;
 }
 
-__device__ __forceinline__ void bitonic_sort(uint32_t* s, int n2) {
-  for (int k = 2; k <= n2; k <<= 1) {
-    for (int j = k >> 1; j > 0; j >>= 1) {
-      for (int i = threadIdx.x; i < n2; i += blockDim.x) {
-        const int ixj = i ^ j;
-        if (ixj > i) {
-          const uint32_t a = s[i], b = s[ixj];
-          const bool up = ((i & k) == 0);
-          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
-        }
-      }
-      __syncthreads();
-    }
-  }
-}
-
 // First index in s[0, n) with s[idx] >= v (s sorted ascending).
 __device__ __forceinline__ int lower_bound_u32(const uint32_t* s, int n, uint32_t v) {
   int lo = 0, hi = n;
@@ -72,35 +56,96 @@ __device__ __forceinline__ int64_t q_to_n(const DepositLaunch& a, int s, uint32_
   return -1;
 }
 
-// Shared-memory layout of one deposit CTA (chunk of C particles):
-//   keys[C] u32 | wx1[C] | wy1[C] | coef[H][C] double2 | fx,fy[neven][C] |
-//   radial bins d[L*F*nr] double2 | modified diagonal [L*F*nr] double
-// The radial pass reuses the 2-D record area for {wr1[C], ez[L*F][C]}.
+// Stable LSD radix sort (4-bit digits) of n <= C packed items held in a[]
+// (the key in the high bits above `qb` index bits), NT threads in a blocked
+// arrangement.  cnt[16*NT] u16 scratch; result left in a[] (b[] is the
+// ping-pong buffer).  Equal keys keep their input order.
+template <int NT>
+__device__ void block_radix_sort(uint32_t* a, uint32_t* b, int n, int qb, int nbits, uint16_t* cnt, uint32_t* wsum) {
+  const int t = threadIdx.x;
+  const int K = (n + NT - 1) / NT;
+  const int i0 = t * K, i1 = min(n, i0 + K);
+  uint32_t* src = a;
+  uint32_t* dst = b;
+  for (int shift = 0; shift < nbits; shift += 4) {
+    for (int d = 0; d < 16; ++d) cnt[d * NT + t] = 0;
+    for (int i = i0; i < i1; ++i) cnt[((src[i] >> (qb + shift)) & 15u) * NT + t] += 1;
+    __syncthreads();
+    // exclusive scan of cnt (digit-major): thread t owns entries [16t, 16t+16)
+    uint32_t run = 0;
+    uint16_t loc[16];
+#pragma unroll
+    for (int k = 0; k < 16; ++k) { loc[k] = cnt[16 * t + k]; run += loc[k]; }
+    uint32_t incl = run;
+    for (int o = 1; o < 32; o <<= 1) {
+      const uint32_t v = __shfl_up_sync(0xffffffffu, incl, o);
+      if ((t & 31) >= o) incl += v;
+    }
+    if ((t & 31) == 31) wsum[t >> 5] = incl;
+    __syncthreads();
+    if (t == 0) {
+      uint32_t acc = 0;
+      for (int w = 0; w < NT / 32; ++w) { const uint32_t v = wsum[w]; wsum[w] = acc; acc += v; }
+    }
+    __syncthreads();
+    uint32_t pre = wsum[t >> 5] + incl - run;
+#pragma unroll
+    for (int k = 0; k < 16; ++k) { const uint32_t v = loc[k]; cnt[16 * t + k] = (uint16_t)pre; pre += v; }
+    __syncthreads();
+    for (int i = i0; i < i1; ++i) {
+      const uint32_t v = src[i];
+      const int d = (int)((v >> (qb + shift)) & 15u);
+      const uint16_t pos = cnt[d * NT + t];
+      cnt[d * NT + t] = pos + 1;
+      dst[pos] = v;
+    }
+    __syncthreads();
+    uint32_t* tmp = src; src = dst; dst = tmp;
+  }
+  if (src != a) {
+    for (int i = t; i < n; i += NT) a[i] = src[i];
+    __syncthreads();
+  }
+}
+
+// Shared-memory layout of one deposit CTA (one chunk of C particles at a
+// time): sort buffers A, B (u32[C] each), digit counters u16[16*512],
+// 2-D records {wx1, wy1, coef[H], fx/fy[even H]} in sorted order, or the
+// radial chain terms double2[2C][L*F]; radial bin starts and chain starts;
+// radial accumulators and the Thomas diagonal.
 struct DepLayout {
   int C, qb;
-  size_t keys, wx, wy, coef, fx, fy, wr, ez, bins, bmod, total;
+  size_t A, B, cnt, wsum, wx, wy, coef, fx, fy, rterm, bstart, cstart, bins, bmod, total;
 };
+
+__host__ __device__ inline int ilog2_ceil(int v) {
+  int b = 0;
+  while ((1 << b) < v) ++b;
+  return b;
+}
 
 __host__ __device__ inline DepLayout dep_layout(int C, int H, int neven, int LF, int nr) {
   DepLayout L;
   L.C = C;
-  int qb = 0;
-  while ((1 << qb) < C) ++qb;
-  L.qb = qb;
+  L.qb = ilog2_ceil(C);
   size_t o = 0;
   auto take = [&](size_t bytes) { size_t r = o; o += (bytes + 15) & ~(size_t)15; return r; };
-  L.keys = take((size_t)C * 4);
-  const size_t rec0 = o;
+  L.A = take((size_t)C * 4);
+  L.B = take((size_t)C * 4);
+  L.cnt = take((size_t)16 * 512 * 2);
+  L.wsum = take(16 * 4);
+  const size_t rec = o;
   L.wx = take((size_t)C * 8);
   L.wy = take((size_t)C * 8);
   L.coef = take((size_t)C * 16 * H);
   L.fx = take((size_t)C * 16 * neven);
   L.fy = take((size_t)C * 16 * neven);
-  const size_t rec2d_end = o;
-  o = rec0;
-  L.wr = take((size_t)C * 8);
-  L.ez = take((size_t)C * 16 * LF);
-  if (o < rec2d_end) o = rec2d_end;
+  const size_t rec_end = o;
+  o = rec;
+  L.rterm = take((size_t)2 * C * 16 * LF);
+  if (o < rec_end) o = rec_end;
+  L.bstart = take((size_t)(nr + 2) * 4);
+  L.cstart = take((size_t)(nr + 2) * 4);
   L.bins = take((size_t)LF * nr * 16);
   L.bmod = take((size_t)LF * nr * 8);
   L.total = o;
@@ -118,17 +163,24 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
   const DepLayout Ly = dep_layout(a.cap, H, a.neven, LFn, nr);
   const int CH = Ly.C, qb = Ly.qb;
   const uint32_t qmask = (1u << qb) - 1u;
-  uint32_t* keys = reinterpret_cast<uint32_t*>(dsm + Ly.keys);
+  uint32_t* A = reinterpret_cast<uint32_t*>(dsm + Ly.A);
+  uint32_t* Bf = reinterpret_cast<uint32_t*>(dsm + Ly.B);
+  uint16_t* cnt = reinterpret_cast<uint16_t*>(dsm + Ly.cnt);
+  uint32_t* wsum = reinterpret_cast<uint32_t*>(dsm + Ly.wsum);
   double* rwx = reinterpret_cast<double*>(dsm + Ly.wx);
   double* rwy = reinterpret_cast<double*>(dsm + Ly.wy);
   double2* rcoef = reinterpret_cast<double2*>(dsm + Ly.coef);
   double2* rfx = reinterpret_cast<double2*>(dsm + Ly.fx);
   double2* rfy = reinterpret_cast<double2*>(dsm + Ly.fy);
-  double* rwr = reinterpret_cast<double*>(dsm + Ly.wr);
-  double2* rez = reinterpret_cast<double2*>(dsm + Ly.ez);
+  double2* rterm = reinterpret_cast<double2*>(dsm + Ly.rterm);
+  int* bstart = reinterpret_cast<int*>(dsm + Ly.bstart);
+  int* cstart = reinterpret_cast<int*>(dsm + Ly.cstart);
   double2* dbin = reinterpret_cast<double2*>(dsm + Ly.bins);
   double* bmod = reinterpret_cast<double*>(dsm + Ly.bmod);
   const size_t tot = (size_t)a.total;
+  // key bits: 2-D cells (plus one invalid value) and radial bins
+  const int kbits2 = ilog2_ceil(N + 1), kbitsr = ilog2_ceil(nr + 1);
+  const uint32_t inval2 = (1u << kbits2) - 1u, invalr = (1u << kbitsr) - 1u;
   // ---- slice particle count (all species) ----
   int64_t Pt = 0, Plast0 = 0, Plast = 0;
   for (int sp = 0; sp < G.nspecies; ++sp) {
@@ -136,7 +188,7 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
     if (sp == G.nspecies - 1) { Plast0 = Pt; Plast = e - b; }
     Pt += e - b;
   }
-  // ---- box of occupied 2-D cells over the whole slice ----
+  // ---- box of reachable interior cells over the whole slice ----
   {
     int cmin_i = 1 << 30, cmax_i = -1, cmin_j = 1 << 30, cmax_j = -1;
     for (int64_t q = threadIdx.x; q < Pt; q += blockDim.x) {
@@ -164,7 +216,6 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
         i0 = min(i0, red_i[0][w]); i1 = max(i1, red_i[1][w]);
         j0 = min(j0, red_i[2][w]); j1 = max(j1, red_i[3][w]);
       }
-      // interior cells a key can reach
       const int ti0 = max(1, i0), ti1 = min(nx - 2, i1 + 1), tj0 = max(1, j0), tj1 = min(ny - 2, j1 + 1);
       const bool any = i1 >= 0 && ti0 <= ti1 && tj0 <= tj1;
       sbox[0] = any ? ti0 : 1; sbox[1] = any ? ti1 : 0; sbox[2] = any ? tj0 : 1; sbox[3] = any ? tj1 : 0;
@@ -174,7 +225,6 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
   }
   const int bi0 = sbox[0], bi1 = sbox[1], bj0 = sbox[2], bj1 = sbox[3];
   const int bw = bi1 - bi0 + 1, bh = bj1 - bj0 + 1;
-  // zero the box: cells no particle reaches stay exactly zero
   if (bw > 0 && bh > 0)
     for (int c = threadIdx.x; c < bw * bh; c += blockDim.x) {
       const int t = (bj0 + c / bw) * nx + bi0 + c % bw;
@@ -187,22 +237,16 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
   // ---- phase A: 2-D source, chunk by chunk in particle order ----
   for (int64_t c0 = 0; c0 < Pt && bw > 0 && bh > 0; c0 += CH) {
     const int nc = (int)((Pt - c0) < CH ? (Pt - c0) : CH);
-    int n2 = 1;
-    while (n2 < nc) n2 <<= 1;
-    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
-      uint32_t v = 0xFFFFFFFFu;
-      if (q < nc) {
-        const int k = a.dep.key[q_to_n(a, s, (uint32_t)(c0 + q))];
-        if (k >= 0) v = ((uint32_t)k << qb) | (uint32_t)q;
-      }
-      keys[q] = v;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+      const int k = a.dep.key[q_to_n(a, s, (uint32_t)(c0 + q))];
+      A[q] = ((k >= 0 ? (uint32_t)k : inval2) << qb) | (uint32_t)q;
     }
     __syncthreads();
-    bitonic_sort(keys, n2);
-    const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
+    block_radix_sort<512>(A, Bf, nc, qb, kbits2, cnt, wsum);
+    const int V = lower_bound_u32(A, nc, inval2 << qb);
     // records of the chunk, in sorted order
     for (int pos = threadIdx.x; pos < V; pos += blockDim.x) {
-      const int64_t n = q_to_n(a, s, (uint32_t)(c0 + (keys[pos] & qmask)));
+      const int64_t n = q_to_n(a, s, (uint32_t)(c0 + (A[pos] & qmask)));
       rwx[pos] = a.dep.wx1[n];
       rwy[pos] = a.dep.wy1[n];
       int e = 0;
@@ -217,8 +261,7 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
     }
     __syncthreads();
     if (V > 0) {
-      // the chunk's own reach (sorted keys give the row range directly)
-      const int kfirst = (int)(keys[0] >> qb), klast = (int)(keys[V - 1] >> qb);
+      const int kfirst = (int)(A[0] >> qb), klast = (int)(A[V - 1] >> qb);
       const int rj0 = max(bj0, kfirst / nx), rj1 = min(bj1, klast / nx + 1);
       const int rh = rj1 - rj0 + 1;
       for (int c = threadIdx.x; c < bw * max(rh, 0); c += blockDim.x) {
@@ -229,8 +272,8 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
 #pragma unroll
         for (int cb = 0; cb < 4; ++cb) {
           const int k = t - (cb >> 1) * nx - (cb & 1);
-          lo[cb] = lower_bound_u32(keys, V, (uint32_t)k << qb);
-          hi[cb] = lower_bound_u32(keys, V, (uint32_t)(k + 1) << qb);
+          lo[cb] = lower_bound_u32(A, V, (uint32_t)k << qb);
+          hi[cb] = lower_bound_u32(A, V, (uint32_t)(k + 1) << qb);
           any |= lo[cb] < hi[cb];
         }
         if (!any) continue;
@@ -241,17 +284,18 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
           accx[h] = C(vx.x, vx.y);
           accy[h] = C(vy.x, vy.y);
         }
-        while (true) {
-          int best = -1;
-          uint32_t bq = 0xFFFFFFFFu;
+        uint32_t head[4];
 #pragma unroll
-          for (int cb = 0; cb < 4; ++cb)
-            if (lo[cb] < hi[cb]) {
-              const uint32_t q = keys[lo[cb]] & qmask;
-              if (q < bq) { bq = q; best = cb; }
-            }
-          if (best < 0) break;
+        for (int cb = 0; cb < 4; ++cb) head[cb] = lo[cb] < hi[cb] ? (A[lo[cb]] & qmask) : 0xFFFFFFFFu;
+        while (true) {
+          int best = 0;
+          uint32_t bq = head[0];
+#pragma unroll
+          for (int cb = 1; cb < 4; ++cb)
+            if (head[cb] < bq) { bq = head[cb]; best = cb; }
+          if (bq == 0xFFFFFFFFu) break;
           const int pos = lo[best]++;
+          head[best] = lo[best] < hi[best] ? (A[lo[best]] & qmask) : 0xFFFFFFFFu;
           const int ii = best & 1, jj = best >> 1;
           const double wx1 = rwx[pos], wy1 = rwy[pos];
           const double wxv = ii ? wx1 : 1.0 - wx1;
@@ -289,70 +333,86 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
   __syncthreads();
   for (int64_t c0 = 0; c0 < Plast; c0 += CH) {
     const int nc = (int)((Plast - c0) < CH ? (Plast - c0) : CH);
-    int n2 = 1;
-    while (n2 < nc) n2 <<= 1;
-    for (int q = threadIdx.x; q < n2; q += blockDim.x) {
-      uint32_t v = 0xFFFFFFFFu;
-      if (q < nc) {
-        const int rk = a.dep.rkey[q_to_n(a, s, (uint32_t)(Plast0 + c0 + q))];
-        if (rk >= 0) v = ((uint32_t)rk << qb) | (uint32_t)q;
-      }
-      keys[q] = v;
+    for (int q = threadIdx.x; q < nc; q += blockDim.x) {
+      const int rk = a.dep.rkey[q_to_n(a, s, (uint32_t)(Plast0 + c0 + q))];
+      A[q] = ((rk >= 0 ? (uint32_t)rk : invalr) << qb) | (uint32_t)q;
     }
     __syncthreads();
-    bitonic_sort(keys, n2);
-    const int V = lower_bound_u32(keys, n2, 0xFFFFFFFFu);
+    block_radix_sort<512>(A, Bf, nc, qb, kbitsr, cnt, wsum);
+    const int V = lower_bound_u32(A, nc, invalr << qb);
+    // bucket starts per bin (bstart[nr] = V) and chain starts: bin b's chain
+    // merges bucket b (weight wr0) and bucket b-1 (weight wr1) by particle
+    for (int b = threadIdx.x; b <= nr; b += blockDim.x) bstart[b] = lower_bound_u32(A, V, (uint32_t)b << qb);
+    __syncthreads();
+    if (threadIdx.x == 0) {
+      int acc = 0;
+      for (int b = 0; b <= nr - 2; ++b) {
+        cstart[b] = acc;
+        int len = bstart[b + 1] - bstart[b];
+        if (b >= 2) len += bstart[b] - bstart[b - 1];
+        acc += len;
+      }
+      cstart[nr - 1] = acc;
+    }
+    __syncthreads();
+    // every (particle, bin) term at its place in the bin's chain
     for (int pos = threadIdx.x; pos < V; pos += blockDim.x) {
-      const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + c0 + (keys[pos] & qmask)));
-      rwr[pos] = a.dep.wr1[n];
-      for (int lf = 0; lf < LFn; ++lf) rez[(size_t)lf * CH + pos] = a.dep.ez[(size_t)lf * tot + n];
-    }
-    __syncthreads();
-    for (int idx = threadIdx.x; idx < LFn * nr; idx += blockDim.x) {
-      const int lf = idx / nr, b = idx % nr, f = lf % G.F;
-      if (b >= nr - 1 || (f > 0 && b == 0)) continue;
-      int lo0 = lower_bound_u32(keys, V, (uint32_t)b << qb);
-      const int hi0 = lower_bound_u32(keys, V, (uint32_t)(b + 1) << qb);
-      int lo1 = 0, hi1 = 0;
-      if (b >= 2) {
-        lo1 = lower_bound_u32(keys, V, (uint32_t)(b - 1) << qb);
-        hi1 = lo0;
-      }
-      if (lo0 >= hi0 && lo1 >= hi1) continue;
-      const double2 a0 = dbin[idx];
-      cd acc = C(a0.x, a0.y);
-      while (lo0 < hi0 || lo1 < hi1) {
-        const uint32_t q0 = lo0 < hi0 ? (keys[lo0] & qmask) : 0xFFFFFFFFu;
-        const uint32_t q1 = lo1 < hi1 ? (keys[lo1] & qmask) : 0xFFFFFFFFu;
-        const bool take0 = q0 < q1;
-        const int pos = take0 ? lo0++ : lo1++;
-        const double2 v = rez[(size_t)lf * CH + pos];
-        const cd cc = C(v.x, v.y);
-        if (b == 0) {
-          acc = cadd(acc, cc);  // idxR == 0 branch: no radial weight
-        } else {
-          const double wr1 = rwr[pos];
-          acc = cadd(acc, cscale(cc, take0 ? 1.0 - wr1 : wr1));
+      const uint32_t it = A[pos];
+      const int rk = (int)(it >> qb);
+      const uint32_t q = it & qmask;
+      const int64_t n = q_to_n(a, s, (uint32_t)(Plast0 + c0 + q));
+      const double wr1 = a.dep.wr1[n];
+      const int rank = pos - bstart[rk];
+      for (int jj = 0; jj < 2; ++jj) {
+        const int b = rk + jj;
+        if (b > nr - 2 || (rk == 0 && jj == 1)) continue;
+        // the other bucket of chain b: b-1 (for jj = 0, b >= 2) or b (for jj = 1)
+        int other = 0;
+        if (jj == 0 && b >= 2) other = lower_bound_u32(A + bstart[b - 1], bstart[b] - bstart[b - 1], ((uint32_t)(b - 1) << qb) | q);
+        if (jj == 1) other = lower_bound_u32(A + bstart[b], bstart[b + 1] - bstart[b], ((uint32_t)b << qb) | q);
+        const int slot = cstart[b] + rank + other;
+        for (int lf = 0; lf < LFn; ++lf) {
+          const double2 v = a.dep.ez[(size_t)lf * tot + n];
+          double2 tt;
+          if (b == 0) tt = v;  // idxR == 0 branch: no radial weight
+          else {
+            const double w = jj ? wr1 : 1.0 - wr1;
+            tt = make_double2(v.x * w, v.y * w);
+          }
+          rterm[(size_t)slot * LFn + lf] = tt;
         }
       }
-      dbin[idx] = make_double2(acc.re, acc.im);
+    }
+    __syncthreads();
+    for (int idx = threadIdx.x; idx < LFn * (nr - 1); idx += blockDim.x) {
+      const int lf = idx / (nr - 1), b = idx % (nr - 1);
+      if (b == 0 && (lf % G.F) > 0) continue;  // bin 0 of f > 0 stays zero
+      const int k0 = cstart[b], k1 = cstart[b + 1];
+      if (k0 == k1) continue;
+      double2 acc = dbin[(size_t)lf * nr + b];
+      for (int k = k0; k < k1; ++k) {
+        const double2 tt = rterm[(size_t)k * LFn + lf];
+        acc.x = acc.x + tt.x;
+        acc.y = acc.y + tt.y;
+      }
+      dbin[(size_t)lf * nr + b] = acc;
     }
     __syncthreads();
   }
   // Thomas solve in r, one thread per (l, f)
   if ((int)threadIdx.x < LFn) {
     const int lf = threadIdx.x, l = lf / G.F, f = lf % G.F;
-    const double A = a.A;
+    const double Acoef = a.A;
     double2* d = dbin + lf * nr;
     auto acoef = [&](int j) -> double { return (j == 0) ? (f == 0 ? 1.0 : 0.0) : (j == nr - 1 ? 0.0 : j + 0.5); };
     auto ccoef = [&](int j) -> double { return (j == 0 || j == nr - 1) ? 0.0 : j - 0.5; };
     double* bm = bmod + (size_t)lf * nr;
     double bprev;
-    if (f == 0) bprev = -(1.0 + (l + 1.0) * (l + 1.0) * A / 8.0);
+    if (f == 0) bprev = -(1.0 + (l + 1.0) * (l + 1.0) * Acoef / 8.0);
     else { bprev = 1.0; d[0] = make_double2(0.0, 0.0); }
     bm[0] = bprev;
     for (int j = 1; j < nr; ++j) {
-      double bj = (j == nr - 1) ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * A * j - f * f * G.logtab[j];
+      double bj = (j == nr - 1) ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * Acoef * j - f * f * G.logtab[j];
       const double ww = ccoef(j) / bprev;
       bj -= ww * acoef(j - 1);
       cd dj = (j == nr - 1) ? C(0, 0) : C(d[j].x, d[j].y);
@@ -374,35 +434,61 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
 
 // ---- ADI -------------------------------------------------------------------
 __global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
-  extern __shared__ double2 Apl[];  // ny rows of nxp complex
+  extern __shared__ double2 Apl[];  // ny rows of nxp complex, then the recurrence tables
   __shared__ double red[8];
   const DevGeom& G = a.G;
   const int S = G.S, nx = G.nx, ny = G.ny, N = G.N, nxp = a.nxp;
   const int s = blockIdx.x % S;
   const int hp = blockIdx.x / S;  // h*2 + pol
   const int h = hp >> 1, pol = hp & 1;
-  const AdiTab T = a.tab[h];
+  const AdiTab Tg = a.tab[h];
+  // recurrence coefficients of this harmonic, read at every step: shared memory
+  cd* tx = reinterpret_cast<cd*>(Apl + (size_t)ny * nxp);   // ax_p, ax_a, ax_q, ax_cc [nx each]
+  cd* ty = tx + 4 * nx;                                     // ay_p, ay_a, ay_q, ay_cc [ny each]
+  double* dx_ = reinterpret_cast<double*>(ty + 4 * ny);     // ax_pinv, ax_qinv, ax_ccinv [nx each]
+  double* dy_ = dx_ + 3 * nx;                               // ay_*inv [ny each]
+  for (int k = threadIdx.x; k < nx; k += blockDim.x) {
+    tx[k] = Tg.ax_p[k]; tx[nx + k] = Tg.ax_a[k]; tx[2 * nx + k] = Tg.ax_q[k]; tx[3 * nx + k] = Tg.ax_cc[k];
+    dx_[k] = Tg.ax_pinv[k]; dx_[nx + k] = Tg.ax_qinv[k]; dx_[2 * nx + k] = Tg.ax_ccinv[k];
+  }
+  for (int k = threadIdx.x; k < ny; k += blockDim.x) {
+    ty[k] = Tg.ay_p[k]; ty[ny + k] = Tg.ay_a[k]; ty[2 * ny + k] = Tg.ay_q[k]; ty[3 * ny + k] = Tg.ay_cc[k];
+    dy_[k] = Tg.ay_pinv[k]; dy_[ny + k] = Tg.ay_qinv[k]; dy_[2 * ny + k] = Tg.ay_ccinv[k];
+  }
+  AdiTab T = Tg;
+  T.ax_p = tx; T.ax_a = tx + nx; T.ax_q = tx + 2 * nx; T.ax_cc = tx + 3 * nx;
+  T.ax_pinv = dx_; T.ax_qinv = dx_ + nx; T.ax_ccinv = dx_ + 2 * nx;
+  T.ay_p = ty; T.ay_a = ty + ny; T.ay_q = ty + 2 * ny; T.ay_cc = ty + 3 * ny;
+  T.ay_pinv = dy_; T.ay_qinv = dy_ + ny; T.ay_ccinv = dy_ + 2 * ny;
   double2* U = a.U + field_plane(S, h, pol, s, a.ring_base) * N;
   const double2* Sc = a.Sc + ((size_t)hp * S + s) * N;
   const int4 bx = a.box[s];
   const bool src = a.use_source != 0;
   const int tid = threadIdx.x;
-  // ---- x sweep: thread per row j ----
+  // ---- stage the plane (coalesced) ----
+  for (int k = tid; k < N; k += blockDim.x) Apl[(k / nx) * nxp + (k % nx)] = U[k];
+  __syncthreads();
+  // ---- x sweep: thread per row j; one barrier per column so that every row
+  // has read column i of U before any row overwrites it with DD ----
+  const int j = tid;
+  const bool row = j >= 1 && j <= ny - 2;
   {
-    const int j = tid;
-    if (j >= 1 && j <= ny - 2) {
-      const cd rm = T.rx_m[j], r0 = T.rx_0[j], rp = T.rx_p[j];
-      const bool rowin = src && j >= bx.z && j <= bx.w;
-      cd DD = C(0, 0);
-      for (int i = 1; i <= nx - 2; ++i) {
-        const double2 up = U[(j + 1) * nx + i], u0 = U[j * nx + i], um = U[(j - 1) * nx + i];
+    cd rm = C(0, 0), r0 = C(0, 0), rp = C(0, 0);
+    if (row) { rm = T.rx_m[j]; r0 = T.rx_0[j]; rp = T.rx_p[j]; }
+    const bool rowin = row && src && j >= bx.z && j <= bx.w;
+    cd DD = C(0, 0);
+    for (int i = 1; i <= nx - 2; ++i) {
+      double2 up = make_double2(0, 0), u0 = up, um = up, sv = up;
+      if (row) {
+        up = Apl[(j + 1) * nxp + i]; u0 = Apl[j * nxp + i]; um = Apl[(j - 1) * nxp + i];
+        if (rowin && i >= bx.x && i <= bx.y) sv = Sc[j * nx + i];
+      }
+      __syncthreads();
+      if (row) {
         cd t = cmul(rm, C(up.x, up.y));
         t = cadd(t, cmul(r0, C(u0.x, u0.y)));
         t = csub(t, cmul(rp, C(um.x, um.y)));
-        if (rowin && i >= bx.x && i <= bx.y) {
-          const double2 sv = Sc[j * nx + i];
-          t = cadd(t, C(sv.x, sv.y));
-        }
+        if (rowin && i >= bx.x && i <= bx.y) t = cadd(t, C(sv.x, sv.y));
         if (i == 1) {
           DD = cdiv_inv(t, T.ax_p[1], T.ax_pinv[1]);
         } else if (i < nx - 2) {
@@ -412,6 +498,8 @@ __global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
         }
         Apl[j * nxp + i] = make_double2(DD.re, DD.im);
       }
+    }
+    if (row) {
       cd Uc = cdiv_inv(DD, T.ax_cc[nx - 2], T.ax_ccinv[nx - 2]);
       Apl[j * nxp + nx - 2] = make_double2(Uc.re, Uc.im);
       for (int i = nx - 3; i > 0; --i) {
@@ -429,54 +517,57 @@ __global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
   const bool col = i >= 1 && i <= nx - 2;
   cd rm = C(0, 0), r0 = C(0, 0), rp = C(0, 0);
   if (col) { rm = T.ry_m[i]; r0 = T.ry_0[i]; rp = T.ry_p[i]; }
-  const bool colin = src && i >= bx.x && i <= bx.y;
+  const bool colin = col && src && i >= bx.x && i <= bx.y;
   cd DD = C(0, 0);
-  for (int j = 1; j <= ny - 2; ++j) {
-    double2 up = make_double2(0, 0), u0 = up, um = up;
-    if (col) { up = Apl[j * nxp + i + 1]; u0 = Apl[j * nxp + i]; um = Apl[j * nxp + i - 1]; }
+  for (int jr = 1; jr <= ny - 2; ++jr) {
+    double2 up = make_double2(0, 0), u0 = up, um = up, sv = up;
+    if (col) {
+      up = Apl[jr * nxp + i + 1]; u0 = Apl[jr * nxp + i]; um = Apl[jr * nxp + i - 1];
+      if (colin && jr >= bx.z && jr <= bx.w) sv = Sc[jr * nx + i];
+    }
     __syncthreads();
     if (col) {
       cd t = cmul(rm, C(up.x, up.y));
       t = cadd(t, cmul(r0, C(u0.x, u0.y)));
       t = csub(t, cmul(rp, C(um.x, um.y)));
-      if (colin && j >= bx.z && j <= bx.w) {
-        const double2 sv = Sc[j * nx + i];
-        t = cadd(t, C(sv.x, sv.y));
-      }
-      if (j == 1) {
+      if (colin && jr >= bx.z && jr <= bx.w) t = cadd(t, C(sv.x, sv.y));
+      if (jr == 1) {
         DD = cdiv_inv(t, T.ay_p[1], T.ay_pinv[1]);
-      } else if (j < ny - 2) {
-        DD = csub(cdiv_inv(t, T.ay_p[j], T.ay_pinv[j]), cdiv_inv(cmul(T.ay_a[j], DD), T.ay_q[j], T.ay_qinv[j]));
+      } else if (jr < ny - 2) {
+        DD = csub(cdiv_inv(t, T.ay_p[jr], T.ay_pinv[jr]), cdiv_inv(cmul(T.ay_a[jr], DD), T.ay_q[jr], T.ay_qinv[jr]));
       } else {
         DD = csub(t, cdiv_inv(DD, T.ay_cc[ny - 3], T.ay_ccinv[ny - 3]));
       }
-      Apl[j * nxp + i] = make_double2(DD.re, DD.im);
+      Apl[jr * nxp + i] = make_double2(DD.re, DD.im);
     }
   }
-  double e = 0.0;
   if (col) {
     cd Un = cdiv_inv(DD, T.ay_cc[ny - 2], T.ay_ccinv[ny - 2]);
-    U[(ny - 2) * nx + i] = make_double2(Un.re, Un.im);
-    double en[1] = {cnorm(Un)};
-    for (int j = ny - 3; j > 0; --j) {
-      const double2 d = Apl[j * nxp + i];
-      Un = cdiv_inv(csub(C(d.x, d.y), Un), T.ay_cc[j], T.ay_ccinv[j]);
-      U[j * nx + i] = make_double2(Un.re, Un.im);
-      en[0] += cnorm(Un);
+    Apl[(ny - 2) * nxp + i] = make_double2(Un.re, Un.im);
+    for (int jr = ny - 3; jr > 0; --jr) {
+      const double2 d = Apl[jr * nxp + i];
+      Un = cdiv_inv(csub(C(d.x, d.y), Un), T.ay_cc[jr], T.ay_ccinv[jr]);
+      Apl[jr * nxp + i] = make_double2(Un.re, Un.im);
     }
-    e = en[0];
+  }
+  __syncthreads();
+  // ---- write the interior back (coalesced) and sum |U|^2 over the plane;
+  // edge columns keep their old values (the ADI never writes them) ----
+  double e = 0.0;
+  for (int k = tid; k < N; k += blockDim.x) {
+    const int jj = k / nx, ii = k % nx;
+    double2 v;
+    if (jj >= 1 && jj <= ny - 2 && ii >= 1 && ii <= nx - 2) {
+      v = Apl[jj * nxp + ii];
+      U[k] = v;
+    } else if (jj == 0 || jj == ny - 1) {
+      v = Apl[jj * nxp + ii];
+    } else {
+      v = U[k];
+    }
+    e += v.x * v.x + v.y * v.y;
   }
   if (a.energy) {
-    // boundary cells keep their values (the ADI never writes them)
-    if (tid < nx) {
-      const double2 b0 = U[tid], b1 = U[(ny - 1) * nx + tid];
-      e += b0.x * b0.x + b0.y * b0.y + b1.x * b1.x + b1.y * b1.y;
-      if (tid == 0 || tid == nx - 1)
-        for (int j = 1; j <= ny - 2; ++j) {
-          const double2 b = U[j * nx + tid];
-          e += b.x * b.x + b.y * b.y;
-        }
-    }
     const double t = block_sum(e, red);
     if (tid == 0) a.energy[(size_t)hp * S + s] = t;
   }
@@ -526,7 +617,9 @@ void adi_set_smem(size_t bytes) {
   cudaFuncSetAttribute(k_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)bytes);
 }
 
-size_t adi_smem_bytes(int nx, int ny, int nxp) { return (size_t)ny * nxp * sizeof(double2); }
+size_t adi_smem_bytes(int nx, int ny, int nxp) {
+  return (size_t)ny * nxp * sizeof(double2) + (size_t)4 * (nx + ny) * sizeof(double2) + (size_t)3 * (nx + ny) * sizeof(double);
+}
 
 void launch_adi(const AdiLaunch& a, cudaStream_t st) {
   const int mx = a.G.nx > a.G.ny ? a.G.nx : a.G.ny;
