@@ -1,0 +1,173 @@
+"""Pins of the CPU restatement.  The reference has no tests or golden vectors
+and cannot be built here, so the restatement is checked against analytic
+properties of the algorithm it restates (see oracle/felis_oracle.cpp)."""
+import math
+
+import numpy as np
+import pytest
+
+
+def _make(fb, oracle_mod, tmp_path, particles=True, **kw):
+    from felis_b200 import workloads
+
+    path = workloads.write_input(str(tmp_path / "p.inp"), **kw)
+    cfg = fb.Config(path)
+    p = cfg.params
+    o = oracle_mod.Oracle(p, threads=4)
+    b = cfg.load_beam(0, seed=2)
+    if not particles:
+        z = np.zeros(0)
+        b = dict(x=z, y=z, px=z, py=z, theta=z, gamma=z, offsets=np.zeros(p.slice_n + 1, np.int64),
+                 weights=np.zeros(p.slice_n))
+    o.set_particles(0, b["x"], b["y"], b["px"], b["py"], b["theta"], b["gamma"], b["offsets"], b["weights"])
+    return cfg, o, b
+
+
+def _dense_sweep(U, Sc, H, a, aP, b, bP):
+    """solveField.cpp:110-181 for one plane with numpy dense solves: rows
+    1..nx-3 normalised by alphaP, last row H - aP - a with sub-diagonal 1."""
+    ny, nx = U.shape
+
+    def solve(rhs, al, alP, n):
+        m = n - 2  # unknowns 1..n-2
+        A = np.zeros((m, m), dtype=complex)
+        d = np.zeros(m, dtype=complex)
+        for k in range(m):
+            i = k + 1
+            if i < n - 2:
+                if k > 0:
+                    A[k, k - 1] = al[i] / alP[i]
+                A[k, k] = (H - alP[i] - al[i]) / alP[i]
+                if k + 1 < m:
+                    A[k, k + 1] = 1.0
+                d[k] = rhs[i] / alP[i]
+            else:
+                A[k, k - 1] = 1.0
+                A[k, k] = H - alP[i] - al[i]
+                d[k] = rhs[i]
+        return np.linalg.solve(A, d)
+
+    Uc = np.zeros_like(U)
+    for j in range(1, ny - 1):
+        rhs = -bP[j] * U[j + 1] + (H + bP[j] + b[j]) * U[j] - b[j] * U[j - 1] + Sc[j]
+        Uc[j, 1:-1] = solve(rhs, a, aP, nx)
+    Un = U.copy()
+    for i in range(1, nx - 1):
+        rhs = -aP[i] * Uc[:, i + 1] + (H + aP[i] + a[i]) * Uc[:, i] - a[i] * Uc[:, i - 1] + Sc[:, i]
+        Un[1:-1, i] = solve(rhs, b, bP, ny)
+    return Un
+
+
+def test_adi_equals_dense_solve(fb, oracle_mod, tmp_path):
+    cfg, o, _ = _make(fb, oracle_mod, tmp_path, particles=False, kind="sase", slices=2, nx=31)
+    p = cfg.params
+    rng = np.random.default_rng(5)
+    U = rng.normal(size=(p.slice_n + 2, p.ny, p.nx)) + 1j * rng.normal(size=(p.slice_n + 2, p.ny, p.nx))
+    U[0] = 0
+    o.set_field(0, 0, U)
+    o.set_field(0, 1, U * 0.5)
+    lat = o.lattice()
+    lat.current_flag = 0
+    o.set_lattice(lat)
+    o.solve_field()
+    a, aP, b, bP = o.abc()
+    got = o.get_field(0, 0)
+    for s in (1, 2):
+        ref = _dense_sweep(U[s], np.zeros_like(U[s]), 1.0, a, aP, b, bP)
+        np.testing.assert_allclose(got[s], ref, rtol=1e-10, atol=1e-12 * np.abs(ref).max())
+
+
+def _diffraction_error(fb, oracle_mod, tmp_path, nx):
+    sig = 12.0
+    cfg, o, _ = _make(fb, oracle_mod, tmp_path, particles=False, kind="static", nx=nx, window_um=150.0,
+                      seed_sigma_um=sig, total_length=3.0)
+    p = cfg.params
+    ux, uy = cfg.load_seed(0)
+    o.set_field(0, 0, ux)
+    o.set_field(0, 1, uy)
+    steps = 150
+    lat = o.lattice()
+    lat.current_flag = 0
+    o.set_lattice(lat)
+    for _ in range(steps):
+        o.solve_field()
+    u = o.get_field(0, 0)[1]
+    z = steps * p.dz
+    sigR = math.sqrt(2.0) * sig * 1e-6
+    zR = 2.0 * (sig * 1e-6) ** 2 * p.ks
+    w = sigR * math.sqrt(1 + (z / zR) ** 2)
+    x = p.min_x + np.arange(p.nx) * p.dx
+    X, Y = np.meshgrid(x, x)
+    r2 = X ** 2 + Y ** 2
+    amp0 = np.abs(ux[1]).max()
+    expect = amp0 * sigR / w * np.exp(-r2 / (2 * w * w))
+    core = r2 < (2.5 * w) ** 2
+    err = np.abs(np.abs(u) - expect)[core].max() / amp0
+    return err, w / sigR, np.sum(np.abs(u) ** 2) / np.sum(np.abs(ux[1]) ** 2)
+
+
+def test_seed_diffraction_matches_gaussian_beam(fb, oracle_mod, tmp_path):
+    """Free-space propagation of the loaded Gaussian seed through the ADI
+    (no beam) against the closed form of loadSeed.cpp:56-77 further along z,
+    with the second-order convergence of the Crank-Nicolson scheme."""
+    e1, grow, pw = _diffraction_error(fb, oracle_mod, tmp_path, 120)
+    e2, _, _ = _diffraction_error(fb, oracle_mod, tmp_path, 240)
+    assert grow > 1.05  # the beam did diffract
+    assert e1 < 1e-2, e1
+    assert 3.0 < e1 / e2 < 5.0, (e1, e2)  # halving dx cuts the error ~4x
+    assert pw == pytest.approx(1.0, rel=2e-3)  # power conserved away from the absorbing edges
+
+
+@pytest.mark.parametrize("theta,expect", [
+    (0.0, 0.0), (2 * math.pi, 2 * math.pi - 2 * math.pi * 1), (-1e-12, 2 * math.pi - 1e-12),
+    (-2 * math.pi, 2 * math.pi), (7.0, 7.0 - 2 * math.pi), (-7.0, -7.0 + 4 * math.pi), (13.0, 13.0 - 4 * math.pi),
+])
+def test_theta_wrap_edges(fb, oracle_mod, tmp_path, theta, expect):
+    """rearrangeParticles.cpp:301-320: (int) truncation for theta >= dTh and
+    theta/dTh - 1 for theta < 0; theta == dTh exactly is wrapped to 0."""
+    cfg, o, b = _make(fb, oracle_mod, tmp_path, kind="static", beamlets=1)
+    th = np.full_like(b["theta"], theta)
+    o.set_particles(0, b["x"], b["y"], b["px"], b["py"], th, b["gamma"], b["offsets"], b["weights"])
+    o.periodic_particles()
+    got = o.get_particles(0)["theta"]
+    dTh = 2 * math.pi
+    if theta >= dTh:
+        ref = theta - dTh * int(theta / dTh)
+    elif theta < 0:
+        ref = theta - dTh * int(theta / dTh - 1.0)
+    else:
+        ref = theta
+    assert np.all(got == ref)
+    assert got[0] == pytest.approx(expect, abs=1e-12)
+
+
+def test_energy_balance(fb, oracle_mod, tmp_path):
+    """Field energy change equals minus the beam's kinetic energy change
+    (particlePush.cpp dgamma against updateTotalEnergy.cpp power) over the
+    first 3 m of a seeded static run; the rest is diffraction into the
+    absorbing boundary."""
+    cfg, o, b = _make(fb, oracle_mod, tmp_path, kind="static", beamlets=2048, seed_power=5e7, total_length=4.0)
+    p = cfg.params
+    b = cfg.load_beam(0, seed=1)
+    o.set_particles(0, b["x"], b["y"], b["px"], b["py"], b["theta"], b["gamma"], b["offsets"], b["weights"])
+    ux, uy = cfg.load_seed(0)
+    o.set_field(0, 0, ux)
+    o.set_field(0, 1, uy)
+    coef = (9.10938291e-31 * 299792458.0 ** 2 * p.ks / 1.60217662e-19) ** 2 / (2 * 376.730313668) * p.dx * p.dy
+    dt = p.lambda0 / 299792458.0  # one slice of one wavelength
+    g0 = o.get_particles(0)["gamma"].copy()
+    e0 = o.total_energy()[0]
+    o.run(0, 120, diagnostics=False)
+    g1 = o.get_particles(0)["gamma"]
+    e1 = o.total_energy()[0]
+    beam_loss = -np.sum(g1 - g0) * b["weights"][0] * 0.510998918e6 * 1.60217662e-19  # [J]
+    field_gain = (e1 - e0) * coef * dt  # [J]
+    assert abs(field_gain) > 1e-3 * e0 * coef * dt  # a real exchange happened
+    assert 0.9 < field_gain / beam_loss < 1.05, (field_gain, beam_loss)
+
+
+def test_oracle_builds_are_distinct(oracle_mod):
+    strict = oracle_mod.load("strict").orc_build_flags()
+    libm = oracle_mod.load("libm").orc_build_flags()
+    assert strict & 1 == 0 and libm & 1 == 1
+    assert strict & 2 == 0  # no fast-math in the parity golden
