@@ -108,6 +108,7 @@ _sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, _dp, _dp, _dp)
 _sig("felis_edge_deposit_count", C.c_int, _vp, _i64p)
 _sig("felis_sort_by_slice", C.c_int, _i32p, C.c_int64, _i64p)
+_sig("felis_sort_by_slice_noalloc", C.c_int, _vp, C.c_int64, _vp, _vp)
 _sig("felis_sync", C.c_int, _vp)
 _sig("felis_profile", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_kernel_stats", C.c_int, _vp, C.c_int32, _i64p, _dp)
@@ -408,6 +409,15 @@ def sort_by_slice(keys: np.ndarray) -> np.ndarray:
     if st != OK:
         raise FelisError(st, "felis_sort_by_slice")
     return perm
+
+
+SORT_NOALLOC_MAX_KEYS = 262144
+
+
+def sort_by_slice_noalloc(keys_dev_ptr: int, n: int, perm_dev_ptr: int, stream: int = 0) -> int:
+    """felis_sort_by_slice_noalloc on caller-owned device buffers (raw
+    pointers); queued on `stream`, returns the status without waiting."""
+    return _lib.felis_sort_by_slice_noalloc(keys_dev_ptr, n, perm_dev_ptr, stream or None)
 
 
 def detmath_sincos(x: float) -> tuple[float, float]:

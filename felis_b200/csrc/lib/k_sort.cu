@@ -18,7 +18,9 @@
 // element) plus the histograms; the tile sort stays in shared memory.
 #include <cuda_runtime.h>
 #include <stdint.h>
+#include <stdio.h>
 
+#include <mutex>
 #include <vector>
 
 #include "../../../include/felis_b200.h"
@@ -161,4 +163,121 @@ extern "C" felis_status felis_sort_by_slice(const int32_t* keys, int64_t n, int6
   if (hist) cudaFree(hist);
   if (st) cudaStreamDestroy(st);
   return rc;
+}
+
+// ---------------------------------------------------------------------------
+// Allocation-free variant.  Its scratch lives in one file-scope device array:
+// two 32-bit key buffers, two 32-bit index buffers and the per-tile digit
+// histogram, sized for FELIS_SORT_NOALLOC_MAX_KEYS keys.  Every GPU that
+// loads this library holds the array until the process exits.  Each pass
+// writes every scratch word it later reads, so nothing has to be cleared
+// between calls; calls that overlap on the GPU share the array and race.
+namespace {
+
+constexpr int64_t kNaMax = FELIS_SORT_NOALLOC_MAX_KEYS;
+constexpr int64_t kNaTiles = (kNaMax + kTile - 1) / kTile;
+constexpr size_t kNaBytes = (size_t)4 * kNaMax * 4 + (size_t)256 * kNaTiles * 4;
+
+static __device__ __align__(256) unsigned char g_sort_scratch[kNaBytes];
+
+// Device address of g_sort_scratch per device, resolved once per device.
+std::mutex g_na_mu;
+void* g_na_ptr[64] = {nullptr};
+
+__global__ void k_iota32(int32_t* v, int64_t n) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    v[i] = (int32_t)i;
+}
+
+__global__ void __launch_bounds__(kThreads) k_scatter32(const int32_t* kin, const int32_t* vin, int64_t n, int shift,
+                                                        int ntiles, const uint32_t* offs, int32_t* kout,
+                                                        int32_t* vout) {
+  __shared__ uint32_t s[kTile];
+  const int64_t base = (int64_t)blockIdx.x * kTile;
+  for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+    const int64_t e = base + i;
+    s[i] = e < n ? ((((uint32_t)kin[e] >> shift) & 255u) << 12) | (uint32_t)i : 0xFFFFFFFFu;
+  }
+  __syncthreads();
+  for (int k = 2; k <= kTile; k <<= 1)
+    for (int j = k >> 1; j > 0; j >>= 1) {
+      for (int i = threadIdx.x; i < kTile; i += blockDim.x) {
+        const int ixj = i ^ j;
+        if (ixj > i) {
+          const uint32_t a = s[i], b = s[ixj];
+          const bool up = (i & k) == 0;
+          if ((a > b) == up) { s[i] = b; s[ixj] = a; }
+        }
+      }
+      __syncthreads();
+    }
+  for (int q = threadIdx.x; q < kTile; q += blockDim.x) {
+    const uint32_t c = s[q];
+    if (c == 0xFFFFFFFFu) continue;
+    const uint32_t d = c >> 12;
+    int lo = 0, hi = q;
+    while (lo < hi) {
+      const int mid = (lo + hi) >> 1;
+      if ((s[mid] >> 12) < d) lo = mid + 1;
+      else hi = mid;
+    }
+    const int64_t e = base + (c & 4095u);
+    const uint64_t dst = (uint64_t)offs[(size_t)d * ntiles + blockIdx.x] + (uint64_t)(q - lo);
+    kout[dst] = kin[e];
+    vout[dst] = vin[e];
+  }
+}
+
+__global__ void k_widen(const int32_t* v, int64_t n, int64_t* out) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    out[i] = v[i];
+}
+
+}  // namespace
+
+extern "C" felis_status felis_sort_by_slice_noalloc(const int32_t* keys_dev, int64_t n, int64_t* perm_dev,
+                                                    void* stream) {
+  if (n < 0 || (n > 0 && (!keys_dev || !perm_dev))) return FELIS_BAD_ARG;
+  if (n > kNaMax) {
+    fprintf(stderr, "felis_sort_by_slice_noalloc: %lld keys exceed the fixed scratch of %lld keys\n",
+            (long long)n, (long long)kNaMax);
+    return FELIS_BAD_ARG;
+  }
+  if (n == 0) return FELIS_OK;
+  int dev = 0;
+  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FELIS_NO_DEVICE;
+  void* base = nullptr;
+  {
+    std::lock_guard<std::mutex> lock(g_na_mu);
+    if (!g_na_ptr[dev]) {
+      // first call on this device: resolve the array's device address (the
+      // host-side symbol is only a stand-in, not a device address)
+      void* p = nullptr;
+      if (cudaGetSymbolAddress(&p, g_sort_scratch) != cudaSuccess || !p) return FELIS_CUDA_ERROR;
+      g_na_ptr[dev] = p;
+    }
+    base = g_na_ptr[dev];
+  }
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  int32_t* K0 = reinterpret_cast<int32_t*>(base);
+  int32_t* K1 = K0 + kNaMax;
+  int32_t* V0 = K1 + kNaMax;
+  int32_t* V1 = V0 + kNaMax;
+  uint32_t* hist = reinterpret_cast<uint32_t*>(V1 + kNaMax);
+  const int ntiles = (int)((n + kTile - 1) / kTile);
+  // four 8-bit passes: keys ordered as unsigned 32-bit values, stable
+  k_iota32<<<256, 256, 0, st>>>(V0, n);
+  const int32_t* kin = keys_dev;
+  const int32_t* vin = V0;
+  int32_t* kouts[2] = {K1, K0};
+  int32_t* vouts[2] = {V1, V0};
+  for (int p = 0; p < 4; ++p) {
+    k_hist<<<ntiles, kThreads, 0, st>>>(kin, n, 8 * p, ntiles, hist);
+    k_scan<<<1, 1024, 0, st>>>(hist, (int64_t)256 * ntiles);
+    k_scatter32<<<ntiles, kThreads, 0, st>>>(kin, vin, n, 8 * p, ntiles, hist, kouts[p & 1], vouts[p & 1]);
+    kin = kouts[p & 1];
+    vin = vouts[p & 1];
+  }
+  k_widen<<<256, 256, 0, st>>>(vin, n, perm_dev);
+  return cudaGetLastError() == cudaSuccess ? FELIS_OK : FELIS_CUDA_ERROR;
 }

@@ -241,6 +241,24 @@ felis_status felis_last_run_ms(felis_handle* h, double* ms);
  * must lie in [0, 2^30). */
 felis_status felis_sort_by_slice(const int32_t* keys, int64_t n, int64_t* perm);
 
+/* Allocation-free slice sort.  No counterpart in the reference: FELIS itself
+ * never runs on a GPU.  It serves callers that must not allocate device
+ * memory themselves or through this library, for example a host code whose
+ * HBM is owned by another allocator (a framework's caching pool, a
+ * pre-partitioned MPI job) or a loop that cannot afford cudaMalloc's implicit
+ * device synchronisation.  Same result as felis_sort_by_slice for keys in
+ * [0, 2^30) (keys are ordered as unsigned 32-bit values), but keys_dev and
+ * perm_dev are device buffers the caller owns, the work is queued on
+ * `stream` (a cudaStream_t, NULL for the default stream) and the call returns
+ * without waiting for it.  Scratch is a fixed array inside the library
+ * (about 4 MB on every GPU that loads it, kept until exit), so n is limited
+ * to FELIS_SORT_NOALLOC_MAX_KEYS; larger n returns FELIS_BAD_ARG.  The first
+ * call on a device resolves the array's device address; make that first call
+ * before any stream capture.  Calls that overlap on the GPU share the array
+ * and race: serialise them (one stream, or events). */
+#define FELIS_SORT_NOALLOC_MAX_KEYS 262144
+felis_status felis_sort_by_slice_noalloc(const int32_t* keys_dev, int64_t n, int64_t* perm_dev, void* stream);
+
 /* ---- host-side setup of the reference's input format -------------------- */
 /* Parses a FELIS input file ([Domain], [Save], [Seed], [Undulator], [Quad],
  * [EBeam], [Wake_field], [Bessel_table], [Phase_shifter] blocks;
