@@ -17,7 +17,7 @@ LIB_PATH = os.path.join(_HERE, "_lib", "libfelis_b200.so")
 
 if not os.path.exists(LIB_PATH):
     raise ImportError(
-        f"felis_b200: {LIB_PATH} is missing; build it with `python -m felis_b200._build` "
+        f"felis_b200: {LIB_PATH} is missing; build it with `python felis_b200/_build.py` "
         "(the CUDA extension is required, there is no CPU fallback)")
 
 _lib = C.CDLL(LIB_PATH)
@@ -113,6 +113,19 @@ _sig("felis_sync", C.c_int, _vp)
 _sig("felis_profile", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_kernel_stats", C.c_int, _vp, C.c_int32, _i64p, _dp)
 _sig("felis_last_run_ms", C.c_int, _vp, _dp)
+_sig("felis_batch_create", C.c_int, C.POINTER(C.POINTER(Params)), C.c_int32, C.POINTER(_vp))
+_sig("felis_batch_destroy", None, _vp)
+_sig("felis_batch_last_error", C.c_char_p, _vp)
+_sig("felis_batch_upload_particles", C.c_int, _vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp, _i64p, _dp)
+_sig("felis_batch_download_particles", C.c_int, _vp, C.c_int32, _dp, _dp, _dp, _dp, _dp, _dp)
+_sig("felis_batch_upload_field", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp)
+_sig("felis_batch_download_field", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp)
+_sig("felis_batch_run", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_batch_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp)
+_sig("felis_batch_set_launch", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_batch_get_launch", C.c_int, _vp, _i32p, _i32p, _i32p)
+_sig("felis_batch_tune", C.c_int, _vp, C.c_int32, C.c_int32, _i32p)
+_sig("felis_batch_last_run_ms", C.c_int, _vp, _dp)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
 _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
@@ -390,6 +403,91 @@ class Handle:
             self.periodic_particles(it)
             if not lat.drift_flag and self.mode == TIME_DEPENDENT:
                 self.shift_field(it)
+
+
+class Batch:
+    """One felis_batch: an ensemble of independent runs in mixed precision
+    (FP32 particles, field and ADI; FP64 theta, lattice and sums)."""
+
+    def __init__(self, params: list):
+        arr = (C.POINTER(Params) * len(params))(*[C.pointer(p) for p in params])
+        b = _vp()
+        st = _lib.felis_batch_create(arr, len(params), C.byref(b))
+        if st != OK:
+            raise FelisError(st, "felis_batch_create failed (see stderr)")
+        self._b = b
+        self.n = len(params)
+        self.S = [p.slice_n for p in params]
+        self.nx = [p.nx for p in params]
+        self.ny = [p.ny for p in params]
+        self.H = [p.num_harmony for p in params]
+        self._counts = [0] * self.n
+
+    def close(self):
+        if getattr(self, "_b", None):
+            _lib.felis_batch_destroy(self._b)
+            self._b = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, st: int):
+        if st != OK:
+            raise FelisError(st, _lib.felis_batch_last_error(self._b).decode())
+
+    def upload_particles(self, inst: int, x, y, px, py, theta, gamma, offsets, weights):
+        arrs = [_f64(a) for a in (x, y, px, py, theta, gamma)]
+        off = np.ascontiguousarray(offsets, dtype=np.int64)
+        w = _f64(weights)
+        self._ck(_lib.felis_batch_upload_particles(self._b, inst, *(_p(a) for a in arrs),
+                                                   off.ctypes.data_as(_i64p), _p(w)))
+        self._counts[inst] = int(off[-1])
+
+    def download_particles(self, inst: int) -> dict:
+        n = self._counts[inst]
+        keys = ("x", "y", "px", "py", "theta", "gamma")
+        out = {k: np.zeros(n) for k in keys}
+        self._ck(_lib.felis_batch_download_particles(self._b, inst, *(_p(out[k]) for k in keys)))
+        return out
+
+    def upload_field(self, inst: int, hidx: int, pol: int, data: np.ndarray):
+        buf = _cplx_to_interleaved(data)
+        self._ck(_lib.felis_batch_upload_field(self._b, inst, hidx, pol, _p(buf)))
+
+    def download_field(self, inst: int, hidx: int, pol: int) -> np.ndarray:
+        S, nx, ny = self.S[inst], self.nx[inst], self.ny[inst]
+        buf = np.zeros(2 * (S + 2) * nx * ny)
+        self._ck(_lib.felis_batch_download_field(self._b, inst, hidx, pol, _p(buf)))
+        return (buf[0::2] + 1j * buf[1::2]).reshape(S + 2, ny, nx)
+
+    def run(self, it0: int, it1: int):
+        self._ck(_lib.felis_batch_run(self._b, it0, it1))
+
+    def diagnostics(self, inst: int, it0: int, it1: int):
+        n, H = it1 - it0, self.H[inst]
+        e = np.zeros(n * 2 * H)
+        t = np.zeros(n * 6)
+        b = np.zeros(n * 2 * H)
+        self._ck(_lib.felis_batch_get_diagnostics(self._b, inst, it0, it1, _p(e), _p(t), _p(b)))
+        return e.reshape(n, 2 * H), t.reshape(n, 6), b.reshape(n, 2 * H)
+
+    def set_launch(self, push_threads: int, adi_ctas: int):
+        self._ck(_lib.felis_batch_set_launch(self._b, push_threads, adi_ctas))
+
+    def launch(self) -> tuple[int, int, int]:
+        t, c, m = C.c_int32(), C.c_int32(), C.c_int32()
+        self._ck(_lib.felis_batch_get_launch(self._b, C.byref(t), C.byref(c), C.byref(m)))
+        return t.value, c.value, m.value
+
+    def tune(self, it0: int, steps: int) -> int:
+        nxt = C.c_int32(0)
+        self._ck(_lib.felis_batch_tune(self._b, it0, steps, C.byref(nxt)))
+        return nxt.value
+
+    def last_run_ms(self) -> float:
+        ms = C.c_double(0)
+        self._ck(_lib.felis_batch_last_run_ms(self._b, C.byref(ms)))
+        return ms.value
 
 
 def device_info() -> tuple[str, int]:

@@ -3,7 +3,10 @@
 Every CUDA translation unit is compiled for sm_100a only.  The FP64 plain
 path is compiled with --fmad=false (and host code with -ffp-contract=off) so
 that no multiply-add is contracted: the kernels then evaluate the same
-IEEE operations, in the same order, as the CPU restatement of the reference.
+IEEE operations, in the same order, as the CPU restatement of the reference.  The mixed-precision ensemble
+(batch.cu, k_batch.cu) is not bound to the restatement bit for bit: its
+kernels keep the compiler's multiply-add contraction and use the fast FP32
+division, square root and sin/cos.
 """
 from __future__ import annotations
 
@@ -28,6 +31,8 @@ UNITS = [
     ("lib/k_particles.cu", ["--fmad=false"]),
     ("lib/k_field.cu", ["--fmad=false"]),
     ("lib/k_sort.cu", []),
+    ("lib/batch.cu", []),
+    ("lib/k_batch.cu", ["--use_fast_math"]),
     ("host/config.cpp", []),
 ]
 

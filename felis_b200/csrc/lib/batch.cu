@@ -1,0 +1,882 @@
+// Host side of the mixed-precision ensemble engine (felis_batch_*).
+//
+// An ensemble holds many FELIS instances (each one Domain: its own slices,
+// grid, harmonics, lattice and beam) resident on one GPU.  All instances
+// advance together; every iteration is two launches over all instances, the
+// ADI over every field plane and the push (with the next deposit) over every
+// slice, followed by a per-instance diagnostic reduction.  A run of
+// iterations is captured as one CUDA graph.  The lattice
+// (updateK_quadG.cpp:8-94) is evaluated on the host in FP64 for every
+// instance and iteration and uploaded as a table.
+#include <math.h>
+#include <stdio.h>
+#include <string.h>
+
+#include <algorithm>
+#include <map>
+#include <string>
+#include <tuple>
+#include <vector>
+
+#include "batch.cuh"
+
+using namespace felis;
+
+namespace {
+
+struct HUnd {
+  int type, K0_alpha, air;
+  double lambdaU, slopeK, ue;
+  std::vector<double> unitStart, unitEnd, undStart, undEnd, K0;
+};
+struct HQuad {
+  std::vector<double> qdStart, qdEnd, g;
+};
+
+struct Inst {
+  felis_params p{};
+  std::vector<HUnd> und;
+  std::vector<HQuad> quad;
+  felis_lattice lat{};
+  int ring_base = 0;
+  int64_t count = 0;
+  bool uploaded = false;
+  std::vector<double> bessel;
+  // device
+  float *x = nullptr, *y = nullptr, *px = nullptr, *py = nullptr, *dg = nullptr;
+  double* th = nullptr;
+  int64_t* soff = nullptr;
+  float* weight = nullptr;
+  float2* U = nullptr;
+  float2* Ez = nullptr;
+  float* d_bessel = nullptr;
+  double* wake = nullptr;
+  float2* adi = nullptr;
+  float2* src = nullptr;
+  int4* sbox = nullptr;
+  int nsrc = 0;
+  int src_plane[FELIS_MAX_HARMONY] = {0};
+  double* part_e = nullptr;
+  double* part_b = nullptr;
+  int* err = nullptr;
+};
+
+// Same state machine as updateK_quadG.cpp:8-94.
+void update_lattice(Inst& I, int iteration, double half) {
+  felis_lattice& D = I.lat;
+  const double dz = I.p.dz, z = (iteration + half) * dz;
+  double K0 = D.K0, ue = D.ue, lambdaU = D.lambdaU;
+  int K0_alpha = D.K0_alpha, undType = D.und_type;
+  bool inUnd = false, inInter = false, air = false;
+  for (const HUnd& U : I.und)
+    for (size_t n = 0; n < U.unitStart.size(); ++n)
+      if (z >= U.unitStart[n] && z < U.unitEnd[n]) {
+        if (z >= U.undStart[n] && z < U.undEnd[n]) {
+          inUnd = true;
+          K0 = U.K0[n] * (1 + U.slopeK * (z - U.undStart[n]));
+          K0_alpha = U.K0_alpha; ue = U.ue; undType = U.type; lambdaU = U.lambdaU;
+        } else {
+          inInter = true;
+          if (U.air) air = true;
+        }
+      }
+  D.K0 = K0; D.ue = ue; D.K0_alpha = K0_alpha; D.lambdaU = lambdaU; D.ku = 2 * M_PI / lambdaU; D.und_type = undType;
+  D.current_flag = 0;
+  D.drift_flag = 0;
+  if (K0 == 0.0) air = true;
+  if (!inUnd && !inInter) air = true;
+  if (inUnd) D.current_flag = 1;
+  if (air) { D.ku = 0.0; D.drift_flag = 1; D.current_flag = 0; }
+  double g = 0;
+  const double x0 = z, x1 = z + dz * 0.5;
+  for (const HQuad& Q : I.quad)
+    for (size_t n = 0; n < Q.g.size(); ++n) {
+      const double q0 = Q.qdStart[n], q1 = Q.qdEnd[n];
+      if (q1 <= x0 || q0 >= x1) continue;
+      if (x0 < q0 && q1 < x1) g = (q1 - q0) / dz * 2.0 * Q.g[n];
+      else if (x0 < q0 && q0 < x1) g = (x1 - q0) / dz * 2.0 * Q.g[n];
+      else if (x0 < q1 && q1 < x1) g = (q1 - x0) / dz * 2.0 * Q.g[n];
+      else g = 1.0 * Q.g[n];
+      break;
+    }
+  D.g = g;
+}
+
+bool phi_eta(const felis_lattice& L, double* Phi, double eta[4]) {
+  const double ue = L.ue;
+  *Phi = atan2(2.0 * ue / (1.0 + ue * ue), (1.0 - ue * ue) / (1.0 + ue * ue));
+  const double c = cos(*Phi * 0.5), s = sin(*Phi * 0.5);
+  if (L.K0_alpha == 1) { eta[0] = c; eta[1] = 0; eta[2] = 0; eta[3] = s; }
+  else if (L.K0_alpha == -1) { eta[0] = 0; eta[1] = s; eta[2] = c; eta[3] = 0; }
+  else return false;
+  return true;
+}
+
+// Transverse half-push of particlePush.cpp:42-110 for lattice L: for a
+// fixed a = 1/gamma the RK4 step of dz/2 is exact polynomial arithmetic on
+// the linear system s' = A(a) s, s = (x, y, px, py):
+//   x'  = a px - aa a^2 (K0a x + y)        y'  = a py + aa a^2 (K0a x - y)
+//   px' = K0a dd (px - py) - fx x           py' = K0a dd (px + py) - fy y
+// with dd = ku K0^2 ue a^2 / 4, fx = bb a xCoef + cc, fy = bb a yCoef - cc;
+// the step multiplies s by P(hA) = I + hA + (hA)^2/2 + (hA)^3/6 + (hA)^4/24.
+struct HalfPush {
+  double h, K0, ue, ku, aa, bb, cc, xCoef, yCoef, K0a;
+};
+
+HalfPush half_push(const Inst& I, const felis_lattice& L) {
+  HalfPush t;
+  t.h = I.p.dz * 0.5;
+  t.K0 = L.K0; t.ue = L.ue; t.ku = L.ku;
+  t.aa = L.K0 * L.K0 * 0.25 * L.ue * L.ku;
+  t.bb = L.K0 * L.K0 * 0.25 * (1.0 + L.ue * L.ue) * L.ku * L.ku;
+  t.cc = K_ECHARGE * L.g / K_EMASS / K_VELOCITYC;
+  t.xCoef = 0.0; t.yCoef = 0.0;
+  if (L.und_type == FELIS_BIPOLAR) {
+    if (L.K0_alpha == 1) t.xCoef = 1.0;
+    else if (L.K0_alpha == -1) t.yCoef = 1.0;
+  } else {
+    t.xCoef = 1.0; t.yCoef = 1.0;
+  }
+  t.K0a = L.K0_alpha;
+  return t;
+}
+
+typedef std::vector<double> Mat;  // 4 x 4, row-major
+
+Mat matmul(const Mat& A, const Mat& B) {
+  Mat C(16, 0.0);
+  for (int r = 0; r < 4; ++r)
+    for (int c = 0; c < 4; ++c)
+      for (int k = 0; k < 4; ++k) C[r * 4 + c] += A[r * 4 + k] * B[k * 4 + c];
+  return C;
+}
+
+Mat half_map(const HalfPush& t, double a) {
+  const double dd = t.ku * t.K0 * t.K0 * 0.25 * a * a * t.ue;
+  const double fx = t.bb * a * t.xCoef + t.cc, fy = t.bb * a * t.yCoef - t.cc;
+  Mat X = {-t.aa * t.K0a * a * a, -t.aa * a * a, a, 0.0,
+           t.aa * t.K0a * a * a, -t.aa * a * a, 0.0, a,
+           -fx, 0.0, t.K0a * dd, -t.K0a * dd,
+           0.0, -fy, t.K0a * dd, t.K0a * dd};
+  for (double& v : X) v *= t.h;
+  // Horner: I + X (I + X/2 (I + X/3 (I + X/4)))
+  Mat P(16, 0.0);
+  for (int k = 0; k < 4; ++k) P[k * 5] = 1.0;
+  for (int d = 4; d >= 1; --d) {
+    Mat Q = matmul(X, P);
+    for (int k = 0; k < 16; ++k) P[k] = (k % 5 == 0 ? 1.0 : 0.0) + Q[k] / d;
+  }
+  return P;
+}
+
+// Both half pushes (lattices l0 then l1) to second order in a - 1/gamR.
+void transverse_maps(const Inst& I, const felis_lattice& l0, const felis_lattice& l1, BStep& T) {
+  const HalfPush t0 = half_push(I, l0), t1 = half_push(I, l1);
+  const double aR = 1.0 / I.p.gam_r, eps = aR * 1e-3;
+  auto full = [&](double a) { return matmul(half_map(t1, a), half_map(t0, a)); };
+  const Mat M0 = full(aR), Mp = full(aR + eps), Mm = full(aR - eps);
+  for (int k = 0; k < 16; ++k) {
+    T.tD0[k] = (float)(M0[k] - (k % 5 == 0 ? 1.0 : 0.0));
+    T.tM1[k] = (float)((Mp[k] - Mm[k]) / (2.0 * eps));
+    T.tM2[k] = (float)((Mp[k] - 2.0 * M0[k] + Mm[k]) / (2.0 * eps * eps));
+  }
+}
+
+// ADI tables of one harmonic in FP32 (the reference recurrence of
+// solveField.cpp:138-180 rewritten with reciprocals): per direction p = 1/aP
+// (last row 1), m = a/(aP CC[i-1]) (first row 0, last row 1/CC[i-1]),
+// r = 1/CC, and the right-hand-side coefficients.
+void adi_tables(const felis_params& p, int hidx, int M, std::vector<float2>& out) {
+  typedef double2 d2;
+  auto C2 = [](double r, double i) { return make_double2(r, i); };
+  auto mul = [&](d2 a, d2 b) { return C2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
+  auto inv = [&](d2 b) { const double n = b.x * b.x + b.y * b.y; return C2(b.x / n, -b.y / n); };
+  auto sub = [&](d2 a, d2 b) { return C2(a.x - b.x, a.y - b.y); };
+  auto add = [&](d2 a, d2 b) { return C2(a.x + b.x, a.y + b.y); };
+  const double H = p.harmony[hidx];
+  out.assign((size_t)12 * M, make_float2(0.f, 0.f));
+  auto put = [&](int t, int k, d2 v) { out[(size_t)t * M + k] = make_float2((float)v.x, (float)v.y); };
+  for (int dir = 0; dir < 2; ++dir) {
+    const int n = dir == 0 ? p.nx : p.ny;
+    const double* A = dir == 0 ? p.abc_alpha : p.abc_beta;
+    const double* AP = dir == 0 ? p.abc_alpha_p : p.abc_beta_p;
+    std::vector<d2> al(n), ap(n), CC(n);
+    for (int i = 0; i < n; ++i) { al[i] = C2(A[2 * i], A[2 * i + 1]); ap[i] = C2(AP[2 * i], AP[2 * i + 1]); }
+    CC[1] = mul(sub(sub(C2(H, 0), ap[1]), al[1]), inv(ap[1]));
+    for (int i = 2; i < n - 2; ++i)
+      CC[i] = sub(mul(sub(sub(C2(H, 0), ap[i]), al[i]), inv(ap[i])), mul(al[i], inv(mul(ap[i], CC[i - 1]))));
+    CC[n - 2] = sub(sub(sub(C2(H, 0), ap[n - 2]), al[n - 2]), inv(CC[n - 3]));
+    const int tp = dir == 0 ? 0 : 3;
+    for (int i = 1; i < n - 1; ++i) {
+      put(tp + 0, i, i < n - 2 ? inv(ap[i]) : C2(1, 0));
+      put(tp + 1, i, i == 1 ? C2(0, 0) : (i < n - 2 ? mul(al[i], inv(mul(ap[i], CC[i - 1]))) : inv(CC[n - 3])));
+      put(tp + 2, i, inv(CC[i]));
+    }
+    // rhs of the other sweep uses this direction's coefficients
+    const int tr = dir == 0 ? 9 : 6;
+    for (int i = 1; i < n - 1; ++i) {
+      put(tr + 0, i, C2(-ap[i].x, -ap[i].y));
+      put(tr + 1, i, add(add(C2(H, 0), ap[i]), al[i]));
+      put(tr + 2, i, al[i]);
+    }
+  }
+}
+
+}  // namespace
+
+struct felis_batch {
+  std::vector<Inst> in;
+  int device = 0, sms = 0, dev_smem = 0;
+  cudaStream_t st = nullptr;
+  std::string err;
+  int nx_max = 0, ny_max = 0, H_max = 1, LF_max = 1, nr_max = 1, N_max = 0, nsrc_max = 1;
+  BInst* d_inst = nullptr;
+  int4* d_adi_work = nullptr;
+  int4* d_push_work = nullptr;
+  int n_adi = 0, n_push = 0;
+  BStep* d_steps = nullptr;
+  int steps_cap = 0;
+  double *d_he = nullptr, *d_ht = nullptr, *d_hb = nullptr;
+  int hist_n = 0;
+  int adi_threads = 128, adi_smem = 0;
+  int push_threads = 256, push_smem = 0, push_minb = 2, adi_ctas = 2;
+  bool layout_ready = false;
+  int src_valid_it = -1;  // iteration whose solveField source is in the buffers
+  double last_run_ms = 0.0;
+  int* h_err = nullptr;
+};
+
+namespace {
+
+#define BCK(call)                                                                    \
+  do {                                                                               \
+    cudaError_t e_ = (call);                                                         \
+    if (e_ != cudaSuccess) {                                                         \
+      b->err = std::string(#call) + ": " + cudaGetErrorString(e_);                   \
+      return FELIS_CUDA_ERROR;                                                       \
+    }                                                                                \
+  } while (0)
+
+felis_status bfail(felis_batch* b, felis_status s, const std::string& m) {
+  if (b) b->err = m;
+  return s;
+}
+
+felis_status upload_inst_table(felis_batch* b) {
+  std::vector<BInst> h(b->in.size());
+  for (size_t k = 0; k < b->in.size(); ++k) {
+    Inst& I = b->in[k];
+    BInst& D = h[k];
+    const felis_params& p = I.p;
+    D.S = p.slice_n; D.nx = p.nx; D.ny = p.ny; D.N = p.nx * p.ny; D.H = p.num_harmony; D.L = p.scl_mode;
+    D.F = p.scf_mode; D.nr = p.nr; D.nxp = p.nx | 1; D.bn = p.bessel_rows; D.bcols = p.bessel_cols;
+    D.numSlice = p.num_slice; D.minI = p.min_i; D.wakeOn = p.wake_on;
+    D.nsrc = I.nsrc;
+    for (int i = 0; i < FELIS_MAX_HARMONY; ++i) {
+      D.harmony[i] = i < p.num_harmony ? p.harmony[i] : 1;
+      D.src_plane[i] = I.src_plane[i];
+    }
+    D.ks = p.ks; D.dz = p.dz; D.dx = p.dx; D.dy = p.dy; D.dr = p.dr; D.minX = p.min_x; D.minY = p.min_y;
+    D.gamR = p.gam_r; D.dBessel = p.d_bessel;
+    D.x = I.x; D.y = I.y; D.px = I.px; D.py = I.py; D.dg = I.dg; D.th = I.th;
+    D.soff = I.soff; D.weight = I.weight; D.U = I.U; D.Ez = I.Ez; D.src = I.src; D.sbox = I.sbox;
+    D.bessel = I.d_bessel; D.wakeE = I.wake;
+    D.adi_c = I.adi; D.part_e = I.part_e; D.part_b = I.part_b; D.err = I.err;
+  }
+  BCK(cudaMemcpy(b->d_inst, h.data(), h.size() * sizeof(BInst), cudaMemcpyHostToDevice));
+  return FELIS_OK;
+}
+
+// Deposit constants of lattice L (solveField.cpp:209-301; the odd-harmonic
+// fx, fy with the lattice's constant xi).
+bool make_dep(const Inst& I, const felis_lattice& L, BDep* d) {
+  double eta[4], Phi;
+  if (!phi_eta(L, &Phi, eta)) return false;
+  const felis_params& p = I.p;
+  const double K0 = L.K0, ue = L.ue, ks = p.ks;
+  d->K0 = (float)K0; d->ue = (float)ue; d->K0a = (float)L.K0_alpha; d->Phi_half = (float)(Phi * 0.5);
+  d->coef_U = (float)(p.dz * K_ECHARGE * K_ECHARGE * K_MU0 * K0 * sqrt(1.0 + ue * ue) /
+                      (4.0 * ks * K_EMASS * (p.lambda0 * p.num_slice) * p.dx * p.dy));
+  const double xi = 0.25 * K0 * K0 * (1.0 - ue * ue) / (1.0 + (1.0 + ue * ue) * K0 * K0 * 0.5);
+  d->xi = (float)xi;
+  d->coef_Ez = (float)(K_ECHARGE * K_VELOCITYC * K_VELOCITYC * K_MU0 * ks * (1.0 + 0.5 * (1.0 + ue * ue) * K0 * K0) /
+                       (2.0 * M_PI * p.lambda0 * p.num_slice * p.gam_r * p.gam_r));
+  d->A = ks * ks * (1.0 + 0.5 * (1.0 + ue * ue) * K0 * K0) / (p.gam_r * p.gam_r) * p.dr * p.dr;
+  d->etaX = make_float2((float)eta[0], (float)eta[1]);
+  d->etaY = make_float2((float)eta[2], (float)eta[3]);
+  for (int h = 0; h < FELIS_MAX_HARMONY; ++h) d->fconst[h][0] = d->fconst[h][1] = 0.f;
+  for (int h = 0; h < p.num_harmony; ++h) {
+    const int H = p.harmony[h];
+    if (H % 2 == 1) {
+      const double x = H * xi / p.d_bessel;
+      const int i0 = std::max(0, std::min((int)x, p.bessel_rows - 1));
+      const int i1 = std::min(i0 + 1, p.bessel_rows - 1);
+      const double w1 = x - (int)x, w0 = 1.0 - w1;
+      const int bc = p.bessel_cols;
+      const double J1 = I.bessel[(size_t)i0 * bc + (H - 1) / 2] * w0 + I.bessel[(size_t)i1 * bc + (H - 1) / 2] * w1;
+      const double J2 = I.bessel[(size_t)i0 * bc + (H + 1) / 2] * w0 + I.bessel[(size_t)i1 * bc + (H + 1) / 2] * w1;
+      const double sign = ((H - 1) / 2 % 2 == 0) ? 1.0 : -1.0;
+      d->fconst[h][0] = (float)(sign * (J1 - L.K0_alpha * J2));
+      d->fconst[h][1] = (float)(sign * (J1 + L.K0_alpha * J2));
+    }
+  }
+  return true;
+}
+
+// ADI source factors of a deposit made with lattice L: odd harmonics keep one
+// plane m = sum w mc, the ADI adds -eta fx m (x) and -eta fy m (y); even
+// harmonics deposit each polarisation directly.
+void make_sfac(const Inst& I, const BDep& d, float2 sfac[FELIS_MAX_HARMONY][2]) {
+  for (int h = 0; h < FELIS_MAX_HARMONY; ++h) {
+    sfac[h][0] = sfac[h][1] = make_float2(1.f, 0.f);
+    if (h < I.p.num_harmony && (I.p.harmony[h] & 1)) {
+      const double fx = d.fconst[h][0], fy = d.fconst[h][1];
+      sfac[h][0] = make_float2((float)(-d.etaX.x * fx), (float)(-d.etaX.y * fx));
+      sfac[h][1] = make_float2((float)(-d.etaY.x * fy), (float)(-d.etaY.y * fy));
+    }
+  }
+}
+
+// Per-iteration scalars of every instance for iterations [it0, it1), plus
+// one row (index it1 - it0) for a deposit-only launch at it0.
+felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& out) {
+  const int n = (int)b->in.size();
+  out.assign((size_t)(it1 - it0 + 1) * n, BStep{});
+  for (int k = 0; k < n; ++k) {
+    Inst& I = b->in[k];
+    const felis_params& p = I.p;
+    {
+      BStep& D0 = out[(size_t)(it1 - it0) * n + k];
+      D0.ring_base = I.ring_base;
+      D0.deposit = I.lat.current_flag;
+      if (!make_dep(I, I.lat, &D0.dep)) return bfail(b, FELIS_BAD_ARG, "invalid K0_alpha");
+    }
+    for (int it = it0; it < it1; ++it) {
+      BStep& T = out[(size_t)(it - it0) * n + k];
+      const felis_lattice dl = I.lat;  // solveField uses the flag left by the previous iteration
+      update_lattice(I, it, 0);
+      const felis_lattice l0 = I.lat;
+      update_lattice(I, it, 0.5);
+      const felis_lattice l1 = I.lat;
+      T.ring_base = I.ring_base;
+      T.current = dl.current_flag;
+      T.drift = l1.drift_flag;
+      T.shift = !l1.drift_flag && p.mode == FELIS_TIME_DEPENDENT;
+      if (T.shift) I.ring_base = (I.ring_base - 1 + p.slice_n) % p.slice_n;
+      if (l0.und_type != FELIS_BIPOLAR && l0.und_type != FELIS_QUADPOLAR) return bfail(b, FELIS_BAD_ARG, "no undulator_mode");
+      transverse_maps(I, l0, l1, T);
+      BDep dd;
+      if (!make_dep(I, dl, &dd)) return bfail(b, FELIS_BAD_ARG, "invalid K0_alpha");
+      make_sfac(I, dd, T.sfac);
+      T.deposit = l1.current_flag;
+      if (!make_dep(I, l1, &T.dep)) return bfail(b, FELIS_BAD_ARG, "invalid K0_alpha");
+      double eta[4], Phi;
+      phi_eta(l1, &Phi, eta);
+      const double ks = p.ks, K0 = l1.K0, ue = l1.ue, ku = l1.ku, gR = p.gam_r;
+      const double A0 = ks / (2.0 * gR * gR), c1 = (1.0 + ue * ue) * K0 * K0 * 0.5, Q0 = 1.0 + c1;
+      T.R0 = (float)(ku - A0 * Q0);
+      T.A0 = (float)A0;
+      T.AQ0 = (float)(A0 * Q0);
+      T.c1 = (float)c1;
+      T.c2 = (float)(ku * ku * 0.5);
+      T.K0 = (float)K0; T.ue = (float)ue; T.K0a = (float)l1.K0_alpha; T.Phi_half = (float)(Phi * 0.5);
+      T.cxi = ku != 0.0 ? (float)(ks / ku * K0 * K0 / 8.0 * (1.0 - ue * ue)) : 0.f;
+      T.sq = (float)sqrt(ue * ue + 1.0);
+      T.ksK0 = (float)(ks * K0);
+      T.e_mc2 = (float)(K_ECHARGE / K_EMASS / K_VELOCITYC / K_VELOCITYC);
+      T.dPhi = (float)(2 * M_PI * p.num_slice);
+      T.ku = ku;
+      T.A0d = A0;
+      T.etaX = make_float2((float)eta[0], (float)eta[1]);
+      T.etaY = make_float2((float)eta[2], (float)eta[3]);
+    }
+  }
+  return FELIS_OK;
+}
+
+felis_status prepare(felis_batch* b) {
+  if (b->layout_ready) return FELIS_OK;
+  for (auto& I : b->in)
+    if (!I.uploaded) return bfail(b, FELIS_BAD_ARG, "particles of every instance must be uploaded first");
+  // work lists, longest items first (the hardware block scheduler then runs a
+  // longest-processing-time schedule): ADI planes by their sweep length,
+  // slices by their particle count
+  std::vector<int4> adi, push;
+  std::vector<double> ca, cp;
+  for (size_t k = 0; k < b->in.size(); ++k) {
+    const Inst& I = b->in[k];
+    std::vector<int64_t> so(I.p.slice_n + 1);
+    BCK(cudaMemcpy(so.data(), I.soff, so.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    for (int s = 0; s < I.p.slice_n; ++s) {
+      push.push_back(make_int4((int)k, s, 0, 0));
+      cp.push_back((double)(so[s + 1] - so[s]));
+      for (int hp = 0; hp < 2 * I.p.num_harmony; ++hp) {
+        adi.push_back(make_int4((int)k, s, hp, 0));
+        ca.push_back((double)(I.p.nx + I.p.ny) * I.p.nx);
+      }
+    }
+  }
+  auto sorted = [](std::vector<int4>& w, const std::vector<double>& c) {
+    std::vector<int> o(w.size());
+    for (size_t k = 0; k < o.size(); ++k) o[k] = (int)k;
+    std::stable_sort(o.begin(), o.end(), [&](int a, int d) { return c[a] > c[d]; });
+    std::vector<int4> r(w.size());
+    for (size_t k = 0; k < o.size(); ++k) r[k] = w[o[k]];
+    w.swap(r);
+  };
+  sorted(adi, ca);
+  sorted(push, cp);
+  b->n_adi = (int)adi.size();
+  b->n_push = (int)push.size();
+  if (b->d_adi_work) cudaFree(b->d_adi_work);
+  if (b->d_push_work) cudaFree(b->d_push_work);
+  b->d_adi_work = b->d_push_work = nullptr;
+  BCK(cudaMalloc(&b->d_adi_work, adi.size() * sizeof(int4)));
+  BCK(cudaMalloc(&b->d_push_work, push.size() * sizeof(int4)));
+  BCK(cudaMemcpy(b->d_adi_work, adi.data(), adi.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_push_work, push.data(), push.size() * sizeof(int4), cudaMemcpyHostToDevice));
+  felis_status s = upload_inst_table(b);
+  if (s != FELIS_OK) return s;
+  b->layout_ready = true;
+  return FELIS_OK;
+}
+
+// Shared memory of both launches: the ADI holds its plane, 6 tables and as
+// much of the source box as fits beside adi_ctas CTAs per SM (more cells are
+// read from global memory); the push holds the accumulators of up to 6144 source
+// cells (larger boxes accumulate in the source buffer in global memory).
+felis_status ensure_launch(felis_batch* b) {
+  const int M32 = ((std::max(b->nx_max, b->ny_max) + 31) / 32) * 32;
+  if (M32 > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
+  b->adi_threads = std::max(M32, 64);
+  const size_t base = batch_adi_smem(b->nx_max, b->ny_max, 0);
+  if ((int)base > b->dev_smem) return bfail(b, FELIS_UNSUPPORTED, "field plane does not fit in shared memory");
+  const size_t per = (size_t)(b->dev_smem / b->adi_ctas - 1024);
+  size_t src_cells = 0;
+  if (base <= per) src_cells = (per - base) / sizeof(float2);
+  else src_cells = ((size_t)b->dev_smem - base) / sizeof(float2);
+  src_cells = std::min(src_cells, (size_t)b->N_max);
+  b->adi_smem = (int)batch_adi_smem(b->nx_max, b->ny_max, (int)src_cells);
+  const int box = std::min(b->N_max, 6144);
+  b->push_smem = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, box);
+  batch_set_smem(b->H_max, b->push_minb, b->adi_smem, b->push_smem);
+  return FELIS_OK;
+}
+
+felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
+  const int n = (int)b->in.size();
+  const int se = 2 * b->H_max, stt = 6, sb = 2 * b->H_max;
+  const int steps = it1 - it0;
+  const BStep* row_d0 = b->d_steps + (size_t)steps * n;
+  if (it0 < b->hist_n) {
+    // diagnostics of the state at it0 (row d0 carries the ring offset, no shift)
+    launch_batch_measure(b->d_inst, row_d0, b->d_push_work, b->n_push, b->st);
+    launch_batch_reduce(b->d_inst, n, row_d0, b->d_he + (size_t)it0 * se, b->d_ht + (size_t)it0 * stt,
+                        b->d_hb + (size_t)it0 * sb, se * b->hist_n, stt * b->hist_n, sb * b->hist_n, b->st);
+  }
+  if (deposit0) {
+    BatchLaunch d{};
+    d.inst = b->d_inst; d.step = row_d0; d.work = b->d_push_work; d.nwork = b->n_push;
+    d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY;
+    launch_batch_push(d, b->H_max, b->push_minb, b->push_threads, b->st);
+  }
+  for (int it = it0; it < it1; ++it) {
+    const BStep* T = b->d_steps + (size_t)(it - it0) * n;
+    BatchLaunch a{};
+    a.inst = b->d_inst; a.step = T; a.work = b->d_adi_work; a.nwork = b->n_adi; a.smem_bytes = b->adi_smem;
+    launch_batch_adi(a, b->adi_threads, b->st);
+    BatchLaunch p{};
+    p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
+    p.mode = BATCH_PUSH;
+    launch_batch_push(p, b->H_max, b->push_minb, b->push_threads, b->st);
+    if (it + 1 < b->hist_n)
+      launch_batch_reduce(b->d_inst, n, T, b->d_he + (size_t)(it + 1) * se, b->d_ht + (size_t)(it + 1) * stt,
+                          b->d_hb + (size_t)(it + 1) * sb, se * b->hist_n, stt * b->hist_n, sb * b->hist_n, b->st);
+  }
+  BCK(cudaGetLastError());
+  return FELIS_OK;
+}
+
+felis_status check_batch_err(felis_batch* b) {
+  for (auto& I : b->in) {
+    BCK(cudaMemcpy(b->h_err, I.err, ERR_SLOTS * sizeof(int), cudaMemcpyDeviceToHost));
+    felis_status s = FELIS_OK;
+    if (b->h_err[ERR_THETA_OVERFLOW]) s = bfail(b, FELIS_THETA_OVERFLOW, "push_theta_gamma: |dtheta| > 2 pi numSlice");
+    else if (b->h_err[ERR_OUT_OF_RANGE]) s = bfail(b, FELIS_OUT_OF_RANGE, "theta outside [0, dTh] after the wrap");
+    else if (b->h_err[ERR_NAN]) s = bfail(b, FELIS_NAN, "non-finite particle state");
+    if (s != FELIS_OK) {
+      BCK(cudaMemset(I.err, 0, ERR_SLOTS * sizeof(int)));
+      return s;
+    }
+  }
+  return FELIS_OK;
+}
+
+}  // namespace
+
+extern "C" {
+
+felis_status felis_batch_create(const felis_params* const* instances, int32_t n, felis_batch** out) {
+  if (!instances || n < 1 || !out) return FELIS_BAD_ARG;
+  *out = nullptr;
+  int ndev = 0;
+  if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FELIS_NO_DEVICE;
+  felis_batch* b = new felis_batch();
+  cudaGetDevice(&b->device);
+  cudaDeviceGetAttribute(&b->sms, cudaDevAttrMultiProcessorCount, b->device);
+  cudaDeviceGetAttribute(&b->dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, b->device);
+  auto bad = [&](felis_status s, const char* m) {
+    fprintf(stderr, "felis_batch_create: %s\n", m);
+    felis_batch_destroy(b);
+    return s;
+  };
+  if (cudaStreamCreateWithFlags(&b->st, cudaStreamNonBlocking) != cudaSuccess) return bad(FELIS_CUDA_ERROR, "stream");
+  if (cudaMallocHost(&b->h_err, ERR_SLOTS * sizeof(int)) != cudaSuccess) return bad(FELIS_CUDA_ERROR, "host buffer");
+  b->in.resize(n);
+  int max_step = 1;
+  for (int k = 0; k < n; ++k) {
+    const felis_params* p = instances[k];
+    if (!p || p->abi_version != FELIS_ABI_VERSION || p->dimension != 3 || p->num_species != 1 || p->slice_n < 1 ||
+        p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY || p->nx < 4 || p->ny < 4 || p->scl_mode < 1 ||
+        p->scl_mode > 4 || p->scf_mode < 1 || p->scl_mode * p->scf_mode > 16 || !p->bessel || !p->abc_alpha)
+      return bad(FELIS_BAD_ARG, "instance parameters rejected (one species, 3D, L <= 4)");
+    Inst& I = b->in[k];
+    I.p = *p;
+    for (int u = 0; u < p->num_undulators; ++u) {
+      const felis_undulator& U = p->undulators[u];
+      HUnd o;
+      o.type = U.type; o.K0_alpha = U.K0_alpha; o.air = U.air; o.lambdaU = U.lambdaU; o.slopeK = U.slopeK; o.ue = U.ue;
+      o.unitStart.assign(U.unit_start, U.unit_start + U.numbers);
+      o.unitEnd.assign(U.unit_end, U.unit_end + U.numbers);
+      o.undStart.assign(U.und_start, U.und_start + U.numbers);
+      o.undEnd.assign(U.und_end, U.und_end + U.numbers);
+      o.K0.assign(U.K0, U.K0 + U.numbers);
+      I.und.push_back(o);
+    }
+    for (int q = 0; q < p->num_quads; ++q) {
+      const felis_quad& Q = p->quads[q];
+      HQuad o;
+      o.qdStart.assign(Q.qd_start, Q.qd_start + Q.numbers);
+      o.qdEnd.assign(Q.qd_end, Q.qd_end + Q.numbers);
+      o.g.assign(Q.g, Q.g + Q.numbers);
+      I.quad.push_back(o);
+    }
+    I.lat.K0 = p->K0_init; I.lat.ue = p->ue_init; I.lat.lambdaU = p->lambdaU_init;
+    I.lat.ku = 2.0 * M_PI / p->lambdaU_init; I.lat.K0_alpha = p->K0_alpha_init; I.lat.und_type = p->und_type_init;
+    I.bessel.assign(p->bessel, p->bessel + (size_t)p->bessel_rows * p->bessel_cols);
+    b->nx_max = std::max(b->nx_max, p->nx);
+    b->ny_max = std::max(b->ny_max, p->ny);
+    b->N_max = std::max(b->N_max, p->nx * p->ny);
+    b->H_max = std::max(b->H_max, p->num_harmony);
+    b->LF_max = std::max(b->LF_max, p->scl_mode * p->scf_mode);
+    b->nr_max = std::max(b->nr_max, p->nr);
+    max_step = std::max(max_step, p->max_step);
+    const int S = p->slice_n, N = p->nx * p->ny, H = p->num_harmony, M = std::max(p->nx, p->ny);
+    I.nsrc = 0;
+    for (int h = 0; h < H; ++h) {
+      I.src_plane[h] = I.nsrc;
+      I.nsrc += (p->harmony[h] & 1) ? 1 : 2;
+    }
+    b->nsrc_max = std::max(b->nsrc_max, I.nsrc);
+    cudaError_t e = cudaSuccess;
+    if (e == cudaSuccess) e = cudaMalloc(&I.src, (size_t)S * I.nsrc * N * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMalloc(&I.sbox, (size_t)S * sizeof(int4));
+    if (e == cudaSuccess) {
+      std::vector<int4> empty(S, make_int4(1, 0, 1, 0));
+      e = cudaMemcpy(I.sbox, empty.data(), S * sizeof(int4), cudaMemcpyHostToDevice);
+    }
+    const size_t un = (size_t)H * 2 * S * N;
+    if (e == cudaSuccess) e = cudaMalloc(&I.U, un * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemset(I.U, 0, un * sizeof(float2));
+    const size_t ezn = (size_t)p->scl_mode * S * p->scf_mode * p->nr;
+    if (e == cudaSuccess) e = cudaMalloc(&I.Ez, ezn * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemset(I.Ez, 0, ezn * sizeof(float2));
+    std::vector<float> bf(I.bessel.begin(), I.bessel.end());
+    if (e == cudaSuccess) e = cudaMalloc(&I.d_bessel, bf.size() * sizeof(float));
+    if (e == cudaSuccess) e = cudaMemcpy(I.d_bessel, bf.data(), bf.size() * sizeof(float), cudaMemcpyHostToDevice);
+    std::vector<double> wk(std::max(p->global_slice_n, 1), 0.0);
+    if (p->wake_e) std::copy(p->wake_e, p->wake_e + p->global_slice_n, wk.begin());
+    if (e == cudaSuccess) e = cudaMalloc(&I.wake, wk.size() * sizeof(double));
+    if (e == cudaSuccess) e = cudaMemcpy(I.wake, wk.data(), wk.size() * sizeof(double), cudaMemcpyHostToDevice);
+    std::vector<float2> tabs;
+    for (int h = 0; h < H; ++h) {
+      std::vector<float2> t;
+      adi_tables(*p, h, M, t);
+      tabs.insert(tabs.end(), t.begin(), t.end());
+    }
+    if (e == cudaSuccess) e = cudaMalloc(&I.adi, tabs.size() * sizeof(float2));
+    if (e == cudaSuccess) e = cudaMemcpy(I.adi, tabs.data(), tabs.size() * sizeof(float2), cudaMemcpyHostToDevice);
+    if (e == cudaSuccess) e = cudaMalloc(&I.part_e, (size_t)S * 2 * H * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&I.part_b, (size_t)S * (8 + 2 * H) * sizeof(double));
+    if (e == cudaSuccess) e = cudaMalloc(&I.err, ERR_SLOTS * sizeof(int));
+    if (e == cudaSuccess) e = cudaMemset(I.err, 0, ERR_SLOTS * sizeof(int));
+    if (e == cudaSuccess) e = cudaMalloc(&I.soff, (size_t)(S + 1) * sizeof(int64_t));
+    if (e == cudaSuccess) e = cudaMalloc(&I.weight, (size_t)S * sizeof(float));
+    if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
+    I.p.undulators = nullptr; I.p.quads = nullptr; I.p.bessel = nullptr; I.p.wake_e = nullptr;
+    // keep the ABC tables for later table rebuilds
+  }
+  b->hist_n = max_step + 1;
+  cudaError_t e = cudaMalloc(&b->d_inst, (size_t)n * sizeof(BInst));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_he, (size_t)n * b->hist_n * 2 * b->H_max * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_ht, (size_t)n * b->hist_n * 6 * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&b->d_hb, (size_t)n * b->hist_n * 2 * b->H_max * sizeof(double));
+  if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
+  for (auto& I : b->in) { I.p.abc_alpha = I.p.abc_alpha_p = I.p.abc_beta = I.p.abc_beta_p = nullptr; }
+  if (std::max(b->nx_max, b->ny_max) > 256) return bad(FELIS_UNSUPPORTED, "grid wider than 256 points");
+  b->push_threads = 256;
+  b->adi_ctas = 2;
+  // register budget of the push kernel: a property of the compiled kernel
+  // class (like the harmonic bound), fixed so that results never depend on
+  // tuning: 80 registers (3 CTAs of 256 per SM) up to 2 harmonics, else 128
+  b->push_minb = b->H_max <= 2 ? 3 : 2;
+  *out = b;
+  return FELIS_OK;
+}
+
+void felis_batch_destroy(felis_batch* b) {
+  if (!b) return;
+  if (b->st) cudaStreamSynchronize(b->st);
+  for (auto& I : b->in) {
+    void* ptrs[] = {I.x, I.y, I.px, I.py, I.dg, I.th, I.soff, I.weight, I.U, I.Ez, I.d_bessel, I.wake, I.adi,
+                    I.src, I.sbox, I.part_e, I.part_b, I.err};
+    for (void* q : ptrs) if (q) cudaFree(q);
+  }
+  void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_he, b->d_ht, b->d_hb};
+  for (void* q : ptrs) if (q) cudaFree(q);
+  if (b->h_err) cudaFreeHost(b->h_err);
+  if (b->st) cudaStreamDestroy(b->st);
+  delete b;
+}
+
+const char* felis_batch_last_error(const felis_batch* b) { return b ? b->err.c_str() : "null ensemble"; }
+
+felis_status felis_batch_upload_particles(felis_batch* b, int32_t inst, const double* x, const double* y,
+                                          const double* px, const double* py, const double* theta,
+                                          const double* gamma, const int64_t* slice_offsets, const double* weights) {
+  if (!b || inst < 0 || inst >= (int)b->in.size() || !slice_offsets || !weights) return bfail(b, FELIS_BAD_ARG, "bad argument");
+  Inst& I = b->in[inst];
+  const int S = I.p.slice_n;
+  if (slice_offsets[0] != 0) return bfail(b, FELIS_BAD_ARG, "slice_offsets[0] must be 0");
+  for (int s = 0; s < S; ++s)
+    if (slice_offsets[s + 1] < slice_offsets[s]) return bfail(b, FELIS_BAD_ARG, "slice_offsets must be non-decreasing");
+  const int64_t n = slice_offsets[S];
+  if (n > 0 && (!x || !y || !px || !py || !theta || !gamma)) return bfail(b, FELIS_BAD_ARG, "null particle array");
+  if (n != I.count || !I.x) {
+    float** fa[5] = {&I.x, &I.y, &I.px, &I.py, &I.dg};
+    for (auto a : fa) {
+      if (*a) cudaFree(*a);
+      *a = nullptr;
+      BCK(cudaMalloc(a, std::max<int64_t>(n, 1) * sizeof(float)));
+    }
+    if (I.th) cudaFree(I.th);
+    I.th = nullptr;
+    BCK(cudaMalloc(&I.th, std::max<int64_t>(n, 1) * sizeof(double)));
+    I.count = n;
+  }
+  b->layout_ready = false;    // work lists follow the particle counts
+  b->src_valid_it = -1;       // the next run deposits first
+  const double* src[5] = {x, y, px, py, gamma};
+  float* dst[5] = {I.x, I.y, I.px, I.py, I.dg};
+  std::vector<float> tmp(n);
+  for (int k = 0; k < 5; ++k) {
+    const double off = k == 4 ? I.p.gam_r : 0.0;  // gamma is stored as gamma - gamR
+    for (int64_t i = 0; i < n; ++i) tmp[i] = (float)(src[k][i] - off);
+    if (n) BCK(cudaMemcpy(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  }
+  if (n) BCK(cudaMemcpy(I.th, theta, n * sizeof(double), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(I.soff, slice_offsets, (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
+  std::vector<float> w(weights, weights + S);
+  BCK(cudaMemcpy(I.weight, w.data(), S * sizeof(float), cudaMemcpyHostToDevice));
+  I.uploaded = true;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_download_particles(felis_batch* b, int32_t inst, double* x, double* y, double* px,
+                                            double* py, double* theta, double* gamma) {
+  if (!b || inst < 0 || inst >= (int)b->in.size() || !b->in[inst].uploaded) return bfail(b, FELIS_BAD_ARG, "bad argument");
+  Inst& I = b->in[inst];
+  BCK(cudaStreamSynchronize(b->st));
+  const int64_t n = I.count;
+  std::vector<float> tmp(n);
+  double* dst[5] = {x, y, px, py, gamma};
+  const float* src[5] = {I.x, I.y, I.px, I.py, I.dg};
+  for (int k = 0; k < 5; ++k) {
+    if (!dst[k] || !n) continue;
+    BCK(cudaMemcpy(tmp.data(), src[k], n * sizeof(float), cudaMemcpyDeviceToHost));
+    const double off = k == 4 ? I.p.gam_r : 0.0;
+    for (int64_t i = 0; i < n; ++i) dst[k][i] = off + (double)tmp[i];
+  }
+  if (theta && n) BCK(cudaMemcpy(theta, I.th, n * sizeof(double), cudaMemcpyDeviceToHost));
+  return FELIS_OK;
+}
+
+felis_status felis_batch_upload_field(felis_batch* b, int32_t inst, int32_t hidx, int32_t pol, const double* data) {
+  if (!b || inst < 0 || inst >= (int)b->in.size() || !data) return bfail(b, FELIS_BAD_ARG, "bad argument");
+  Inst& I = b->in[inst];
+  if (hidx < 0 || hidx >= I.p.num_harmony || pol < 0 || pol > 1) return bfail(b, FELIS_BAD_ARG, "bad harmonic/pol");
+  const int S = I.p.slice_n;
+  const size_t N = (size_t)I.p.nx * I.p.ny;
+  std::vector<float2> plane(N);
+  for (int s = 0; s < S; ++s) {
+    const double* src = data + 2 * (size_t)(s + 1) * N;
+    for (size_t k = 0; k < N; ++k) plane[k] = make_float2((float)src[2 * k], (float)src[2 * k + 1]);
+    const int phys = (s + I.ring_base) % S;
+    BCK(cudaMemcpy(I.U + ((size_t)(hidx * 2 + pol) * S + phys) * N, plane.data(), N * sizeof(float2), cudaMemcpyHostToDevice));
+  }
+  return FELIS_OK;
+}
+
+felis_status felis_batch_download_field(felis_batch* b, int32_t inst, int32_t hidx, int32_t pol, double* data) {
+  if (!b || inst < 0 || inst >= (int)b->in.size() || !data) return bfail(b, FELIS_BAD_ARG, "bad argument");
+  Inst& I = b->in[inst];
+  if (hidx < 0 || hidx >= I.p.num_harmony || pol < 0 || pol > 1) return bfail(b, FELIS_BAD_ARG, "bad harmonic/pol");
+  BCK(cudaStreamSynchronize(b->st));
+  const int S = I.p.slice_n;
+  const size_t N = (size_t)I.p.nx * I.p.ny;
+  std::vector<float2> plane(N);
+  memset(data, 0, 2 * (size_t)(S + 2) * N * sizeof(double));
+  for (int s = 0; s < S; ++s) {
+    const int phys = (s + I.ring_base) % S;
+    BCK(cudaMemcpy(plane.data(), I.U + ((size_t)(hidx * 2 + pol) * S + phys) * N, N * sizeof(float2), cudaMemcpyDeviceToHost));
+    double* dst = data + 2 * (size_t)(s + 1) * N;
+    for (size_t k = 0; k < N; ++k) { dst[2 * k] = plane[k].x; dst[2 * k + 1] = plane[k].y; }
+  }
+  return FELIS_OK;
+}
+
+felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas) {
+  if (!b || (push_threads != 128 && push_threads != 256) || adi_ctas < 1 || adi_ctas > 2)
+    return bfail(b, FELIS_BAD_ARG, "bad launch shape (push threads 128 or 256, ADI CTAs per SM 1 or 2)");
+  b->push_threads = push_threads;
+  b->adi_ctas = adi_ctas;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas, int32_t* push_regs) {
+  if (!b) return FELIS_BAD_ARG;
+  if (push_threads) *push_threads = b->push_threads;
+  if (adi_ctas) *adi_ctas = b->adi_ctas;
+  if (push_regs) *push_regs = b->push_minb >= 3 ? 80 : 128;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1) {
+  if (!b || it1 < it0) return FELIS_BAD_ARG;
+  if (it1 == it0) return FELIS_OK;
+  felis_status s = prepare(b);
+  if (s != FELIS_OK) return s;
+  s = ensure_launch(b);
+  if (s != FELIS_OK) return s;
+  const int n = (int)b->in.size();
+  const int steps = it1 - it0;
+  // snapshot of the host lattice state: a failed run leaves it unchanged
+  std::vector<std::pair<felis_lattice, int>> saved;
+  for (auto& I : b->in) saved.push_back(std::make_pair(I.lat, I.ring_base));
+  auto restore = [&]() {
+    for (size_t k = 0; k < b->in.size(); ++k) { b->in[k].lat = saved[k].first; b->in[k].ring_base = saved[k].second; }
+  };
+  std::vector<BStep> tab;
+  s = build_steps(b, it0, it1, tab);
+  if (s != FELIS_OK) { restore(); return s; }
+  if (steps > b->steps_cap) {
+    if (b->d_steps) cudaFree(b->d_steps);
+    b->d_steps = nullptr;
+    b->steps_cap = steps;
+    BCK(cudaMalloc(&b->d_steps, (size_t)(b->steps_cap + 1) * n * sizeof(BStep)));
+  }
+  BCK(cudaMemcpy(b->d_steps, tab.data(), tab.size() * sizeof(BStep), cudaMemcpyHostToDevice));
+  BCK(cudaStreamSynchronize(b->st));
+  const bool deposit0 = b->src_valid_it != it0;
+  cudaGraph_t graph = nullptr;
+  cudaGraphExec_t exec = nullptr;
+  BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  s = enqueue_run(b, it0, it1, deposit0);
+  cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
+  if (s != FELIS_OK) { if (graph) cudaGraphDestroy(graph); restore(); return s; }
+  if (ce != cudaSuccess) { restore(); return bfail(b, FELIS_CUDA_ERROR, std::string("capture: ") + cudaGetErrorString(ce)); }
+  ce = cudaGraphInstantiate(&exec, graph, 0);
+  cudaEvent_t e0 = nullptr, e1 = nullptr;
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e0);
+  if (ce == cudaSuccess) ce = cudaEventCreate(&e1);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e0, b->st);
+  if (ce == cudaSuccess) ce = cudaGraphLaunch(exec, b->st);
+  if (ce == cudaSuccess) ce = cudaEventRecord(e1, b->st);
+  if (ce == cudaSuccess) ce = cudaStreamSynchronize(b->st);
+  if (ce == cudaSuccess) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, e0, e1);
+    b->last_run_ms = ms;
+  }
+  if (e0) cudaEventDestroy(e0);
+  if (e1) cudaEventDestroy(e1);
+  if (exec) cudaGraphExecDestroy(exec);
+  cudaGraphDestroy(graph);
+  if (ce != cudaSuccess) return bfail(b, FELIS_CUDA_ERROR, std::string("graph run: ") + cudaGetErrorString(ce));
+  b->src_valid_it = it1;
+  return check_batch_err(b);
+}
+
+// Online launch-shape tuner.  The particle state and the fields after a step
+// do not depend on the launch shape (fixed-point deposit, one thread per ADI
+// row or column, one thread per particle), so the tuner advances the
+// ensemble through real iterations, each candidate shape for `steps` of
+// them, and keeps the fastest.  Results are cached per ensemble geometry.
+felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it) {
+  if (!b || steps < 1 || !next_it) return FELIS_BAD_ARG;
+  *next_it = it0;
+  static std::map<std::tuple<int, int, int, int, int, int, int64_t>, std::pair<int, int>> cache;
+  int64_t total = 0;
+  for (auto& I : b->in) total += I.count;
+  const auto key = std::make_tuple(b->nx_max, b->ny_max, b->H_max, b->LF_max, b->nr_max, (int)b->in.size(),
+                                   total >> 16);
+  auto hit = cache.find(key);
+  if (hit != cache.end()) {
+    std::tie(b->push_threads, b->adi_ctas) = hit->second;
+    return FELIS_OK;
+  }
+  double best = 1e300;
+  std::pair<int, int> pick(b->push_threads, b->adi_ctas);
+  int it = it0;
+  // the first run after an upload also deposits: spend it outside the timing
+  if (b->src_valid_it != it) {
+    felis_status s = felis_batch_run(b, it, it + 1);
+    if (s != FELIS_OK) return s;
+    it += 1;
+  }
+  for (int t : {128, 256})
+    for (int c : {1, 2}) {
+      b->push_threads = t;
+      b->adi_ctas = c;
+      felis_status s = felis_batch_run(b, it, it + steps);
+      if (s != FELIS_OK) return s;
+      it += steps;
+      const double per = b->last_run_ms / steps;
+      if (per < best) { best = per; pick = std::make_pair(t, c); }
+    }
+  std::tie(b->push_threads, b->adi_ctas) = pick;
+  cache[key] = pick;
+  *next_it = it;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_last_run_ms(felis_batch* b, double* ms) {
+  if (!b || !ms) return FELIS_BAD_ARG;
+  *ms = b->last_run_ms;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t it0, int32_t it1, double* energy,
+                                         double* twiss, double* bfactor) {
+  if (!b || inst < 0 || inst >= (int)b->in.size() || it0 < 0 || it1 < it0 || it1 > b->hist_n) return bfail(b, FELIS_BAD_ARG, "bad range");
+  BCK(cudaStreamSynchronize(b->st));
+  const int H = b->in[inst].p.num_harmony, se = 2 * b->H_max, sb = 2 * b->H_max;
+  for (int it = it0; it < it1; ++it) {
+    if (energy) BCK(cudaMemcpy(energy + (size_t)(it - it0) * 2 * H, b->d_he + (size_t)inst * se * b->hist_n + (size_t)it * se, 2 * H * sizeof(double), cudaMemcpyDeviceToHost));
+    if (twiss) BCK(cudaMemcpy(twiss + (size_t)(it - it0) * 6, b->d_ht + (size_t)inst * 6 * b->hist_n + (size_t)it * 6, 6 * sizeof(double), cudaMemcpyDeviceToHost));
+    if (bfactor) BCK(cudaMemcpy(bfactor + (size_t)(it - it0) * 2 * H, b->d_hb + (size_t)inst * sb * b->hist_n + (size_t)it * sb, 2 * H * sizeof(double), cudaMemcpyDeviceToHost));
+  }
+  return FELIS_OK;
+}
+
+}  // extern "C"

@@ -1,0 +1,831 @@
+// Mixed-precision ensemble kernels: two launches per iteration.
+//
+//   k_batch_adi   one CTA per field plane (instance, slice, harmonic,
+//                 polarisation): the ADI of solveField.cpp:80-185 in FP32 with
+//                 the plane, the recurrence tables and the slice's source box
+//                 staged in shared memory; emits the plane's |U|^2 sum.
+//   k_batch_push  one CTA per (instance, slice): both transverse half-pushes,
+//                 push_theta_gamma or the drift, the theta wrap, the beam
+//                 partial sums (particlePush.cpp, rearrangeParticles.cpp,
+//                 twiss.cpp, saveFile.cpp), then the source deposit and the
+//                 radial Ez solve of the next iteration's solveField
+//                 (solveField.cpp:233-399) from the pushed particles, which the
+//                 CTA reads back from L2.
+//
+// Every (instance, slice) of an iteration is independent of the others: the
+// slippage shift only renames planes (ring buffer), and the CTA of the last
+// slice clears the plane that becomes the new first slice.
+//
+// The deposit accumulates 32-bit fixed-point integers (shared-memory
+// atomics), so the sums do not depend on the order of the atomics: a run is
+// reproducible bit for bit and independent of the launch shape and of the
+// other instances.
+#include "batch.cuh"
+
+namespace felis {
+
+namespace {
+
+constexpr double kTwoPi = 6.283185307179586476925286766559;
+
+__device__ __forceinline__ float2 cm(float2 a, float2 b) {
+  return make_float2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x);
+}
+__device__ __forceinline__ float2 cs(float2 a, float s) { return make_float2(a.x * s, a.y * s); }
+__device__ __forceinline__ float2 cad(float2 a, float2 b) { return make_float2(a.x + b.x, a.y + b.y); }
+__device__ __forceinline__ float2 csb(float2 a, float2 b) { return make_float2(a.x - b.x, a.y - b.y); }
+
+// e^{i x} for an FP32 phase of moderate size (|x| < 2^14): Cody-Waite
+// reduction by 2 pi with a two-part constant (6.28125 is exact in 9 bits, so
+// k * 6.28125 is exact), then the hardware sin/cos on [-pi, pi].
+__device__ __forceinline__ float2 expif(float x) {
+  const float k = rintf(x * 0.159154943091895336f);
+  float r = fmaf(-k, 6.28125f, x);
+  r = fmaf(-k, 1.93530717958647692e-3f, r);
+  float s, c;
+  __sincosf(r, &s, &c);
+  return make_float2(c, s);
+}
+
+// theta (FP64, up to 2 pi numSlice) reduced to [-pi, pi] in FP32.
+__device__ __forceinline__ float theta_red(double th) { return (float)(th - kTwoPi * rint(th * (1.0 / kTwoPi))); }
+
+__device__ __forceinline__ double block_sum_d(double v, double* red) {
+  for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  double t = 0.0;
+  if (threadIdx.x == 0)
+    for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t += red[k];
+  return t;
+}
+
+__device__ __forceinline__ float block_max_f(float v, float* red) {
+  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  float t = 0.f;
+  for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t = fmaxf(t, red[k]);
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ int block_min_i(int v, int* red) {
+  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
+  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
+  __syncthreads();
+  if (l == 0) red[w] = v;
+  __syncthreads();
+  int t = 1 << 30;
+  for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t = min(t, red[k]);
+  __syncthreads();
+  return t;
+}
+
+__device__ __forceinline__ float bj(const BInst& I, int row, int col) {
+  row = row < 0 ? 0 : (row >= I.bn ? I.bn - 1 : row);
+  return __ldg(I.bessel + row * I.bcols + col);
+}
+
+// fx, fy of harmonic H for the push (sign conventions of
+// particlePush.cpp:336-360) or the deposit (solveField.cpp:277-300).
+__device__ __forceinline__ void ffac(const BInst& I, int H, float xi, float xi2, float K0a, float2 eP, bool deposit,
+                                     float2* fx, float2* fy) {
+  const float x = (float)H * xi / (float)I.dBessel;
+  const int idx = (int)x;
+  const float w1 = x - (float)idx, w0 = 1.f - w1;
+  const float2 eM = make_float2(eP.x, -eP.y);
+  if (H & 1) {
+    const float sign = (((H - 1) / 2) % 2 == 0) ? 1.f : -1.f;
+    const float J1 = bj(I, idx, (H - 1) / 2) * w0 + bj(I, idx + 1, (H - 1) / 2) * w1;
+    const float J2 = bj(I, idx, (H + 1) / 2) * w0 + bj(I, idx + 1, (H + 1) / 2) * w1;
+    if (deposit) { *fx = make_float2(sign * (J1 - K0a * J2), 0.f); *fy = make_float2(sign * (J1 + K0a * J2), 0.f); }
+    else { *fx = make_float2(sign * (K0a * J1 - J2), 0.f); *fy = make_float2(sign * (K0a * J1 + J2), 0.f); }
+  } else {
+    const float sign = ((H / 2) % 2 == 0) ? 1.f : -1.f;
+    const float J1 = bj(I, idx, (H - 2) / 2) * w0 + bj(I, idx + 1, (H - 2) / 2) * w1;
+    const float J2 = bj(I, idx, H / 2) * w0 + bj(I, idx + 1, H / 2) * w1;
+    const float J3 = bj(I, idx, (H + 2) / 2) * w0 + bj(I, idx + 1, (H + 2) / 2) * w1;
+    const float sx = sign * xi2 * H * 0.5f;
+    if (deposit) {
+      *fx = cs(cad(cs(eM, J1 - K0a * J2), cs(eP, J2 - K0a * J3)), sx);
+      *fy = cs(cad(cs(eM, J1 + K0a * J2), cs(eP, J2 + K0a * J3)), sx);
+    } else {
+      *fx = cs(cad(cs(eP, K0a * J1 - J2), cs(eM, K0a * J2 - J3)), sx);
+      *fy = cs(cad(cs(eP, K0a * J1 + J2), cs(eM, K0a * J2 + J3)), sx);
+    }
+  }
+}
+
+// xi2 and e^{i (B - Phi/2)} of particlePush.cpp:272-279 / solveField.cpp:259-266.
+__device__ __forceinline__ void pol_phase(float K0, float ue, float K0a, float Phi_half, float px, float py,
+                                          float* xi2, float2* eP) {
+  *xi2 = 1.41421356f * K0 / (1.f + K0 * K0 * 0.5f * (1.f + ue * ue)) *
+         sqrtf((1.f + K0a) * (px * px + ue * ue * py * py) + (1.f - K0a) * (px * px * ue * ue + py * py));
+  const float B = atanf(2.f * K0a * ue * (px - py) /
+                        ((1.f + K0a) * (px + ue * ue * py) + (1.f - K0a) * (px * ue * ue + py)));
+  *eP = expif(B - Phi_half);
+}
+
+// Both transverse half-pushes of particlePush.cpp:82-110.  For a fixed
+// gamma they are RK4 steps of a linear ODE, i.e. the state is multiplied by
+// the RK4 polynomial of the step matrix; the host forms the product of the
+// two half-step maps as a function of a = 1/gamma to second order about
+// 1/gamR: s' = s + D0 s + da (M1 s + da M2 s), da = 1/gamma - 1/gamR.
+__device__ __forceinline__ void transverse_map(const BStep& T, float& x, float& y, float& px, float& py, float da) {
+  const float s0 = x, s1 = y, s2 = px, s3 = py;
+  float o[4];
+#pragma unroll
+  for (int r = 0; r < 4; ++r) {
+    const float* D = T.tD0 + 4 * r;
+    const float* A = T.tM1 + 4 * r;
+    const float* B = T.tM2 + 4 * r;
+    const float m2 = B[0] * s0 + B[1] * s1 + B[2] * s2 + B[3] * s3;
+    const float m1 = A[0] * s0 + A[1] * s1 + A[2] * s2 + A[3] * s3 + da * m2;
+    const float d0 = D[0] * s0 + D[1] * s1 + D[2] * s2 + D[3] * s3;
+    o[r] = d0 + da * m1;
+  }
+  x = s0 + o[0]; y = s1 + o[1]; px = s2 + o[2]; py = s3 + o[3];
+}
+
+// Asynchronous 8-byte global -> shared copies (all in flight at once), then
+// one wait for every copy of the thread.
+__device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
+  const unsigned d = (unsigned)__cvta_generic_to_shared(dst_smem);
+  asm volatile("cp.async.ca.shared.global [%0], [%1], 8;\n" ::"r"(d), "l"(src) : "memory");
+}
+__device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
+
+// ---- fixed-point accumulation ------------------------------------------------
+constexpr int kAccBits = 31;
+
+// v / q rounded to an integer; q is a power of two, so v * (1/q) is exact in
+// FP32 and only the rounding to an integer is inexact
+__device__ __forceinline__ acc_t fix(float v, float inv_q) { return (acc_t)__float2int_rn(v * inv_q); }
+__device__ __forceinline__ void acc_add(acc_t* p, acc_t v) {
+  if (v != 0) atomicAdd(p, v);
+}
+// quantum 2^e with bound / 2^e < 2^(kAccBits - 1): the rounded terms add at
+// most half a quantum each on top of the exact sum, so no sum overflows
+__device__ __forceinline__ float quantum(float bound) {
+  if (!(bound > 0.f)) return 1.f;
+  const int e = max(ilogbf(bound) + 2 - kAccBits, -120);  // 1/q stays a finite float
+  return ldexpf(1.f, e);
+}
+
+// ============================================================================
+// ADI (solveField.cpp:80-185), one CTA per plane, thread per row / column.
+// ============================================================================
+__global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ double redd[8];
+  const int4 wi = a.work[blockIdx.x];
+  const BInst& I = a.inst[wi.x];
+  const BStep& T = a.step[wi.x];
+  const int s = wi.y, hp = wi.z, h = hp >> 1, pol = hp & 1;
+  const int S = I.S, nx = I.nx, ny = I.ny, N = I.N, nxp = I.nxp, Mx = nx > ny ? nx : ny;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  float2* U = I.U + ((size_t)hp * S + (s + T.ring_base) % S) * N;
+  const float2* ad = I.adi_c + (size_t)h * 12 * Mx;
+  float2* pl = reinterpret_cast<float2*>(sm);
+  float2* tb = pl + (size_t)ny * nxp;  // 6 recurrence tables of Mx complex
+  float2* ssrc = tb + 6 * Mx;
+  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+  for (int k = tid; k < 6 * Mx; k += nt) cp_async8(tb + k, ad + k);
+  for (int r = warp; r < ny; r += nwarp)
+    for (int c = lane; c < nx; c += 32) cp_async8(pl + r * nxp + c, U + r * nx + c);
+  // source of this plane: odd harmonic -eta f m (one plane m for both
+  // polarisations), even harmonic its own plane
+  int bi0 = 1, bi1 = 0, bj0 = 1, bj1 = 0, bw = 0;
+  const float2* Sc = nullptr;
+  const float2 sfac = T.sfac[h][pol];
+  if (T.current) {
+    const int4 b = I.sbox[s];
+    bi0 = b.x; bi1 = b.y; bj0 = b.z; bj1 = b.w;
+    bw = bi1 - bi0 + 1;
+    const int cells = (bw > 0 && bj1 >= bj0) ? bw * (bj1 - bj0 + 1) : 0;
+    const int p = I.src_plane[h] + ((I.harmony[h] & 1) ? 0 : pol);
+    const float2* g = I.src + ((size_t)s * I.nsrc + p) * N;
+    const size_t used = ((size_t)ny * nxp + 6 * (size_t)Mx) * sizeof(float2);
+    if (cells > 0 && used + (size_t)cells * sizeof(float2) <= (size_t)a.smem_bytes) {
+      for (int k = tid; k < cells; k += nt) cp_async8(ssrc + k, g + k);
+      Sc = ssrc;
+    } else if (cells > 0) {
+      Sc = g;
+    } else {
+      bi0 = 1; bi1 = 0;
+    }
+  }
+  const bool src = Sc != nullptr;
+  cp_async_wait_all();
+  __syncthreads();
+  const float2* px_ = tb;             // 1/alphaP (last: 1)
+  const float2* mx_ = tb + Mx;        // alpha / (alphaP CC[i-1])
+  const float2* rx_ = tb + 2 * Mx;    // 1/CC
+  const float2* py_ = tb + 3 * Mx;
+  const float2* my_ = tb + 4 * Mx;
+  const float2* ry_ = tb + 5 * Mx;
+  // x sweep (thread per row), one barrier per column so that every row has
+  // read column i of U before any row overwrites it
+  const int j = tid;
+  const bool row = j >= 1 && j <= ny - 2;
+  float2 DD = make_float2(0.f, 0.f);
+  float2 ra = make_float2(0, 0), rb = ra, rc = ra, edge0 = ra, edge1 = ra;
+  if (row) {
+    ra = ad[6 * Mx + j]; rb = ad[7 * Mx + j]; rc = ad[8 * Mx + j];  // -betaP, H+betaP+beta, beta
+    edge0 = pl[j * nxp]; edge1 = pl[j * nxp + nx - 1];             // the ADI keeps the edge columns
+  }
+  const bool rowin = row && src && j >= bj0 && j <= bj1;
+  for (int i = 1; i <= nx - 2; ++i) {
+    float2 up = make_float2(0, 0), u0 = up, um = up, sv = up;
+    if (row) {
+      up = pl[(j + 1) * nxp + i]; u0 = pl[j * nxp + i]; um = pl[(j - 1) * nxp + i];
+      if (rowin && i >= bi0 && i <= bi1) sv = cm(sfac, Sc[(j - bj0) * bw + (i - bi0)]);
+    }
+    __syncthreads();
+    if (row) {
+      const float2 t = cad(cad(cm(ra, up), cm(rb, u0)), csb(sv, cm(rc, um)));
+      DD = csb(cm(t, px_[i]), cm(mx_[i], DD));
+      pl[j * nxp + i] = DD;
+    }
+  }
+  if (row) {
+    float2 Uc = cm(DD, rx_[nx - 2]);
+    pl[j * nxp + nx - 2] = Uc;
+    for (int i = nx - 3; i > 0; --i) {
+      Uc = cm(csb(pl[j * nxp + i], Uc), rx_[i]);
+      pl[j * nxp + i] = Uc;
+    }
+    pl[j * nxp] = make_float2(0.f, 0.f);
+    pl[j * nxp + nx - 1] = make_float2(0.f, 0.f);
+  }
+  __syncthreads();
+  // y sweep (thread per column), one barrier per row
+  const int i = tid;
+  const bool col = i >= 1 && i <= nx - 2;
+  if (col) { ra = ad[9 * Mx + i]; rb = ad[10 * Mx + i]; rc = ad[11 * Mx + i]; }  // -alphaP, H+alphaP+alpha, alpha
+  const bool colin = col && src && i >= bi0 && i <= bi1;
+  DD = make_float2(0.f, 0.f);
+  for (int jr = 1; jr <= ny - 2; ++jr) {
+    float2 up = make_float2(0, 0), u0 = up, um = up, sv = up;
+    if (col) {
+      up = pl[jr * nxp + i + 1]; u0 = pl[jr * nxp + i]; um = pl[jr * nxp + i - 1];
+      if (colin && jr >= bj0 && jr <= bj1) sv = cm(sfac, Sc[(jr - bj0) * bw + (i - bi0)]);
+    }
+    __syncthreads();
+    if (col) {
+      const float2 t = cad(cad(cm(ra, up), cm(rb, u0)), csb(sv, cm(rc, um)));
+      DD = csb(cm(t, py_[jr]), cm(my_[jr], DD));
+      pl[jr * nxp + i] = DD;
+    }
+  }
+  if (col) {
+    float2 Un = cm(DD, ry_[ny - 2]);
+    pl[(ny - 2) * nxp + i] = Un;
+    for (int jr = ny - 3; jr > 0; --jr) {
+      Un = cm(csb(pl[jr * nxp + i], Un), ry_[jr]);
+      pl[jr * nxp + i] = Un;
+    }
+  }
+  __syncthreads();
+  if (row) { pl[j * nxp] = edge0; pl[j * nxp + nx - 1] = edge1; }
+  __syncthreads();
+  // write the plane back and sum |U|^2 over it (edge rows and columns keep
+  // their old values: the ADI never writes them)
+  double e = 0.0;
+  for (int r = warp; r < ny; r += nwarp)
+    for (int c = lane; c < nx; c += 32) {
+      const float2 v = pl[r * nxp + c];
+      U[r * nx + c] = v;
+      e += (double)(v.x * v.x + v.y * v.y);
+    }
+  const double et = block_sum_d(e, redd);
+  if (tid == 0) I.part_e[(size_t)s * 2 * I.H + hp] = et;
+}
+
+// ============================================================================
+// Push and the next deposit, one CTA per (instance, slice).
+// ============================================================================
+template <int HM, int MINB>
+__global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
+  extern __shared__ __align__(16) unsigned char sm[];
+  __shared__ double redd[8];
+  __shared__ float redf[8];
+  __shared__ int redi[8];
+  const int4 wi = a.work[blockIdx.x];
+  const BInst& I = a.inst[wi.x];
+  const BStep& T = a.step[wi.x];
+  const int s = wi.y;
+  const int tid = threadIdx.x, nt = blockDim.x;
+  const int S = I.S, nx = I.nx, ny = I.ny, N = I.N, H = I.H, nr = I.nr, L = I.L, F = I.F, LF = L * F;
+  const int64_t p0 = I.soff[s], p1 = I.soff[s + 1];
+  const int P = (int)(p1 - p0);
+  const float weight = I.weight[s];
+  const float gRf = (float)I.gamR, igR = (float)(1.0 / I.gamR);
+  const float minX = (float)I.minX, minY = (float)I.minY, idx_ = (float)(1.0 / I.dx), idy_ = (float)(1.0 / I.dy);
+  const float dr = (float)I.dr, idr2 = (float)(1.0 / (I.dr * I.dr));
+  const int plane = (s + T.ring_base) % S;
+  bool has_even = false;
+  int Hmax = 1;
+#pragma unroll
+  for (int h = 0; h < HM; ++h)
+    if (h < H) { has_even |= (I.harmony[h] % 2 == 0); Hmax = max(Hmax, I.harmony[h]); }
+  // shared memory: Ez of the slice | radial accumulators | 2D accumulators
+  float2* sEz = reinterpret_cast<float2*>(sm);
+  const size_t o1 = ((size_t)LF * nr * sizeof(float2) + 15) & ~(size_t)15;
+  const size_t o2 = o1 + (((size_t)LF * nr * 2 * sizeof(acc_t) + 15) & ~(size_t)15);
+  acc_t* sR = reinterpret_cast<acc_t*>(sm + o1);
+  unsigned char* area = sm + o2;
+  const size_t area_bytes = (size_t)a.smem_bytes - o2;
+  const bool push = a.mode == BATCH_PUSH;
+  const bool dep = T.deposit != 0 && P > 0;
+  const BDep& D = T.dep;
+  // deposit statistics of the (pushed) beam: cell box and fixed-point bounds
+  int ci0 = 1 << 30, ci1 = -(1 << 30), cj0 = 1 << 30, cj1 = -(1 << 30);
+  float bmax = 0.f, rmax = 0.f;
+  auto stats = [&](float x, float y, float px, float py, float g) {
+    const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+    const int ii = (int)gx, jj = (int)gy;
+    if (ii >= 0 && ii < nx && jj >= 0 && jj < ny) {
+      ci0 = min(ci0, ii); ci1 = max(ci1, ii); cj0 = min(cj0, jj); cj1 = max(cj1, jj);
+      const float w1 = gx - ii, v1 = gy - jj;
+      const float wm = fmaxf(fabsf(w1), fabsf(1.f - w1)) * fmaxf(fabsf(v1), fabsf(1.f - v1));
+      float fb = 1.f;  // odd harmonics accumulate w mc (|f| applied later)
+      if (has_even) {
+        float xi2;
+        float2 eP;
+        pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
+        fb = fmaxf(fb, 2.f * xi2 * Hmax);
+      }
+      bmax = fmaxf(bmax, wm * fb / fabsf(g));
+    }
+    const float r = sqrtf(x * x + y * y);
+    const int ir = (int)(r / dr + 0.5f);
+    if (ir >= 0 && ir < nr) {
+      const float wr1 = ir > 0 ? fabsf((r * r * idr2 - (float)(ir * ir)) / (2.f * ir)) : 0.f;
+      rmax = fmaxf(rmax, (1.f + wr1) / (ir > 0 ? (float)ir : 1.f));
+    }
+  };
+  // ================= pass 1: push (particlePush.cpp) =================
+  if (push) {
+    for (int k = tid; k < LF * nr; k += nt) {
+      const int l = k / (F * nr), rest = k % (F * nr);
+      sEz[k] = I.Ez[((size_t)l * S + s) * F * nr + rest];
+    }
+    __syncthreads();
+    const int stride = 7 + 2 * H + 1;
+    double acc7[7] = {0, 0, 0, 0, 0, 0, 0};
+    double bre[HM], bim[HM];
+#pragma unroll
+    for (int h = 0; h < HM; ++h) { bre[h] = 0.0; bim[h] = 0.0; }
+    double wsum = 0.0;
+    const double wakeE = I.wakeOn ? I.wakeE[s + I.minI] / (K_MC2 * 1.0e6) : 0.0;
+    const float dwake = (float)(I.dz * wakeE);
+    const double dTh = I.numSlice * 2 * M_PI, idTh = 1.0 / dTh;
+    const float dzf = (float)I.dz;
+    const float2* Ubase = I.U + (size_t)plane * N;
+    const size_t hpstride = (size_t)S * N;
+    int bad_over = 0, bad_range = 0, bad_nan = 0;
+    for (int q = tid; q < P; q += nt) {
+      const int64_t n = p0 + q;
+      float x = I.x[n], y = I.y[n], px = I.px[n], py = I.py[n], dg = I.dg[n];
+      double th = I.th[n];
+      const float g = gRf + dg;
+      transverse_map(T, x, y, px, py, -dg * igR / g);
+      const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+      const int ii = (int)gx, jj = (int)gy;
+      if (ii >= 0 && ii < nx - 1 && jj >= 0 && jj < ny - 1) {
+        const float wx1 = gx - ii, wy1 = gy - jj, wx0 = 1.f - wx1, wy0 = 1.f - wy1;
+        float2 Ux[HM], Uy[HM];
+        float sumU2 = 0.f;
+#pragma unroll
+        for (int h = 0; h < HM; ++h) {
+          if (h >= H) break;
+          const float2* Px = Ubase + (2 * h) * hpstride + jj * nx + ii;
+          const float2* Py = Px + hpstride;
+          Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[nx], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[nx + 1], wx1 * wy1)));
+          Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[nx], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[nx + 1], wx1 * wy1)));
+          const float Hh = (float)I.harmony[h];
+          sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
+        }
+        if (!T.drift) {
+          const float r2 = x * x + y * y;
+          const float k2 = px * px + py * py + T.c1 * T.c2 * r2;  // K2 - Q0
+          const float xi = T.cxi * igR * igR / ((1.f + dg * igR) * (1.f + dg * igR));
+          float xi2 = 0.f;
+          float2 eP = make_float2(1.f, 0.f);
+          if (has_even) pol_phase(T.K0, T.ue, T.K0a, T.Phi_half, px, py, &xi2, &eP);
+#pragma unroll
+          for (int h = 0; h < HM; ++h) {  // fold the polarisation factors into the field
+            if (h >= H) break;
+            float2 fx, fy;
+            ffac(I, I.harmony[h], xi, xi2, T.K0a, eP, false, &fx, &fy);
+            Ux[h] = cm(cm(T.etaX, fx), Ux[h]);
+            Uy[h] = cm(cm(T.etaY, fy), Uy[h]);
+          }
+          const float r = sqrtf(r2);
+          const int ir = (int)(r / dr + 0.5f);
+          float2 Em[4] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+          if (ir >= 0 && ir < nr) {
+            const float wr1 = ir > 0 ? (r2 * idr2 - (float)(ir * ir)) / (2.f * ir) : 1.f;
+            const float wr0 = ir > 0 ? 1.f - wr1 : 1.f;
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+              if (l >= L) break;
+              for (int f = 0; f < F; ++f) {
+                const float2 a0 = sEz[(l * F + f) * nr + ir];
+                const float2 a1 = (ir + 1 < nr) ? sEz[(l * F + f) * nr + ir + 1] : make_float2(0.f, 0.f);
+                Em[l] = cad(Em[l], cad(cs(a0, wr0), cs(a1, wr1)));
+              }
+            }
+          }
+          // RK4 in z of (theta, gamma); the theta slope in FP32 relative to
+          // the resonance (BStep), theta itself accumulated in FP64
+          const float thr = theta_red(th);
+          float kth_prev = 0.f, kth_sum = 0.f, kg_prev = 0.f, kg_sum = 0.f;
+#pragma unroll
+          for (int m = 1; m < 5; ++m) {
+            const float clm = (m == 1) ? 0.f : (m == 4 ? 1.f : 0.5f);
+            const float tm = thr + dzf * kth_prev * clm;
+            const float dgm = dg + dzf * kg_prev * clm;
+            const float d = dgm * igR;
+            const float inv2 = 1.f / ((1.f + d) * (1.f + d));
+            float sumEz = 0.f, sumTh = 0.f, sumG = 0.f;
+#pragma unroll
+            for (int l = 0; l < 4; ++l) {
+              if (l >= L) break;
+              const float2 e = expif((l + 1.f) * tm);
+              sumEz += 2.f * (Em[l].x * e.x - Em[l].y * e.y);
+            }
+#pragma unroll
+            for (int h = 0; h < HM; ++h) {
+              if (h >= H) break;
+              const float Hh = (float)I.harmony[h];
+              const float2 e = expif(Hh * (tm + T.Phi_half));
+              const float2 tc = cm(e, csb(Ux[h], Uy[h]));
+              sumTh += -tc.y / Hh;
+              sumG += tc.x;
+            }
+            sumG *= 0.5f / (gRf + dgm);
+            kth_prev = T.R0 + T.AQ0 * (d * (2.f + d) * inv2) - T.A0 * inv2 * (k2 + sumU2 + T.K0 * T.sq * sumTh);
+            kg_prev = T.ksK0 * T.sq * sumG + T.e_mc2 * sumEz;
+            const float wgt = (m == 1 || m == 4) ? 1.f : 2.f;
+            kth_sum += wgt * kth_prev;
+            kg_sum += wgt * kg_prev;
+          }
+          const float dth = dzf / 6.f * kth_sum;
+          if (dth > T.dPhi || dth < -T.dPhi) bad_over = 1;
+          th += (double)dth;
+          dg += dzf / 6.f * kg_sum - dwake;
+        } else {
+          const double K2 = 1.0 + (double)px * px + (double)py * py;
+          const double tmp = T.ku - T.A0d * (K2 + sumU2);
+          th += tmp * I.dz;
+          th -= I.dz * wakeE;
+        }
+      }
+      // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
+      if (th >= dTh || th < 0) {
+        th -= dTh * floor(th * idTh);
+        if (th >= dTh) th -= dTh;
+        else if (th < 0) th += dTh;
+      }
+      if (th > dTh || th < 0) bad_range = 1;
+      if (!(dg - dg == 0.f) || !(th - th == 0.0) || !(x - x == 0.f)) bad_nan = 1;
+      I.x[n] = x; I.y[n] = y; I.px[n] = px; I.py[n] = py; I.dg[n] = dg; I.th[n] = th;
+      // twiss / bFactor partial sums of the new state (twiss.cpp, saveFile.cpp)
+      const float ig = 1.f / (gRf + dg), xp = px * ig, yp = py * ig;
+      acc7[0] += (double)(x * x); acc7[1] += (double)(y * y); acc7[2] += (double)(xp * xp);
+      acc7[3] += (double)(yp * yp); acc7[4] += (double)(x * xp); acc7[5] += (double)(y * yp); acc7[6] += 1.0;
+      const float thn = theta_red(th);
+#pragma unroll
+      for (int h = 0; h < HM; ++h) {
+        if (h >= H) break;
+        const float2 e = expif((float)I.harmony[h] * thn);
+        bre[h] += (double)e.x * weight;
+        bim[h] += (double)e.y * weight;
+      }
+      wsum += weight;
+      if (dep) stats(x, y, px, py, gRf + dg);
+    }
+    if (bad_over) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
+    if (bad_range) atomicOr(I.err + ERR_OUT_OF_RANGE, 1);
+    if (bad_nan) atomicOr(I.err + ERR_NAN, 1);
+    double* out = I.part_b + (size_t)s * stride;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const double t = block_sum_d(acc7[k], redd);
+      if (tid == 0) out[k] = t;
+    }
+#pragma unroll
+    for (int h = 0; h < HM; ++h) {
+      if (h >= H) break;
+      const double tr = block_sum_d(bre[h], redd), ti = block_sum_d(bim[h], redd);
+      if (tid == 0) { out[7 + 2 * h] = tr; out[8 + 2 * h] = ti; }
+    }
+    const double tw = block_sum_d(wsum, redd);
+    if (tid == 0) out[7 + 2 * H] = tw;
+    // slippage shift: the plane of the last slice becomes the new first slice
+    if (T.shift && s == S - 1) {
+      __syncthreads();
+      for (int hp = 0; hp < 2 * H; ++hp) {
+        float2* Up = I.U + ((size_t)hp * S + plane) * N;
+        for (int k = tid; k < N; k += nt) Up[k] = make_float2(0.f, 0.f);
+      }
+    }
+  } else if (dep) {
+    for (int q = tid; q < P; q += nt) {
+      const int64_t n = p0 + q;
+      stats(I.x[n], I.y[n], has_even ? I.px[n] : 0.f, has_even ? I.py[n] : 0.f, gRf + I.dg[n]);
+    }
+  }
+  if (!dep) return;
+  // ================= pass 2: deposit of the next solveField =================
+  const int mi1 = -block_min_i(-ci1, redi), mi0 = block_min_i(ci0, redi);
+  const int mj1 = -block_min_i(-cj1, redi), mj0 = block_min_i(cj0, redi);
+  // bounds: |w mc| <= wm H weight coef_U / g for odd harmonics, times |f| <=
+  // 2 xi2 H for even ones (|eta| <= 1, |e| = 1); radial |w c| <= coef_Ez L
+  // weight (1 + |wr1|) / max(ir, 1)
+  const float bnd = block_max_f(bmax, redf) * 1.0625f * Hmax * weight * fabsf(D.coef_U) * (float)P;
+  const float rbnd = block_max_f(rmax, redf) * 1.0625f * L * weight * fabsf(D.coef_Ez) * (float)P;
+  // interior targets a particle can reach
+  const int bi0 = max(1, mi0), bi1 = min(nx - 2, mi1 + 1), bj0 = max(1, mj0), bj1 = min(ny - 2, mj1 + 1);
+  const int bw = bi1 - bi0 + 1, bh = bj1 - bj0 + 1;
+  const int cells = (bw > 0 && bh > 0) ? bw * bh : 0;
+  const float q2 = quantum(bnd), qr = quantum(rbnd);
+  const float iq2 = 1.f / q2, iqr = 1.f / qr;
+  // accumulators: one interleaved (re, im) pair per cell of each source plane
+  const int nsrc = I.nsrc;
+  const size_t nacc = (size_t)nsrc * cells * 2;
+  float2* gsrc = I.src + (size_t)s * nsrc * N;
+  const bool in_smem = nacc * sizeof(acc_t) <= area_bytes;
+  acc_t* acc = in_smem ? reinterpret_cast<acc_t*>(area) : reinterpret_cast<acc_t*>(gsrc);
+  for (size_t k = tid; k < nacc; k += nt) acc[k] = 0;
+  for (int k = tid; k < LF * nr * 2; k += nt) sR[k] = 0;
+  __syncthreads();
+  const float coef_U = D.coef_U;
+  for (int q = tid; q < P; q += nt) {
+    const int64_t n = p0 + q;
+    const float x = I.x[n], y = I.y[n], g = gRf + I.dg[n];
+    const float thr = theta_red(I.th[n]);
+    const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+    const int ii = (int)gx, jj = (int)gy;
+    if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
+      const float wx1 = gx - ii, wy1 = gy - jj;
+      float xi2 = 0.f;
+      float2 eP = make_float2(1.f, 0.f);
+      if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, I.px[n], I.py[n], &xi2, &eP);
+      int cidx[4];
+      float wv[4];
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
+        const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
+        cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
+        wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
+      }
+      const float ig = 1.f / g;
+#pragma unroll
+      for (int h = 0; h < HM; ++h) {
+        if (h >= H) break;
+        const int Hh = I.harmony[h];
+        const float2 e = expif(-(float)Hh * (thr + D.Phi_half));
+        const float2 mc = cs(e, (float)Hh * weight * coef_U * ig);
+        acc_t* base = acc + (size_t)I.src_plane[h] * cells * 2;
+        if (Hh & 1) {
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            if (cidx[cb] < 0) continue;
+            acc_add(base + 2 * cidx[cb], fix(mc.x * wv[cb], iq2));
+            acc_add(base + 2 * cidx[cb] + 1, fix(mc.y * wv[cb], iq2));
+          }
+        } else {
+          float2 fx, fy;
+          ffac(I, Hh, D.xi, xi2, D.K0a, eP, true, &fx, &fy);
+          const float2 ax = cm(cm(D.etaX, fx), mc), ay = cm(cm(D.etaY, fy), mc);
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            if (cidx[cb] < 0) continue;
+            acc_add(base + 2 * cidx[cb], fix(-ax.x * wv[cb], iq2));
+            acc_add(base + 2 * cidx[cb] + 1, fix(-ax.y * wv[cb], iq2));
+            acc_add(base + 2 * (cells + cidx[cb]), fix(-ay.x * wv[cb], iq2));
+            acc_add(base + 2 * (cells + cidx[cb]) + 1, fix(-ay.y * wv[cb], iq2));
+          }
+        }
+      }
+    }
+    // radial source: every particle (solveField.cpp:331-357)
+    const float r = sqrtf(x * x + y * y);
+    const int ir = (int)(r / dr + 0.5f);
+    if (ir >= 0 && ir < nr - 1) {
+      const float phi = (F > 1) ? ((x == 0.f) ? 0.f : atan2f(y, x)) : 0.f;
+      const float wr1 = ir > 0 ? (r * r * idr2 - (float)(ir * ir)) / (2.f * ir) : 0.f;
+      const float w0 = ir > 0 ? 1.f - wr1 : 1.f;
+      const bool two = ir > 0 && ir + 1 < nr - 1;
+      const float mag0 = D.coef_Ez * weight / (ir > 0 ? (float)ir : 1.f);
+      for (int l = 0; l < L; ++l)
+        for (int f = 0; f < F; ++f) {
+          if (ir == 0 && f > 0) continue;
+          const float2 e = expif(-((float)(l + 1) * thr + (float)f * phi));
+          const float mag = mag0 * (l + 1.f);
+          const float2 cc = make_float2(-e.y * mag, e.x * mag);  // i * coef * e^{-i..}
+          acc_t* b0 = sR + ((l * F + f) * nr + ir) * 2;
+          acc_add(b0, fix(cc.x * w0, iqr));
+          acc_add(b0 + 1, fix(cc.y * w0, iqr));
+          if (two) {
+            acc_add(b0 + 2, fix(cc.x * wr1, iqr));
+            acc_add(b0 + 3, fix(cc.y * wr1, iqr));
+          }
+        }
+    }
+  }
+  __syncthreads();
+  // source box of the next ADI (float2 per cell, in place when the
+  // accumulators live in the source buffer itself)
+  for (size_t k = tid; k < nacc / 2; k += nt) {
+    const int2 v = reinterpret_cast<const int2*>(acc)[k];
+    gsrc[k] = make_float2((float)v.x * q2, (float)v.y * q2);
+  }
+  if (tid == 0) I.sbox[s] = make_int4(bi0, cells > 0 ? bi1 : bi0 - 1, bj0, bj1);
+  __syncthreads();
+  // radial Thomas solve in FP64 (solveField.cpp:361-397), one thread per (l, f)
+  if (tid < LF) {
+    const int l = tid / F, f = tid % F;
+    const double A = D.A;
+    double bprev, dre, dim;
+    if (f == 0) {
+      bprev = -(1.0 + (l + 1.0) * (l + 1.0) * A / 8.0);
+      dre = (double)sR[(tid * nr) * 2] * qr;
+      dim = (double)sR[(tid * nr) * 2 + 1] * qr;
+    } else {
+      bprev = 1.0; dre = 0.0; dim = 0.0;
+    }
+    double* dbuf = reinterpret_cast<double*>(area) + (size_t)tid * nr * 3;  // d re, d im, b
+    dbuf[0] = dre; dbuf[1] = dim; dbuf[2] = bprev;
+    double aprev = (f == 0) ? 1.0 : 0.0;
+    for (int j = 1; j < nr; ++j) {
+      const bool last = j == nr - 1;
+      const double aj = last ? 0.0 : j + 0.5, cj = last ? 0.0 : j - 0.5;
+      double bj_ = last ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * A * j - f * f * log((j + 0.5) / (j - 0.5));
+      const double ww = cj / bprev;
+      bj_ -= ww * aprev;
+      double djr = last ? 0.0 : (double)sR[(tid * nr + j) * 2] * qr;
+      double dji = last ? 0.0 : (double)sR[(tid * nr + j) * 2 + 1] * qr;
+      djr -= ww * dre;
+      dji -= ww * dim;
+      dbuf[j * 3] = djr; dbuf[j * 3 + 1] = dji; dbuf[j * 3 + 2] = bj_;
+      dre = djr; dim = dji; bprev = bj_; aprev = aj;
+    }
+    for (int j = nr - 2; j >= 0; --j) {
+      const float2 v = make_float2((float)(dbuf[j * 3] / dbuf[j * 3 + 2]), (float)(dbuf[j * 3 + 1] / dbuf[j * 3 + 2]));
+      I.Ez[((size_t)l * S + s) * F * nr + (size_t)f * nr + j] = v;
+    }
+  }
+}
+
+// Diagnostics of the current state without stepping (the row of the first
+// iteration of a run): plane energies and beam partial sums per slice.
+__global__ void __launch_bounds__(256) k_batch_measure(const BInst* inst, const BStep* step, const int4* work,
+                                                       int nwork) {
+  __shared__ double red[8];
+  for (int w = blockIdx.x; w < nwork; w += gridDim.x) {
+    const int4 wi = work[w];
+    const BInst& I = inst[wi.x];
+    const BStep& T = step[wi.x];
+    const int s = wi.y, S = I.S, N = I.N, H = I.H;
+    for (int hp = 0; hp < 2 * H; ++hp) {
+      const float2* U = I.U + ((size_t)hp * S + ((s + T.ring_base) % S)) * N;
+      double e = 0.0;
+      for (int k = threadIdx.x; k < N; k += blockDim.x) e += (double)U[k].x * U[k].x + (double)U[k].y * U[k].y;
+      const double t = block_sum_d(e, red);
+      if (threadIdx.x == 0) I.part_e[(size_t)s * 2 * H + hp] = t;
+    }
+    const int stride = 7 + 2 * H + 1;
+    const float weight = I.weight[s];
+    double acc[7 + 2 * FELIS_MAX_HARMONY + 1];
+    for (int k = 0; k < stride; ++k) acc[k] = 0.0;
+    for (int64_t n = I.soff[s] + threadIdx.x; n < I.soff[s + 1]; n += blockDim.x) {
+      const double x = I.x[n], y = I.y[n], ig = 1.0 / (I.gamR + (double)I.dg[n]), xp = I.px[n] * ig, yp = I.py[n] * ig;
+      acc[0] += x * x; acc[1] += y * y; acc[2] += xp * xp; acc[3] += yp * yp; acc[4] += x * xp; acc[5] += y * yp;
+      acc[6] += 1.0;
+      const float thr = theta_red(I.th[n]);
+      for (int h = 0; h < H; ++h) {
+        const float2 e = expif((float)I.harmony[h] * thr);
+        acc[7 + 2 * h] += (double)e.x * weight;
+        acc[8 + 2 * h] += (double)e.y * weight;
+      }
+      acc[7 + 2 * H] += weight;
+    }
+    for (int k = 0; k < stride; ++k) {
+      const double t = block_sum_d(acc[k], red);
+      if (threadIdx.x == 0) I.part_b[(size_t)s * stride + k] = t;
+    }
+  }
+}
+
+// One block per instance: the power of the new state (slices of the shifted
+// ring) and the twiss / bFactor of the pushed beam, summed in slice order.
+__global__ void __launch_bounds__(256) k_batch_reduce(const BInst* inst, const BStep* step, double* hist_e,
+                                                      double* hist_t, double* hist_b, int se, int st_, int sb) {
+  __shared__ double red[8];
+  const BInst& I = inst[blockIdx.x];
+  const BStep& T = step[blockIdx.x];
+  const int H = I.H, S = I.S, stride = 7 + 2 * H + 1;
+  double* he = hist_e + (size_t)blockIdx.x * se;
+  double* ht = hist_t + (size_t)blockIdx.x * st_;
+  double* hb = hist_b + (size_t)blockIdx.x * sb;
+  const int last = T.shift ? S - 1 : S;
+  for (int hp = 0; hp < 2 * H; ++hp) {
+    double v = 0.0;
+    for (int s = threadIdx.x; s < last; s += blockDim.x) v += I.part_e[(size_t)s * 2 * H + hp];
+    const double t = block_sum_d(v, red);
+    if (threadIdx.x == 0) he[hp] = t;
+  }
+  double acc[7 + 2 * FELIS_MAX_HARMONY + 1];
+  for (int k = 0; k < stride; ++k) {
+    double v = 0.0;
+    for (int s = threadIdx.x; s < S; s += blockDim.x) v += I.part_b[(size_t)s * stride + k];
+    acc[k] = block_sum_d(v, red);
+  }
+  if (threadIdx.x == 0) {
+    for (int k = 0; k < 6; ++k) ht[k] = 0.0;
+    const double cnt = acc[6];
+    if (cnt > 0) {
+      const double ax = acc[0] / cnt, ay = acc[1] / cnt, axp = acc[2] / cnt, ayp = acc[3] / cnt;
+      const double cx = acc[4] / cnt, cy = acc[5] / cnt;
+      const double ex = sqrt(ax * axp - cx * cx), ey = sqrt(ay * ayp - cy * cy);
+      ht[0] = ex; ht[1] = ax / ex; ht[2] = -cx / ex; ht[3] = ey; ht[4] = ay / ey; ht[5] = -cy / ey;
+    }
+    for (int k = 0; k < 2 * H; ++k) hb[k] = acc[7 + k] / acc[7 + 2 * H];
+  }
+}
+
+// Instances by the largest harmonic count (register arrays) and by the
+// register budget: MINB = 2 (128 registers) or 3 (80 registers) CTAs of 256
+// threads per SM.
+typedef void (*PushKernel)(BatchLaunch);
+template <int MINB>
+PushKernel push_kernel_b(int H) {
+  if (H <= 1) return k_batch_push<1, MINB>;
+  if (H <= 2) return k_batch_push<2, MINB>;
+  if (H <= 4) return k_batch_push<4, MINB>;
+  return k_batch_push<FELIS_MAX_HARMONY, MINB>;
+}
+PushKernel push_kernel(int H, int minb) { return minb >= 3 ? push_kernel_b<3>(H) : push_kernel_b<2>(H); }
+
+}  // namespace
+
+size_t batch_adi_smem(int nx_max, int ny_max, int src_cells) {
+  const int M = nx_max > ny_max ? nx_max : ny_max;
+  return ((size_t)ny_max * (nx_max | 1) + 6 * (size_t)M + (size_t)src_cells) * sizeof(float2);
+}
+
+size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
+  const size_t head = (((size_t)LF_max * nr_max * sizeof(float2) + 15) & ~(size_t)15) +
+                      (((size_t)LF_max * nr_max * 2 * sizeof(acc_t) + 15) & ~(size_t)15);
+  size_t area = (size_t)nsrc_max * box_cells * 2 * sizeof(acc_t);  // a (re, im) pair per cell and plane
+  const size_t thomas = (size_t)LF_max * nr_max * 3 * sizeof(double);
+  if (thomas > area) area = thomas;
+  return head + area;
+}
+
+void batch_set_smem(int H, int minb, int adi_bytes, int push_bytes) {
+  cudaFuncSetAttribute(k_batch_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, adi_bytes);
+  cudaFuncSetAttribute(push_kernel(H, minb), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
+}
+
+int batch_resident_adi(int threads, int smem_bytes) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_adi, threads, smem_bytes) != cudaSuccess) return 0;
+  return n;
+}
+
+int batch_resident_push(int H, int minb, int threads, int smem_bytes) {
+  int n = 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_kernel(H, minb), threads, smem_bytes) != cudaSuccess)
+    return 0;
+  return n;
+}
+
+void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st) {
+  if (a.nwork > 0) k_batch_adi<<<a.nwork, threads, a.smem_bytes, st>>>(a);
+}
+
+void launch_batch_push(const BatchLaunch& a, int H, int minb, int threads, cudaStream_t st) {
+  if (a.nwork > 0) push_kernel(H, minb)<<<a.nwork, threads, a.smem_bytes, st>>>(a);
+}
+
+void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st) {
+  if (nwork > 0) k_batch_measure<<<nwork < 1184 ? nwork : 1184, 256, 0, st>>>(inst, step, work, nwork);
+}
+
+void launch_batch_reduce(const BInst* inst, int ninst, const BStep* step, double* hist_e, double* hist_t,
+                         double* hist_b, int se, int st_, int sb, cudaStream_t st) {
+  k_batch_reduce<<<ninst, 256, 0, st>>>(inst, step, hist_e, hist_t, hist_b, se, st_, sb);
+}
+
+}  // namespace felis

@@ -259,6 +259,61 @@ felis_status felis_sort_by_slice(const int32_t* keys, int64_t n, int64_t* perm);
 #define FELIS_SORT_NOALLOC_MAX_KEYS 262144
 felis_status felis_sort_by_slice_noalloc(const int32_t* keys_dev, int64_t n, int64_t* perm_dev, void* stream);
 
+/* ---- mixed-precision ensemble ------------------------------------------
+ * Many independent FELIS runs (one felis_params each: own slices, grid,
+ * harmonics, lattice and beam) advanced together on one GPU.  No counterpart
+ * in the reference, which runs one Domain per MPI job; each instance follows
+ * the loop of main.cpp:92-156 with the FP64 plain path's operator order, but
+ * computes in mixed precision: particles x, y, px, py, gamma - gamR, the
+ * field, the ADI sweeps and the theta slope (taken relative to the
+ * resonance) in FP32; theta itself, the lattice (updateK_quadG.cpp on the
+ * host), the radial Ez solve and all diagnostic sums in FP64.  The source deposit accumulates fixed-point integers, so a
+ * run is reproducible bit for bit, and an instance's results depend neither
+ * on the launch shape nor on the other instances, as long as the ensemble's
+ * largest harmonic count stays in the same class (1, 2, 3-4 or 5-8: it
+ * selects the compiled kernel).  One species, 3D,
+ * SCLmode <= 4, grids up to 256 points wide.  Every iteration is two kernel
+ * launches over all instances (the ADI of every field plane; the push of
+ * every slice with the deposit of the next iteration's source) plus one
+ * reduction launch; felis_batch_run captures a range of iterations as one
+ * CUDA graph. */
+typedef struct felis_batch felis_batch;
+felis_status felis_batch_create(const felis_params* const* instances, int32_t n, felis_batch** out);
+void felis_batch_destroy(felis_batch* b);
+const char* felis_batch_last_error(const felis_batch* b);
+/* Same arrays and layouts as felis_upload_particles / felis_upload_field
+ * (species 0), converted to the ensemble's storage precision. */
+felis_status felis_batch_upload_particles(felis_batch* b, int32_t inst, const double* x, const double* y,
+                                          const double* px, const double* py, const double* theta,
+                                          const double* gamma, const int64_t* slice_offsets,
+                                          const double* weights);
+felis_status felis_batch_download_particles(felis_batch* b, int32_t inst, double* x, double* y, double* px,
+                                            double* py, double* theta, double* gamma);
+felis_status felis_batch_upload_field(felis_batch* b, int32_t inst, int32_t harmonic_index, int32_t pol,
+                                      const double* data);
+felis_status felis_batch_download_field(felis_batch* b, int32_t inst, int32_t harmonic_index, int32_t pol,
+                                        double* data);
+/* Iterations [it0, it1) of every instance. */
+felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1);
+/* Per-iteration energy (2H), twiss (6) and bFactor (2H) of one instance,
+ * same meaning as felis_get_diagnostics. */
+felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t it0, int32_t it1,
+                                         double* energy, double* twiss, double* bfactor);
+/* Launch shape: threads per CTA of the push launch (128 or 256) and the CTAs
+ * per SM that the ADI launch sizes its shared memory for (1 or 2; the rest of
+ * the shared memory stages the slice's source box).  get_launch also reports
+ * the push kernel's register budget per thread (80 up to 2 harmonics, else
+ * 128: part of the compiled kernel class, never tuned). */
+felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas);
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas, int32_t* push_regs);
+/* Tries each launch shape for `steps` real iterations starting at it0 (the
+ * ensemble advances; results do not depend on the shape), keeps the fastest
+ * and returns the next iteration to run in *next_it.  Shapes are cached per
+ * ensemble geometry: a second call on a matching ensemble runs nothing. */
+felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it);
+/* Device time of the last felis_batch_run graph launch. */
+felis_status felis_batch_last_run_ms(felis_batch* b, double* ms);
+
 /* ---- host-side setup of the reference's input format -------------------- */
 /* Parses a FELIS input file ([Domain], [Save], [Seed], [Undulator], [Quad],
  * [EBeam], [Wake_field], [Bessel_table], [Phase_shifter] blocks;
