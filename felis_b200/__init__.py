@@ -123,7 +123,7 @@ _sig("felis_batch_download_field", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32
 _sig("felis_batch_run", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_batch_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp)
 _sig("felis_batch_set_launch", C.c_int, _vp, C.c_int32, C.c_int32)
-_sig("felis_batch_get_launch", C.c_int, _vp, _i32p, _i32p, _i32p)
+_sig("felis_batch_get_launch", C.c_int, _vp, _i32p, _i32p)
 _sig("felis_batch_tune", C.c_int, _vp, C.c_int32, C.c_int32, _i32p)
 _sig("felis_batch_last_run_ms", C.c_int, _vp, _dp)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
@@ -474,10 +474,10 @@ class Batch:
     def set_launch(self, push_threads: int, adi_ctas: int):
         self._ck(_lib.felis_batch_set_launch(self._b, push_threads, adi_ctas))
 
-    def launch(self) -> tuple[int, int, int]:
-        t, c, m = C.c_int32(), C.c_int32(), C.c_int32()
-        self._ck(_lib.felis_batch_get_launch(self._b, C.byref(t), C.byref(c), C.byref(m)))
-        return t.value, c.value, m.value
+    def launch(self) -> tuple[int, int]:
+        t, c = C.c_int32(), C.c_int32()
+        self._ck(_lib.felis_batch_get_launch(self._b, C.byref(t), C.byref(c)))
+        return t.value, c.value
 
     def tune(self, it0: int, steps: int) -> int:
         nxt = C.c_int32(0)

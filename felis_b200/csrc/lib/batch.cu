@@ -239,7 +239,7 @@ struct felis_batch {
   double *d_he = nullptr, *d_ht = nullptr, *d_hb = nullptr;
   int hist_n = 0;
   int adi_threads = 128, adi_smem = 0;
-  int push_threads = 256, push_smem = 0, push_minb = 2, adi_ctas = 2;
+  int push_threads = 128, push_smem = 0, adi_ctas = 2;
   bool layout_ready = false;
   int src_valid_it = -1;  // iteration whose solveField source is in the buffers
   double last_run_ms = 0.0;
@@ -459,7 +459,7 @@ felis_status ensure_launch(felis_batch* b) {
   b->adi_smem = (int)batch_adi_smem(b->nx_max, b->ny_max, (int)src_cells);
   const int box = std::min(b->N_max, 6144);
   b->push_smem = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, box);
-  batch_set_smem(b->H_max, b->push_minb, b->adi_smem, b->push_smem);
+  batch_set_smem(b->H_max, b->adi_smem, b->push_smem);
   return FELIS_OK;
 }
 
@@ -478,7 +478,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
     BatchLaunch d{};
     d.inst = b->d_inst; d.step = row_d0; d.work = b->d_push_work; d.nwork = b->n_push;
     d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY;
-    launch_batch_push(d, b->H_max, b->push_minb, b->push_threads, b->st);
+    launch_batch_push(d, b->H_max, b->push_threads, b->st);
   }
   for (int it = it0; it < it1; ++it) {
     const BStep* T = b->d_steps + (size_t)(it - it0) * n;
@@ -488,7 +488,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
     BatchLaunch p{};
     p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
     p.mode = BATCH_PUSH;
-    launch_batch_push(p, b->H_max, b->push_minb, b->push_threads, b->st);
+    launch_batch_push(p, b->H_max, b->push_threads, b->st);
     if (it + 1 < b->hist_n)
       launch_batch_reduce(b->d_inst, n, T, b->d_he + (size_t)(it + 1) * se, b->d_ht + (size_t)(it + 1) * stt,
                           b->d_hb + (size_t)(it + 1) * sb, se * b->hist_n, stt * b->hist_n, sb * b->hist_n, b->st);
@@ -624,12 +624,8 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
   if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
   for (auto& I : b->in) { I.p.abc_alpha = I.p.abc_alpha_p = I.p.abc_beta = I.p.abc_beta_p = nullptr; }
   if (std::max(b->nx_max, b->ny_max) > 256) return bad(FELIS_UNSUPPORTED, "grid wider than 256 points");
-  b->push_threads = 256;
+  b->push_threads = 128;
   b->adi_ctas = 2;
-  // register budget of the push kernel: a property of the compiled kernel
-  // class (like the harmonic bound), fixed so that results never depend on
-  // tuning: 80 registers (3 CTAs of 256 per SM) up to 2 harmonics, else 128
-  b->push_minb = b->H_max <= 2 ? 3 : 2;
   *out = b;
   return FELIS_OK;
 }
@@ -753,11 +749,10 @@ felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_
   return FELIS_OK;
 }
 
-felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas, int32_t* push_regs) {
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas) {
   if (!b) return FELIS_BAD_ARG;
   if (push_threads) *push_threads = b->push_threads;
   if (adi_ctas) *adi_ctas = b->adi_ctas;
-  if (push_regs) *push_regs = b->push_minb >= 3 ? 80 : 128;
   return FELIS_OK;
 }
 

@@ -80,9 +80,8 @@ struct BatchLaunch {
 enum { BATCH_PUSH = 0, BATCH_DEPOSIT_ONLY = 1 };
 
 void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st);
-// H: the largest harmonic count of the ensemble; minb: 2 or 3 CTAs of 256
-// threads per SM (register budget).  Both select the kernel instance.
-void launch_batch_push(const BatchLaunch& a, int H, int minb, int threads, cudaStream_t st);
+// H: the largest harmonic count of the ensemble (selects the kernel instance).
+void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st);
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);
 void launch_batch_reduce(const BInst* inst, int ninst, const BStep* step, double* hist_e, double* hist_t,
                          double* hist_b, int hist_stride_e, int hist_stride_t, int hist_stride_b, cudaStream_t st);
@@ -91,9 +90,9 @@ size_t batch_adi_smem(int nx_max, int ny_max, int src_cells);
 // Shared memory of the push launch with room for the accumulators of
 // `box_cells` source cells of every source plane.
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells);
-void batch_set_smem(int H, int minb, int adi_bytes, int push_bytes);
+void batch_set_smem(int H, int adi_bytes, int push_bytes);
 // CTAs of each kernel that fit on one SM with this shape.
 int batch_resident_adi(int threads, int smem_bytes);
-int batch_resident_push(int H, int minb, int threads, int smem_bytes);
+int batch_resident_push(int H, int threads, int smem_bytes);
 
 }  // namespace felis

@@ -86,41 +86,6 @@ __device__ __forceinline__ int block_min_i(int v, int* red) {
   return t;
 }
 
-__device__ __forceinline__ float bj(const BInst& I, int row, int col) {
-  row = row < 0 ? 0 : (row >= I.bn ? I.bn - 1 : row);
-  return __ldg(I.bessel + row * I.bcols + col);
-}
-
-// fx, fy of harmonic H for the push (sign conventions of
-// particlePush.cpp:336-360) or the deposit (solveField.cpp:277-300).
-__device__ __forceinline__ void ffac(const BInst& I, int H, float xi, float xi2, float K0a, float2 eP, bool deposit,
-                                     float2* fx, float2* fy) {
-  const float x = (float)H * xi / (float)I.dBessel;
-  const int idx = (int)x;
-  const float w1 = x - (float)idx, w0 = 1.f - w1;
-  const float2 eM = make_float2(eP.x, -eP.y);
-  if (H & 1) {
-    const float sign = (((H - 1) / 2) % 2 == 0) ? 1.f : -1.f;
-    const float J1 = bj(I, idx, (H - 1) / 2) * w0 + bj(I, idx + 1, (H - 1) / 2) * w1;
-    const float J2 = bj(I, idx, (H + 1) / 2) * w0 + bj(I, idx + 1, (H + 1) / 2) * w1;
-    if (deposit) { *fx = make_float2(sign * (J1 - K0a * J2), 0.f); *fy = make_float2(sign * (J1 + K0a * J2), 0.f); }
-    else { *fx = make_float2(sign * (K0a * J1 - J2), 0.f); *fy = make_float2(sign * (K0a * J1 + J2), 0.f); }
-  } else {
-    const float sign = ((H / 2) % 2 == 0) ? 1.f : -1.f;
-    const float J1 = bj(I, idx, (H - 2) / 2) * w0 + bj(I, idx + 1, (H - 2) / 2) * w1;
-    const float J2 = bj(I, idx, H / 2) * w0 + bj(I, idx + 1, H / 2) * w1;
-    const float J3 = bj(I, idx, (H + 2) / 2) * w0 + bj(I, idx + 1, (H + 2) / 2) * w1;
-    const float sx = sign * xi2 * H * 0.5f;
-    if (deposit) {
-      *fx = cs(cad(cs(eM, J1 - K0a * J2), cs(eP, J2 - K0a * J3)), sx);
-      *fy = cs(cad(cs(eM, J1 + K0a * J2), cs(eP, J2 + K0a * J3)), sx);
-    } else {
-      *fx = cs(cad(cs(eP, K0a * J1 - J2), cs(eM, K0a * J2 - J3)), sx);
-      *fy = cs(cad(cs(eP, K0a * J1 + J2), cs(eM, K0a * J2 + J3)), sx);
-    }
-  }
-}
-
 // xi2 and e^{i (B - Phi/2)} of particlePush.cpp:272-279 / solveField.cpp:259-266.
 __device__ __forceinline__ void pol_phase(float K0, float ue, float K0a, float Phi_half, float px, float py,
                                           float* xi2, float2* eP) {
@@ -129,27 +94,6 @@ __device__ __forceinline__ void pol_phase(float K0, float ue, float K0a, float P
   const float B = atanf(2.f * K0a * ue * (px - py) /
                         ((1.f + K0a) * (px + ue * ue * py) + (1.f - K0a) * (px * ue * ue + py)));
   *eP = expif(B - Phi_half);
-}
-
-// Both transverse half-pushes of particlePush.cpp:82-110.  For a fixed
-// gamma they are RK4 steps of a linear ODE, i.e. the state is multiplied by
-// the RK4 polynomial of the step matrix; the host forms the product of the
-// two half-step maps as a function of a = 1/gamma to second order about
-// 1/gamR: s' = s + D0 s + da (M1 s + da M2 s), da = 1/gamma - 1/gamR.
-__device__ __forceinline__ void transverse_map(const BStep& T, float& x, float& y, float& px, float& py, float da) {
-  const float s0 = x, s1 = y, s2 = px, s3 = py;
-  float o[4];
-#pragma unroll
-  for (int r = 0; r < 4; ++r) {
-    const float* D = T.tD0 + 4 * r;
-    const float* A = T.tM1 + 4 * r;
-    const float* B = T.tM2 + 4 * r;
-    const float m2 = B[0] * s0 + B[1] * s1 + B[2] * s2 + B[3] * s3;
-    const float m1 = A[0] * s0 + A[1] * s1 + A[2] * s2 + A[3] * s3 + da * m2;
-    const float d0 = D[0] * s0 + D[1] * s1 + D[2] * s2 + D[3] * s3;
-    o[r] = d0 + da * m1;
-  }
-  x = s0 + o[0]; y = s1 + o[1]; px = s2 + o[2]; py = s3 + o[3];
 }
 
 // Asynchronous 8-byte global -> shared copies (all in flight at once), then
@@ -166,9 +110,6 @@ constexpr int kAccBits = 31;
 // v / q rounded to an integer; q is a power of two, so v * (1/q) is exact in
 // FP32 and only the rounding to an integer is inexact
 __device__ __forceinline__ acc_t fix(float v, float inv_q) { return (acc_t)__float2int_rn(v * inv_q); }
-__device__ __forceinline__ void acc_add(acc_t* p, acc_t v) {
-  if (v != 0) atomicAdd(p, v);
-}
 // quantum 2^e with bound / 2^e < 2^(kAccBits - 1): the rounded terms add at
 // most half a quantum each on top of the exact sum, so no sum overflows
 __device__ __forceinline__ float quantum(float bound) {
@@ -310,30 +251,199 @@ __global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
 // ============================================================================
 // Push and the next deposit, one CTA per (instance, slice).
 // ============================================================================
-template <int HM, int MINB>
-__global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
+// Bessel table lookup held in registers.
+struct BesselTab {
+  const float* __restrict__ t;
+  int bn, bcols;
+  float idb;  // 1 / dBessel
+};
+__device__ __forceinline__ float bjt(const BesselTab& B, int row, int col) {
+  row = row < 0 ? 0 : (row >= B.bn ? B.bn - 1 : row);
+  return __ldg(B.t + row * B.bcols + col);
+}
+
+// fx, fy of harmonic H for the push (sign conventions of
+// particlePush.cpp:336-360) or the deposit (solveField.cpp:277-300).
+__device__ __forceinline__ void ffac_t(const BesselTab& B, int H, float xi, float xi2, float K0a, float2 eP,
+                                       bool deposit, float2* fx, float2* fy) {
+  const float x = (float)H * xi * B.idb;
+  const int idx = (int)x;
+  const float w1 = x - (float)idx, w0 = 1.f - w1;
+  const float2 eM = make_float2(eP.x, -eP.y);
+  if (H & 1) {
+    const float sign = (((H - 1) / 2) % 2 == 0) ? 1.f : -1.f;
+    const float J1 = bjt(B, idx, (H - 1) / 2) * w0 + bjt(B, idx + 1, (H - 1) / 2) * w1;
+    const float J2 = bjt(B, idx, (H + 1) / 2) * w0 + bjt(B, idx + 1, (H + 1) / 2) * w1;
+    if (deposit) { *fx = make_float2(sign * (J1 - K0a * J2), 0.f); *fy = make_float2(sign * (J1 + K0a * J2), 0.f); }
+    else { *fx = make_float2(sign * (K0a * J1 - J2), 0.f); *fy = make_float2(sign * (K0a * J1 + J2), 0.f); }
+  } else {
+    const float sign = ((H / 2) % 2 == 0) ? 1.f : -1.f;
+    const float J1 = bjt(B, idx, (H - 2) / 2) * w0 + bjt(B, idx + 1, (H - 2) / 2) * w1;
+    const float J2 = bjt(B, idx, H / 2) * w0 + bjt(B, idx + 1, H / 2) * w1;
+    const float J3 = bjt(B, idx, (H + 2) / 2) * w0 + bjt(B, idx + 1, (H + 2) / 2) * w1;
+    const float sx = sign * xi2 * H * 0.5f;
+    if (deposit) {
+      *fx = cs(cad(cs(eM, J1 - K0a * J2), cs(eP, J2 - K0a * J3)), sx);
+      *fy = cs(cad(cs(eM, J1 + K0a * J2), cs(eP, J2 + K0a * J3)), sx);
+    } else {
+      *fx = cs(cad(cs(eP, K0a * J1 - J2), cs(eM, K0a * J2 - J3)), sx);
+      *fy = cs(cad(cs(eP, K0a * J1 + J2), cs(eM, K0a * J2 + J3)), sx);
+    }
+  }
+}
+
+// Fixed-point adds without a return value: shared-memory accumulators by
+// their 32-bit shared address, global ones by pointer.
+__device__ __forceinline__ void red_s(unsigned saddr, acc_t v) {
+  if (v != 0) asm volatile("red.shared.add.s32 [%0], %1;\n" ::"r"(saddr), "r"(v) : "memory");
+}
+template <bool SH>
+__device__ __forceinline__ void acc_to(acc_t* gbase, unsigned sbase, int idx, acc_t v) {
+  if (SH) red_s(sbase + 4u * (unsigned)idx, v);
+  else if (v != 0) atomicAdd(gbase + idx, v);
+}
+
+// Constants of the deposit launch in registers.
+struct DepConst {
+  float K0, ue, K0a, Phi_half, coef_U, xi, coef_Ez;
+  float2 etaX, etaY;
+};
+
+// Pass 2: the source deposit (solveField.cpp:252-357) of the pushed
+// particles into the fixed-point accumulators (2D: shared or global, radial:
+// shared).
+template <int HM, bool SH>
+__device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const float* __restrict__ ys,
+                                             const float* __restrict__ pxs, const float* __restrict__ pys,
+                                             const float* __restrict__ dgs, const double* __restrict__ ths,
+                                             int64_t p0, int P, const int (&hh)[HM], const int (&sp)[HM], int H,
+                                             bool has_even, const DepConst& D, const BesselTab& B, float weight,
+                                             float gRf, float minX, float minY, float idx_, float idy_, int nx,
+                                             int ny, int bi0, int bi1, int bj0, int bj1, int bw, int cells,
+                                             float iq2, float iqr, acc_t* gacc, unsigned sacc, unsigned sR,
+                                             float dr, float idr2, int nr, int L, int F) {
+  for (int q = threadIdx.x; q < P; q += blockDim.x) {
+    const int64_t n = p0 + q;
+    const float x = xs[n], y = ys[n], g = gRf + dgs[n];
+    const float thr = theta_red(ths[n]);
+    const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+    const int ii = (int)gx, jj = (int)gy;
+    if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
+      const float wx1 = gx - ii, wy1 = gy - jj;
+      float xi2 = 0.f;
+      float2 eP = make_float2(1.f, 0.f);
+      if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, pxs[n], pys[n], &xi2, &eP);
+      int cidx[4];
+      float wv[4];
+#pragma unroll
+      for (int cb = 0; cb < 4; ++cb) {
+        const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
+        const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
+        cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
+        wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
+      }
+      const float ig = 1.f / g;
+#pragma unroll
+      for (int h = 0; h < HM; ++h) {
+        if (h >= H) break;
+        const int Hh = hh[h];
+        const float2 e = expif(-(float)Hh * (thr + D.Phi_half));
+        const float2 mc = cs(e, (float)Hh * weight * D.coef_U * ig);
+        const int base = sp[h] * cells * 2;
+        if (Hh & 1) {
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            if (cidx[cb] < 0) continue;
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], fix(mc.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, fix(mc.y * wv[cb], iq2));
+          }
+        } else {
+          float2 fx, fy;
+          ffac_t(B, Hh, D.xi, xi2, D.K0a, eP, true, &fx, &fy);
+          const float2 ax = cm(cm(D.etaX, fx), mc), ay = cm(cm(D.etaY, fy), mc);
+#pragma unroll
+          for (int cb = 0; cb < 4; ++cb) {
+            if (cidx[cb] < 0) continue;
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], fix(-ax.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, fix(-ax.y * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]), fix(-ay.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]) + 1, fix(-ay.y * wv[cb], iq2));
+          }
+        }
+      }
+    }
+    // radial source: every particle (solveField.cpp:331-357)
+    const float r = sqrtf(x * x + y * y);
+    const int ir = (int)(r / dr + 0.5f);
+    if (ir >= 0 && ir < nr - 1) {
+      const float phi = (F > 1) ? ((x == 0.f) ? 0.f : atan2f(y, x)) : 0.f;
+      const float wr1 = ir > 0 ? (r * r * idr2 - (float)(ir * ir)) / (2.f * ir) : 0.f;
+      const float w0 = ir > 0 ? 1.f - wr1 : 1.f;
+      const bool two = ir > 0 && ir + 1 < nr - 1;
+      const float mag0 = D.coef_Ez * weight / (ir > 0 ? (float)ir : 1.f);
+      for (int l = 0; l < L; ++l)
+        for (int f = 0; f < F; ++f) {
+          if (ir == 0 && f > 0) continue;
+          const float2 e = expif(-((float)(l + 1) * thr + (float)f * phi));
+          const float mag = mag0 * (l + 1.f);
+          const float2 cc = make_float2(-e.y * mag, e.x * mag);  // i * coef * e^{-i..}
+          const unsigned b0 = sR + 8u * (unsigned)((l * F + f) * nr + ir);
+          red_s(b0, fix(cc.x * w0, iqr));
+          red_s(b0 + 4u, fix(cc.y * w0, iqr));
+          if (two) {
+            red_s(b0 + 8u, fix(cc.x * wr1, iqr));
+            red_s(b0 + 12u, fix(cc.y * wr1, iqr));
+          }
+        }
+    }
+  }
+}
+
+template <int HM>
+__global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ double redd[8];
   __shared__ float redf[8];
   __shared__ int redi[8];
+  __shared__ __align__(16) float smap[48];  // transverse map: D0, M1, M2 (row-major 4x4 each)
   const int4 wi = a.work[blockIdx.x];
   const BInst& I = a.inst[wi.x];
   const BStep& T = a.step[wi.x];
   const int s = wi.y;
   const int tid = threadIdx.x, nt = blockDim.x;
+  // instance and step constants in registers; the particle arrays are
+  // restrict-qualified, so the stores below cannot alias them
   const int S = I.S, nx = I.nx, ny = I.ny, N = I.N, H = I.H, nr = I.nr, L = I.L, F = I.F, LF = L * F;
+  float* __restrict__ xs = I.x;
+  float* __restrict__ ys = I.y;
+  float* __restrict__ pxs = I.px;
+  float* __restrict__ pys = I.py;
+  float* __restrict__ dgs = I.dg;
+  double* __restrict__ ths = I.th;
   const int64_t p0 = I.soff[s], p1 = I.soff[s + 1];
   const int P = (int)(p1 - p0);
   const float weight = I.weight[s];
-  const float gRf = (float)I.gamR, igR = (float)(1.0 / I.gamR);
+  const double gR = I.gamR;
+  const float gRf = (float)gR, igR = (float)(1.0 / gR);
   const float minX = (float)I.minX, minY = (float)I.minY, idx_ = (float)(1.0 / I.dx), idy_ = (float)(1.0 / I.dy);
   const float dr = (float)I.dr, idr2 = (float)(1.0 / (I.dr * I.dr));
+  const BesselTab B{I.bessel, I.bn, I.bcols, (float)(1.0 / I.dBessel)};
   const int plane = (s + T.ring_base) % S;
+  int hh[HM], sp[HM];
   bool has_even = false;
   int Hmax = 1;
 #pragma unroll
-  for (int h = 0; h < HM; ++h)
-    if (h < H) { has_even |= (I.harmony[h] % 2 == 0); Hmax = max(Hmax, I.harmony[h]); }
+  for (int h = 0; h < HM; ++h) {
+    hh[h] = h < H ? I.harmony[h] : 1;
+    sp[h] = h < H ? I.src_plane[h] : 0;
+    if (h < H) { has_even |= (hh[h] % 2 == 0); Hmax = max(Hmax, hh[h]); }
+  }
+  const bool push = a.mode == BATCH_PUSH;
+  const bool dep = T.deposit != 0 && P > 0;
+  DepConst D;
+  D.K0 = T.dep.K0; D.ue = T.dep.ue; D.K0a = T.dep.K0a; D.Phi_half = T.dep.Phi_half; D.coef_U = T.dep.coef_U;
+  D.xi = T.dep.xi; D.coef_Ez = T.dep.coef_Ez; D.etaX = T.dep.etaX; D.etaY = T.dep.etaY;
+  const double depA = T.dep.A;
   // shared memory: Ez of the slice | radial accumulators | 2D accumulators
   float2* sEz = reinterpret_cast<float2*>(sm);
   const size_t o1 = ((size_t)LF * nr * sizeof(float2) + 15) & ~(size_t)15;
@@ -341,9 +451,6 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
   acc_t* sR = reinterpret_cast<acc_t*>(sm + o1);
   unsigned char* area = sm + o2;
   const size_t area_bytes = (size_t)a.smem_bytes - o2;
-  const bool push = a.mode == BATCH_PUSH;
-  const bool dep = T.deposit != 0 && P > 0;
-  const BDep& D = T.dep;
   // deposit statistics of the (pushed) beam: cell box and fixed-point bounds
   int ci0 = 1 << 30, ci1 = -(1 << 30), cj0 = 1 << 30, cj1 = -(1 << 30);
   float bmax = 0.f, rmax = 0.f;
@@ -372,30 +479,61 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
   };
   // ================= pass 1: push (particlePush.cpp) =================
   if (push) {
+    for (int k = tid; k < 48; k += nt) smap[k] = k < 16 ? T.tD0[k] : (k < 32 ? T.tM1[k - 16] : T.tM2[k - 32]);
     for (int k = tid; k < LF * nr; k += nt) {
       const int l = k / (F * nr), rest = k % (F * nr);
       sEz[k] = I.Ez[((size_t)l * S + s) * F * nr + rest];
     }
-    __syncthreads();
+    const float R0 = T.R0, A0 = T.A0, AQ0 = T.AQ0, c12 = T.c1 * T.c2, K0 = T.K0, ue = T.ue, K0a = T.K0a;
+    const float Phi_half = T.Phi_half, cxi = T.cxi, K0sq = T.K0 * T.sq, ksK0sq = T.ksK0 * T.sq, e_mc2 = T.e_mc2;
+    const float dPhi = T.dPhi;
+    const float2 etaX = T.etaX, etaY = T.etaY;
+    const int drift = T.drift, shift = T.shift;
+    const double ku = T.ku, A0d = T.A0d;
     const int stride = 7 + 2 * H + 1;
+    const double wakeE = I.wakeOn ? I.wakeE[s + I.minI] / (K_MC2 * 1.0e6) : 0.0;
+    const double dz = I.dz;
+    const float dwake = (float)(dz * wakeE);
+    const double dTh = I.numSlice * 2 * M_PI, idTh = 1.0 / dTh;
+    const float dzf = (float)dz;
+    const float2* __restrict__ Ubase = I.U + (size_t)plane * N;
+    const size_t hpstride = (size_t)S * N;
+    __syncthreads();
+    const float4* m4 = reinterpret_cast<const float4*>(smap);
     double acc7[7] = {0, 0, 0, 0, 0, 0, 0};
     double bre[HM], bim[HM];
 #pragma unroll
     for (int h = 0; h < HM; ++h) { bre[h] = 0.0; bim[h] = 0.0; }
     double wsum = 0.0;
-    const double wakeE = I.wakeOn ? I.wakeE[s + I.minI] / (K_MC2 * 1.0e6) : 0.0;
-    const float dwake = (float)(I.dz * wakeE);
-    const double dTh = I.numSlice * 2 * M_PI, idTh = 1.0 / dTh;
-    const float dzf = (float)I.dz;
-    const float2* Ubase = I.U + (size_t)plane * N;
-    const size_t hpstride = (size_t)S * N;
     int bad_over = 0, bad_range = 0, bad_nan = 0;
+    // the next particle's state is loaded one iteration ahead
+    float nxv = 0.f, nyv = 0.f, npx = 0.f, npy = 0.f, ndg = 0.f;
+    double nth = 0.0;
+    if (tid < P) {
+      const int64_t n = p0 + tid;
+      nxv = xs[n]; nyv = ys[n]; npx = pxs[n]; npy = pys[n]; ndg = dgs[n]; nth = ths[n];
+    }
     for (int q = tid; q < P; q += nt) {
       const int64_t n = p0 + q;
-      float x = I.x[n], y = I.y[n], px = I.px[n], py = I.py[n], dg = I.dg[n];
-      double th = I.th[n];
+      float x = nxv, y = nyv, px = npx, py = npy, dg = ndg;
+      double th = nth;
+      if (q + nt < P) {
+        const int64_t m = n + nt;
+        nxv = xs[m]; nyv = ys[m]; npx = pxs[m]; npy = pys[m]; ndg = dgs[m]; nth = ths[m];
+      }
       const float g = gRf + dg;
-      transverse_map(T, x, y, px, py, -dg * igR / g);
+      {  // both transverse half-pushes as one linear map (see BStep)
+        const float da = -dg * igR / g;
+        float o[4];
+#pragma unroll
+        for (int r = 0; r < 4; ++r) {
+          const float4 Dr = m4[r], Ar = m4[4 + r], Br = m4[8 + r];
+          const float m2 = Br.x * x + Br.y * y + Br.z * px + Br.w * py;
+          const float m1 = Ar.x * x + Ar.y * y + Ar.z * px + Ar.w * py + da * m2;
+          o[r] = Dr.x * x + Dr.y * y + Dr.z * px + Dr.w * py + da * m1;
+        }
+        x += o[0]; y += o[1]; px += o[2]; py += o[3];
+      }
       const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
       const int ii = (int)gx, jj = (int)gy;
       if (ii >= 0 && ii < nx - 1 && jj >= 0 && jj < ny - 1) {
@@ -409,23 +547,23 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
           const float2* Py = Px + hpstride;
           Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[nx], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[nx + 1], wx1 * wy1)));
           Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[nx], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[nx + 1], wx1 * wy1)));
-          const float Hh = (float)I.harmony[h];
+          const float Hh = (float)hh[h];
           sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
         }
-        if (!T.drift) {
+        if (!drift) {
           const float r2 = x * x + y * y;
-          const float k2 = px * px + py * py + T.c1 * T.c2 * r2;  // K2 - Q0
-          const float xi = T.cxi * igR * igR / ((1.f + dg * igR) * (1.f + dg * igR));
+          const float k2 = px * px + py * py + c12 * r2;  // K2 - Q0
+          const float xi = cxi * igR * igR / ((1.f + dg * igR) * (1.f + dg * igR));
           float xi2 = 0.f;
           float2 eP = make_float2(1.f, 0.f);
-          if (has_even) pol_phase(T.K0, T.ue, T.K0a, T.Phi_half, px, py, &xi2, &eP);
+          if (has_even) pol_phase(K0, ue, K0a, Phi_half, px, py, &xi2, &eP);
 #pragma unroll
           for (int h = 0; h < HM; ++h) {  // fold the polarisation factors into the field
             if (h >= H) break;
             float2 fx, fy;
-            ffac(I, I.harmony[h], xi, xi2, T.K0a, eP, false, &fx, &fy);
-            Ux[h] = cm(cm(T.etaX, fx), Ux[h]);
-            Uy[h] = cm(cm(T.etaY, fy), Uy[h]);
+            ffac_t(B, hh[h], xi, xi2, K0a, eP, false, &fx, &fy);
+            Ux[h] = cm(cm(etaX, fx), Ux[h]);
+            Uy[h] = cm(cm(etaY, fy), Uy[h]);
           }
           const float r = sqrtf(r2);
           const int ir = (int)(r / dr + 0.5f);
@@ -464,28 +602,28 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
 #pragma unroll
             for (int h = 0; h < HM; ++h) {
               if (h >= H) break;
-              const float Hh = (float)I.harmony[h];
-              const float2 e = expif(Hh * (tm + T.Phi_half));
+              const float Hh = (float)hh[h];
+              const float2 e = expif(Hh * (tm + Phi_half));
               const float2 tc = cm(e, csb(Ux[h], Uy[h]));
               sumTh += -tc.y / Hh;
               sumG += tc.x;
             }
             sumG *= 0.5f / (gRf + dgm);
-            kth_prev = T.R0 + T.AQ0 * (d * (2.f + d) * inv2) - T.A0 * inv2 * (k2 + sumU2 + T.K0 * T.sq * sumTh);
-            kg_prev = T.ksK0 * T.sq * sumG + T.e_mc2 * sumEz;
+            kth_prev = R0 + AQ0 * (d * (2.f + d) * inv2) - A0 * inv2 * (k2 + sumU2 + K0sq * sumTh);
+            kg_prev = ksK0sq * sumG + e_mc2 * sumEz;
             const float wgt = (m == 1 || m == 4) ? 1.f : 2.f;
             kth_sum += wgt * kth_prev;
             kg_sum += wgt * kg_prev;
           }
           const float dth = dzf / 6.f * kth_sum;
-          if (dth > T.dPhi || dth < -T.dPhi) bad_over = 1;
+          if (dth > dPhi || dth < -dPhi) bad_over = 1;
           th += (double)dth;
           dg += dzf / 6.f * kg_sum - dwake;
         } else {
           const double K2 = 1.0 + (double)px * px + (double)py * py;
-          const double tmp = T.ku - T.A0d * (K2 + sumU2);
-          th += tmp * I.dz;
-          th -= I.dz * wakeE;
+          const double tmp = ku - A0d * (K2 + sumU2);
+          th += tmp * dz;
+          th -= dz * wakeE;
         }
       }
       // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
@@ -496,7 +634,7 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
       }
       if (th > dTh || th < 0) bad_range = 1;
       if (!(dg - dg == 0.f) || !(th - th == 0.0) || !(x - x == 0.f)) bad_nan = 1;
-      I.x[n] = x; I.y[n] = y; I.px[n] = px; I.py[n] = py; I.dg[n] = dg; I.th[n] = th;
+      xs[n] = x; ys[n] = y; pxs[n] = px; pys[n] = py; dgs[n] = dg; ths[n] = th;
       // twiss / bFactor partial sums of the new state (twiss.cpp, saveFile.cpp)
       const float ig = 1.f / (gRf + dg), xp = px * ig, yp = py * ig;
       acc7[0] += (double)(x * x); acc7[1] += (double)(y * y); acc7[2] += (double)(xp * xp);
@@ -505,13 +643,13 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
 #pragma unroll
       for (int h = 0; h < HM; ++h) {
         if (h >= H) break;
-        const float2 e = expif((float)I.harmony[h] * thn);
-        bre[h] += (double)e.x * weight;
-        bim[h] += (double)e.y * weight;
+        const float2 e = expif((float)hh[h] * thn);
+        bre[h] += (double)e.x;
+        bim[h] += (double)e.y;
       }
-      wsum += weight;
       if (dep) stats(x, y, px, py, gRf + dg);
     }
+    wsum = (double)weight * (double)max(0, (P - tid + nt - 1) / nt);
     if (bad_over) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
     if (bad_range) atomicOr(I.err + ERR_OUT_OF_RANGE, 1);
     if (bad_nan) atomicOr(I.err + ERR_NAN, 1);
@@ -525,12 +663,12 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
     for (int h = 0; h < HM; ++h) {
       if (h >= H) break;
       const double tr = block_sum_d(bre[h], redd), ti = block_sum_d(bim[h], redd);
-      if (tid == 0) { out[7 + 2 * h] = tr; out[8 + 2 * h] = ti; }
+      if (tid == 0) { out[7 + 2 * h] = tr * weight; out[8 + 2 * h] = ti * weight; }
     }
     const double tw = block_sum_d(wsum, redd);
     if (tid == 0) out[7 + 2 * H] = tw;
     // slippage shift: the plane of the last slice becomes the new first slice
-    if (T.shift && s == S - 1) {
+    if (shift && s == S - 1) {
       __syncthreads();
       for (int hp = 0; hp < 2 * H; ++hp) {
         float2* Up = I.U + ((size_t)hp * S + plane) * N;
@@ -540,7 +678,7 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
   } else if (dep) {
     for (int q = tid; q < P; q += nt) {
       const int64_t n = p0 + q;
-      stats(I.x[n], I.y[n], has_even ? I.px[n] : 0.f, has_even ? I.py[n] : 0.f, gRf + I.dg[n]);
+      stats(xs[n], ys[n], has_even ? pxs[n] : 0.f, has_even ? pys[n] : 0.f, gRf + dgs[n]);
     }
   }
   if (!dep) return;
@@ -567,82 +705,16 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
   for (size_t k = tid; k < nacc; k += nt) acc[k] = 0;
   for (int k = tid; k < LF * nr * 2; k += nt) sR[k] = 0;
   __syncthreads();
-  const float coef_U = D.coef_U;
-  for (int q = tid; q < P; q += nt) {
-    const int64_t n = p0 + q;
-    const float x = I.x[n], y = I.y[n], g = gRf + I.dg[n];
-    const float thr = theta_red(I.th[n]);
-    const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
-    const int ii = (int)gx, jj = (int)gy;
-    if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
-      const float wx1 = gx - ii, wy1 = gy - jj;
-      float xi2 = 0.f;
-      float2 eP = make_float2(1.f, 0.f);
-      if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, I.px[n], I.py[n], &xi2, &eP);
-      int cidx[4];
-      float wv[4];
-#pragma unroll
-      for (int cb = 0; cb < 4; ++cb) {
-        const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
-        const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
-        cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
-        wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
-      }
-      const float ig = 1.f / g;
-#pragma unroll
-      for (int h = 0; h < HM; ++h) {
-        if (h >= H) break;
-        const int Hh = I.harmony[h];
-        const float2 e = expif(-(float)Hh * (thr + D.Phi_half));
-        const float2 mc = cs(e, (float)Hh * weight * coef_U * ig);
-        acc_t* base = acc + (size_t)I.src_plane[h] * cells * 2;
-        if (Hh & 1) {
-#pragma unroll
-          for (int cb = 0; cb < 4; ++cb) {
-            if (cidx[cb] < 0) continue;
-            acc_add(base + 2 * cidx[cb], fix(mc.x * wv[cb], iq2));
-            acc_add(base + 2 * cidx[cb] + 1, fix(mc.y * wv[cb], iq2));
-          }
-        } else {
-          float2 fx, fy;
-          ffac(I, Hh, D.xi, xi2, D.K0a, eP, true, &fx, &fy);
-          const float2 ax = cm(cm(D.etaX, fx), mc), ay = cm(cm(D.etaY, fy), mc);
-#pragma unroll
-          for (int cb = 0; cb < 4; ++cb) {
-            if (cidx[cb] < 0) continue;
-            acc_add(base + 2 * cidx[cb], fix(-ax.x * wv[cb], iq2));
-            acc_add(base + 2 * cidx[cb] + 1, fix(-ax.y * wv[cb], iq2));
-            acc_add(base + 2 * (cells + cidx[cb]), fix(-ay.x * wv[cb], iq2));
-            acc_add(base + 2 * (cells + cidx[cb]) + 1, fix(-ay.y * wv[cb], iq2));
-          }
-        }
-      }
-    }
-    // radial source: every particle (solveField.cpp:331-357)
-    const float r = sqrtf(x * x + y * y);
-    const int ir = (int)(r / dr + 0.5f);
-    if (ir >= 0 && ir < nr - 1) {
-      const float phi = (F > 1) ? ((x == 0.f) ? 0.f : atan2f(y, x)) : 0.f;
-      const float wr1 = ir > 0 ? (r * r * idr2 - (float)(ir * ir)) / (2.f * ir) : 0.f;
-      const float w0 = ir > 0 ? 1.f - wr1 : 1.f;
-      const bool two = ir > 0 && ir + 1 < nr - 1;
-      const float mag0 = D.coef_Ez * weight / (ir > 0 ? (float)ir : 1.f);
-      for (int l = 0; l < L; ++l)
-        for (int f = 0; f < F; ++f) {
-          if (ir == 0 && f > 0) continue;
-          const float2 e = expif(-((float)(l + 1) * thr + (float)f * phi));
-          const float mag = mag0 * (l + 1.f);
-          const float2 cc = make_float2(-e.y * mag, e.x * mag);  // i * coef * e^{-i..}
-          acc_t* b0 = sR + ((l * F + f) * nr + ir) * 2;
-          acc_add(b0, fix(cc.x * w0, iqr));
-          acc_add(b0 + 1, fix(cc.y * w0, iqr));
-          if (two) {
-            acc_add(b0 + 2, fix(cc.x * wr1, iqr));
-            acc_add(b0 + 3, fix(cc.y * wr1, iqr));
-          }
-        }
-    }
-  }
+  const unsigned sacc = (unsigned)__cvta_generic_to_shared(area);
+  const unsigned sRa = (unsigned)__cvta_generic_to_shared(sR);
+  if (in_smem)
+    deposit_pass<HM, true>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
+                           idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, iq2, iqr, nullptr, sacc, sRa, dr,
+                           idr2, nr, L, F);
+  else
+    deposit_pass<HM, false>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
+                            idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, iq2, iqr, acc, 0u, sRa, dr, idr2, nr,
+                            L, F);
   __syncthreads();
   // source box of the next ADI (float2 per cell, in place when the
   // accumulators live in the source buffer itself)
@@ -655,10 +727,9 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
   // radial Thomas solve in FP64 (solveField.cpp:361-397), one thread per (l, f)
   if (tid < LF) {
     const int l = tid / F, f = tid % F;
-    const double A = D.A;
     double bprev, dre, dim;
     if (f == 0) {
-      bprev = -(1.0 + (l + 1.0) * (l + 1.0) * A / 8.0);
+      bprev = -(1.0 + (l + 1.0) * (l + 1.0) * depA / 8.0);
       dre = (double)sR[(tid * nr) * 2] * qr;
       dim = (double)sR[(tid * nr) * 2 + 1] * qr;
     } else {
@@ -670,7 +741,7 @@ __global__ void __launch_bounds__(256, MINB) k_batch_push(BatchLaunch a) {
     for (int j = 1; j < nr; ++j) {
       const bool last = j == nr - 1;
       const double aj = last ? 0.0 : j + 0.5, cj = last ? 0.0 : j - 0.5;
-      double bj_ = last ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * A * j - f * f * log((j + 0.5) / (j - 0.5));
+      double bj_ = last ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * depA * j - f * f * log((j + 0.5) / (j - 0.5));
       const double ww = cj / bprev;
       bj_ -= ww * aprev;
       double djr = last ? 0.0 : (double)sR[(tid * nr + j) * 2] * qr;
@@ -764,18 +835,14 @@ __global__ void __launch_bounds__(256) k_batch_reduce(const BInst* inst, const B
   }
 }
 
-// Instances by the largest harmonic count (register arrays) and by the
-// register budget: MINB = 2 (128 registers) or 3 (80 registers) CTAs of 256
-// threads per SM.
+// Instances by the largest harmonic count (sizes of the register arrays).
 typedef void (*PushKernel)(BatchLaunch);
-template <int MINB>
-PushKernel push_kernel_b(int H) {
-  if (H <= 1) return k_batch_push<1, MINB>;
-  if (H <= 2) return k_batch_push<2, MINB>;
-  if (H <= 4) return k_batch_push<4, MINB>;
-  return k_batch_push<FELIS_MAX_HARMONY, MINB>;
+PushKernel push_kernel(int H) {
+  if (H <= 1) return k_batch_push<1>;
+  if (H <= 2) return k_batch_push<2>;
+  if (H <= 4) return k_batch_push<4>;
+  return k_batch_push<FELIS_MAX_HARMONY>;
 }
-PushKernel push_kernel(int H, int minb) { return minb >= 3 ? push_kernel_b<3>(H) : push_kernel_b<2>(H); }
 
 }  // namespace
 
@@ -793,9 +860,9 @@ size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
   return head + area;
 }
 
-void batch_set_smem(int H, int minb, int adi_bytes, int push_bytes) {
+void batch_set_smem(int H, int adi_bytes, int push_bytes) {
   cudaFuncSetAttribute(k_batch_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, adi_bytes);
-  cudaFuncSetAttribute(push_kernel(H, minb), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
+  cudaFuncSetAttribute(push_kernel(H), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
 }
 
 int batch_resident_adi(int threads, int smem_bytes) {
@@ -804,10 +871,9 @@ int batch_resident_adi(int threads, int smem_bytes) {
   return n;
 }
 
-int batch_resident_push(int H, int minb, int threads, int smem_bytes) {
+int batch_resident_push(int H, int threads, int smem_bytes) {
   int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_kernel(H, minb), threads, smem_bytes) != cudaSuccess)
-    return 0;
+  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_kernel(H), threads, smem_bytes) != cudaSuccess) return 0;
   return n;
 }
 
@@ -815,8 +881,8 @@ void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st) {
   if (a.nwork > 0) k_batch_adi<<<a.nwork, threads, a.smem_bytes, st>>>(a);
 }
 
-void launch_batch_push(const BatchLaunch& a, int H, int minb, int threads, cudaStream_t st) {
-  if (a.nwork > 0) push_kernel(H, minb)<<<a.nwork, threads, a.smem_bytes, st>>>(a);
+void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st) {
+  if (a.nwork > 0) push_kernel(H)<<<a.nwork, threads, a.smem_bytes, st>>>(a);
 }
 
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st) {

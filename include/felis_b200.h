@@ -301,11 +301,9 @@ felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t i
                                          double* energy, double* twiss, double* bfactor);
 /* Launch shape: threads per CTA of the push launch (128 or 256) and the CTAs
  * per SM that the ADI launch sizes its shared memory for (1 or 2; the rest of
- * the shared memory stages the slice's source box).  get_launch also reports
- * the push kernel's register budget per thread (80 up to 2 harmonics, else
- * 128: part of the compiled kernel class, never tuned). */
+ * the shared memory stages the slice's source box). */
 felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas);
-felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas, int32_t* push_regs);
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas);
 /* Tries each launch shape for `steps` real iterations starting at it0 (the
  * ensemble advances; results do not depend on the shape), keeps the fastest
  * and returns the next iteration to run in *next_it.  Shapes are cached per
