@@ -1,18 +1,24 @@
 """Throughput of the FELIS slice loop on B200.
 
-Workload (default `sase`): plain FP64 time-dependent SASE, 8 GeV beam,
-flat-top 3 kA over 1024 slices of 8192 particles (8,388,608 in all) with
-shot-noise phases, BiPolar undulator lambda_u = 2.6 cm, K0 = 2.6,
-102 x 102 grid over +-300 um, one step per undulator period.  A "step" is
-one iteration of the reference loop (main.cpp:117-155) over every slice.
+Workload (default `sase`): time-dependent SASE, 8 GeV beam, flat-top 3 kA
+over 1024 slices of 8192 particles (8,388,608 in all) with shot-noise
+phases, BiPolar undulator lambda_u = 2.6 cm, K0 = 2.6, 102 x 102 grid over
++-300 um, one step per undulator period.  A "step" is one iteration of the
+reference loop (main.cpp:117-155) over every slice.
 
   python bench.py [--gpus N] [--steps K] [--warmup W] [--impl felis|reference]
 
---impl felis      the GPU library: W untimed iterations, then K iterations
-                  replayed from one CUDA graph, timed with CUDA events on the
-                  library's stream (inputs resident in HBM); also the same
-                  loop end to end through the C ABI with host buffers, and the
-                  CPU restatement on a bounded sample as a reported baseline.
+--impl felis      the GPU library.  The headline `value` is the
+                  mixed-precision engine (felis_batch_*: FP32 push and ADI,
+                  FP64 theta and reductions) on the workload; beside it, the
+                  FP64 plain path on the same workload (`fp64_plain`), the
+                  speed-up and the power error between the two, and the
+                  96-instance batched ensemble (`ensemble`).  Each path runs W
+                  untimed iterations, then K iterations replayed from one CUDA
+                  graph, timed with CUDA events on the library's stream
+                  (inputs resident in HBM); `e2e` is the mixed engine end to
+                  end through the C ABI with host buffers; the CPU
+                  restatement runs on a bounded sample as a reported baseline.
 --impl reference  the reference's CPU path (the oracle port: the reference
                   does not build here, it needs MPI/HDF5/GSL) on the host's
                   cores, on a bounded sample of the same workload.
@@ -265,8 +271,230 @@ def run_felis(args, dist, rank, world):
         "clocks": clk,
         "e2e": e2e,
         "final_power_units": float(e[-1, 0]),
+        "_energy": h.diagnostics(0, W + K + 1)[0],
     }
+    h.close()
     return line
+
+
+BYTES_PARTICLE_STEP_MIXED = 56  # read + write of 5 x 4 B + theta 8 B
+BYTES_ADI_CELL_MIXED = 16       # read + write one FP32 complex cell
+
+
+def _batch_upload(b, k, beam, fields):
+    b.upload_particles(k, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
+                       beam["offsets"], beam["weights"])
+    for hh, (ux, uy) in enumerate(fields):
+        b.upload_field(k, hh, 0, ux)
+        b.upload_field(k, hh, 1, uy)
+
+
+def batch_kernels(b):
+    import felis_b200 as fb
+
+    out = {}
+    for name, k in fb.BATCH_KERNEL_KINDS.items():
+        n, t = b.kernel_stats(k)
+        out[name] = {"launches": n, "ms": t}
+    return out
+
+
+def run_mixed(args, cfg, beam, fields, dist, world, fp64_energy):
+    """The workload through the mixed-precision engine: tuned launch shape,
+    W warm-up iterations, K timed iterations from one graph; power error
+    against the FP64 plain run of the same iterations."""
+    import numpy as np
+
+    import felis_b200 as fb
+    from felis_b200 import analysis
+
+    p = cfg.params
+    P = int(beam["offsets"][-1])
+    cells = p.slice_n * p.nx * p.ny * 2 * p.num_harmony
+    b = fb.Batch([p])
+    _batch_upload(b, 0, beam, fields)
+    W, K = args.warmup, args.steps
+    # the tuner advances the run; start it over for the measured iterations
+    b.tune(0, 2)
+    b.close()
+    b = fb.Batch([p])
+    _batch_upload(b, 0, beam, fields)
+    b.run(0, W)
+    b.profile(True, max_launches=8 * K + 64)
+    barrier(dist)
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    time.sleep(0.3)
+    b.run(W, W + K)
+    ms = b.last_run_ms()
+    clk = clocks.stop()
+    barrier(dist)
+    ms = max_over_ranks(dist, ms)
+    kinds = batch_kernels(b)
+    launches, _ = b.kernel_stats(-1)
+    e, tw, bf = b.diagnostics(0, 0, W + K + 1)
+    P32 = analysis.output_power(e)
+    P64 = analysis.output_power(fp64_energy)
+    ok = P64 > 0
+    rel = np.abs(P32[ok] - P64[ok]) / P64[ok]
+    sec = ms / 1e3
+    peak, peak_kind = peaks()
+    bytes_per_launch = {"push": P * BYTES_PARTICLE_STEP_MIXED, "adi": cells * BYTES_ADI_CELL_MIXED, "reduce": 0}
+    dom = max(("push", "adi"), key=lambda k: kinds[k]["ms"])
+    kd = kinds[dom]
+    avg_ms = kd["ms"] / max(kd["launches"], 1)
+    achieved = bytes_per_launch[dom] / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    step_bytes = P * BYTES_PARTICLE_STEP_MIXED + cells * BYTES_ADI_CELL_MIXED
+    traffic = None
+    prof_path = os.path.join(ROOT, "profiles", "traffic.json")
+    if os.path.exists(prof_path):
+        try:
+            with open(prof_path) as f:
+                traffic = json.load(f).get(args.workload + "_mixed", {}).get(dom)
+        except Exception:
+            traffic = None
+    threads, adi_ctas = b.launch()
+    res = {
+        "value": P * K * world / sec, "ms_per_step": ms / K, "adi_cells_per_s": cells * K * world / sec,
+        "launch": {"push_threads": threads, "adi_ctas_per_sm": adi_ctas},
+        "power_error": {"max_rel": float(rel.max()) if rel.size else None,
+                        "final_rel": float(rel[-1]) if rel.size else None,
+                        "iterations": [0, W + K], "reference": "FP64 plain GPU path, same initial state"},
+        "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                     "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
+                     "bytes_per_launch": bytes_per_launch[dom], "mean_launch_ms": avg_ms},
+        "step_roofline": {"algorithmic_bytes": step_bytes, "achieved_gbs": step_bytes / (ms / K / 1e3) / 1e9,
+                          "frac": step_bytes / (ms / K / 1e3) / 1e9 / peak},
+        "kernels": kinds, "gpu_launches": launches, "clocks": clk,
+    }
+    b.close()
+    return res
+
+
+def run_mixed_e2e(args, cfg, beam, fields, dist):
+    """The mixed engine end to end through the C ABI: upload from pinned host
+    buffers (FP64, converted by the library), K iterations, the per-iteration
+    diagnostics read back, the final particles downloaded."""
+    import numpy as np
+
+    import felis_b200 as fb
+
+    try:
+        import torch
+
+        def pinned(a):
+            t = torch.empty(a.shape, dtype=torch.float64 if a.dtype == np.float64 else torch.complex128, pin_memory=True)
+            t.numpy()[...] = a
+            return t.numpy()
+    except Exception:
+        def pinned(a):
+            return np.array(a)
+
+    p = cfg.params
+    host = {k: pinned(np.asarray(beam[k])) for k in ("x", "y", "px", "py", "theta", "gamma")}
+    hf = [(pinned(ux), pinned(uy)) for ux, uy in fields]
+    K = max(1, min(args.steps, args.e2e_steps))
+    P = int(beam["offsets"][-1])
+    b = fb.Batch([p])
+    barrier(dist)
+    t0 = time.perf_counter()
+    b.upload_particles(0, host["x"], host["y"], host["px"], host["py"], host["theta"], host["gamma"],
+                       beam["offsets"], beam["weights"])
+    for hh, (ux, uy) in enumerate(hf):
+        b.upload_field(0, hh, 0, ux)
+        b.upload_field(0, hh, 1, uy)
+    b.run(0, K)
+    b.diagnostics(0, 0, K + 1)
+    b.download_particles(0)
+    dt = time.perf_counter() - t0
+    barrier(dist)
+    dt = max_over_ranks(dist, dt)
+    world = 1 if dist is None else dist.get_world_size()
+    h2d = 6 * P * 8 + sum(2 * a.nbytes for a, _ in hf)
+    d2h = (K + 1) * (2 * p.num_harmony + 6 + 2 * p.num_harmony) * 8 + 6 * P * 8
+    b.close()
+    return {"value": P * K * world / dt, "unit": UNIT, "steps": K, "seconds": dt,
+            "h2d_bytes_per_step": h2d / K, "d2h_bytes_per_step": d2h / K,
+            "api": "felis_batch_upload_* + felis_batch_run + felis_batch_get_diagnostics + "
+                   "felis_batch_download_particles"}
+
+
+def run_ensemble(args, dist, world):
+    """The 96-instance batched ensemble: aggregate throughput, and the power
+    error of a sample of instances (the smallest of each grid size) against
+    FP64 plain runs of the same iterations."""
+    import numpy as np
+
+    import felis_b200 as fb
+    from felis_b200 import analysis, workloads
+
+    spec = workloads.ensemble(args.ensemble)
+    d = tempfile.mkdtemp(prefix="felis_ens_")
+    cfgs = []
+    for k, kw in enumerate(spec):
+        kw = dict(kw)
+        seed = kw.pop("beam_seed")
+        kw["total_length"] = 40.0
+        cfgs.append((fb.Config(workloads.write_input(os.path.join(d, f"i{k}.inp"), **kw)), seed))
+    t_setup = time.perf_counter()
+    b = fb.Batch([c.params for c, _ in cfgs])
+    P = 0
+    cells = 0
+    sample = {}
+    for k, (c, seed) in enumerate(cfgs):
+        beam = c.load_beam(0, seed=seed)
+        fields = [c.load_seed(h) for h in range(c.params.num_harmony)]
+        _batch_upload(b, k, beam, fields)
+        P += int(beam["offsets"][-1])
+        cells += c.params.slice_n * c.params.nx * c.params.ny * 2 * c.params.num_harmony
+        key = c.params.nx
+        if key not in sample or c.params.slice_n < cfgs[sample[key]][0].params.slice_n:
+            sample[key] = k
+        del beam, fields
+    t_setup = time.perf_counter() - t_setup
+    W, K = args.warmup, args.ensemble_steps
+    nxt = b.tune(0, 1)
+    b.run(nxt, nxt + W)
+    b.profile(True, max_launches=8 * K + 64)
+    barrier(dist)
+    i0 = nxt + W
+    b.run(i0, i0 + K)
+    ms = max_over_ranks(dist, b.last_run_ms())
+    barrier(dist)
+    kinds = batch_kernels(b)
+    launches, _ = b.kernel_stats(-1)
+    # per-instance power error: the same instance from the same initial state
+    # through the FP64 plain path for the same iterations
+    errs = {}
+    for nx, k in sorted(sample.items()):
+        c, seed = cfgs[k]
+        beam = c.load_beam(0, seed=seed)
+        fields = [c.load_seed(h) for h in range(c.params.num_harmony)]
+        h = fb.Handle(c.params)
+        h.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
+                           beam["offsets"], beam["weights"])
+        for hh, (ux, uy) in enumerate(fields):
+            h.upload_field(hh, 0, ux)
+            h.upload_field(hh, 1, uy)
+        h.run(0, i0 + K)
+        P64 = analysis.output_power(h.diagnostics(0, i0 + K + 1)[0])
+        P32 = analysis.output_power(b.diagnostics(k, 0, i0 + K + 1)[0])
+        ok = P64 > 0
+        rel = np.abs(P32[ok] - P64[ok]) / P64[ok]
+        errs[f"instance {k} (slices {c.params.slice_n}, grid {c.params.nx})"] = float(rel.max())
+        h.close()
+    threads, adi_ctas = b.launch()
+    res = {
+        "workload": f"{len(spec)} SASE instances, slices in {{128..2048}}, grids {{66, 102, 152}}, "
+                    f"4096 particles per slice, 2-4 kA, spread 0.5-2e-4, mixed precision",
+        "value": P * K * world / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K,
+        "adi_cells_per_s": cells * K * world / (ms / 1e3), "particles": P, "cells": cells,
+        "steps": K, "iterations": [i0, i0 + K], "setup_s": t_setup,
+        "launch": {"push_threads": threads, "adi_ctas_per_sm": adi_ctas},
+        "kernels": kinds, "gpu_launches": launches,
+        "power_error_max_rel_sample": errs,
+    }
+    b.close()
+    return res
 
 
 def run_e2e(args, cfg, beam, fields, dist):
@@ -327,6 +555,9 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--slices", type=int, default=None, help="smaller sase bunch (profiling captures)")
+    ap.add_argument("--ensemble", type=int, default=96, help="instances of the batched ensemble (0: skip)")
+    ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -349,6 +580,33 @@ def main():
 
     dist, rank, world = dist_init()
     line = run_felis(args, dist, rank, world)
+    if not args.fp64_only:
+        cfg, beam, fields = make_workload(args.workload, rank, args.slices)
+        fp64 = dict(line)
+        e64 = fp64.pop("_energy")
+        mixed = run_mixed(args, cfg, beam, fields, dist, world, e64)
+        e2e = run_mixed_e2e(args, cfg, beam, fields, dist)
+        del beam, fields
+        ens = run_ensemble(args, dist, world) if args.ensemble > 0 else None
+        for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
+                  "data", "cpu_baseline"):
+            fp64.pop(k, None)
+        cfg_line = dict(line["config"])
+        cfg_line["workload"] = cfg_line["workload"].replace("FP64 ", "mixed-precision ")
+        line = {
+            "metric": METRIC, "value": mixed["value"], "unit": UNIT, "n_gpus": world, "steps": args.steps,
+            "warmup": args.warmup, "ms_per_step": mixed["ms_per_step"], "higher_is_better": True,
+            "scaling": "weak", "vs_baseline": None, "dtype": "f32 (theta, lattice, reductions f64)",
+            "data": line["data"], "config": cfg_line,
+            "adi_cells_per_s": mixed["adi_cells_per_s"],
+            "speedup_vs_fp64_plain": mixed["value"] / fp64["value"],
+            "power_error_vs_fp64": mixed["power_error"],
+            "roofline": mixed["roofline"], "step_roofline": mixed["step_roofline"],
+            "kernels": mixed["kernels"], "gpu_launches": mixed["gpu_launches"], "clocks": mixed["clocks"],
+            "launch": mixed["launch"], "e2e": e2e, "fp64_plain": fp64, "ensemble": ens,
+        }
+    else:
+        line.pop("_energy", None)
     if rank == 0:
         if args.no_cpu_baseline:
             line["cpu_baseline"] = None

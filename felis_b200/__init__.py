@@ -31,6 +31,7 @@ STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA_ERROR", 3: "THETA_OVERFLOW", 4: 
                 6: "TIMEOUT", 7: "UNSUPPORTED", 8: "NO_DEVICE", 9: "IO", 10: "NOT_FOUND"}
 STATIC, TIME_DEPENDENT = 1, 2
 KERNEL_KINDS = {"particles": 0, "deposit": 1, "adi": 2, "reduce": 3, "shift": 4}
+BATCH_KERNEL_KINDS = {"adi": 0, "push": 1, "reduce": 2}
 BIPOLAR, QUADPOLAR = 1, 2
 FP64, MIXED = 0, 1
 
@@ -126,6 +127,8 @@ _sig("felis_batch_set_launch", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_batch_get_launch", C.c_int, _vp, _i32p, _i32p)
 _sig("felis_batch_tune", C.c_int, _vp, C.c_int32, C.c_int32, _i32p)
 _sig("felis_batch_last_run_ms", C.c_int, _vp, _dp)
+_sig("felis_batch_profile", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_batch_kernel_stats", C.c_int, _vp, C.c_int32, _i64p, _dp)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
 _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
@@ -488,6 +491,15 @@ class Batch:
         ms = C.c_double(0)
         self._ck(_lib.felis_batch_last_run_ms(self._b, C.byref(ms)))
         return ms.value
+
+    def profile(self, enable: bool, max_launches: int = 0):
+        self._ck(_lib.felis_batch_profile(self._b, 1 if enable else 0, max_launches))
+
+    def kernel_stats(self, kind: int = -1) -> tuple[int, float]:
+        n = C.c_int64(0)
+        ms = C.c_double(0)
+        self._ck(_lib.felis_batch_kernel_stats(self._b, kind, C.byref(n), C.byref(ms)))
+        return n.value, ms.value
 
 
 def device_info() -> tuple[str, int]:

@@ -87,6 +87,9 @@ struct felis_handle {
   std::vector<void*> adi_dev;
   AdiTab* d_adi = nullptr;
   int nxp = 0;
+  double2* adi_scratch = nullptr;  // planes larger than shared memory: one per CTA
+  int adi_big_grid = 0;
+  int sms = 148;
   // diagnostics
   double* d_part = nullptr;
   int diag_stride = 0;
@@ -475,9 +478,11 @@ felis_status run_adi(felis_handle* h, int use_source) {
   a.tab = h->d_adi;
   a.energy = h->d_planes;
   a.nxp = h->nxp;
+  a.scratch = h->adi_scratch;
   {
     KernelScope ks(h, FELIS_KERNEL_ADI);
-    launch_adi(a, h->st);
+    if (h->adi_scratch) launch_adi_big(a, h->adi_big_grid, h->st);
+    else launch_adi(a, h->st);
   }
   CK(cudaGetLastError());
   return FELIS_OK;
@@ -670,6 +675,7 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
     h->err = m;
   };
   cudaError_t ce = cudaGetDevice(&h->device);
+  if (ce == cudaSuccess) cudaDeviceGetAttribute(&h->sms, cudaDevAttrMultiProcessorCount, h->device);
   if (ce == cudaSuccess) ce = cudaStreamCreateWithFlags(&h->st, cudaStreamNonBlocking);
   const size_t N = (size_t)nx * ny;
   if (ce == cudaSuccess) ce = cudaMalloc(&h->U, (size_t)H * 2 * S * N * sizeof(double2));
@@ -743,8 +749,15 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
     const size_t smem = adi_smem_bytes(nx, ny, h->nxp);
     int dev_smem = 0;
     cudaDeviceGetAttribute(&dev_smem, cudaDevAttrMaxSharedMemoryPerBlockOptin, h->device);
-    if (st == FELIS_OK && (int)smem > dev_smem) bail(FELIS_UNSUPPORTED, "FP64 ADI plane does not fit in shared memory (grid too large)");
-    if (st == FELIS_OK) adi_set_smem(smem);
+    if (st == FELIS_OK && (int)smem <= dev_smem - 1024) {
+      adi_set_smem(smem);
+    } else if (st == FELIS_OK) {
+      // plane larger than shared memory: global-memory sweeps, one scratch
+      // plane per CTA of a persistent grid
+      h->adi_big_grid = std::min(S * H * 2, h->sms * 2);
+      if (cudaMalloc(&h->adi_scratch, (size_t)h->adi_big_grid * nx * ny * sizeof(double2)) != cudaSuccess)
+        bail(FELIS_CUDA_ERROR, "ADI scratch allocation failed");
+    }
     if (st == FELIS_OK && std::max(nx, ny) > 256) bail(FELIS_UNSUPPORTED, "grid wider than 256 points");
   }
   // geometry
@@ -774,7 +787,8 @@ void felis_destroy(felis_handle* h) {
   void* ptrs[] = {h->x, h->y, h->px, h->py, h->th, h->ga, h->d_soff, h->d_weight, h->d_tiles, h->U, h->Sc, h->box,
                   h->Ez, h->d_bessel, h->d_wake, h->d_log, h->d_adi, h->d_part, h->d_planes, h->d_planes2,
                   h->d_hist_e, h->d_hist_t, h->d_hist_b, h->d_tmp, h->d_l1, h->d_err,
-                  h->dep.key, h->dep.rkey, h->dep.wx1, h->dep.wy1, h->dep.wr1, h->dep.coef, h->dep.fx, h->dep.fy, h->dep.ez};
+                  h->dep.key, h->dep.rkey, h->dep.wx1, h->dep.wy1, h->dep.wr1, h->dep.coef, h->dep.fx, h->dep.fy, h->dep.ez,
+                  h->adi_scratch};
   for (void* q : ptrs) if (q) cudaFree(q);
   for (void* q : h->adi_dev) if (q) cudaFree(q);
   if (h->h_err) cudaFreeHost(h->h_err);

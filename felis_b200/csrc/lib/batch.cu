@@ -224,8 +224,21 @@ void adi_tables(const felis_params& p, int hidx, int M, std::vector<float2>& out
 
 }  // namespace
 
+// ADI planes of one grid size: one launch each, so that small grids are not
+// given the shared memory of the largest.
+struct AdiClass {
+  int nx, ny, offset, count, threads, smem;
+};
+
 struct felis_batch {
   std::vector<Inst> in;
+  std::vector<AdiClass> adi_classes;
+  // event-timed launches (felis_batch_profile)
+  bool prof = false, capturing = false;
+  std::vector<cudaEvent_t> ev;
+  size_t ev_used = 0;
+  std::vector<std::pair<int, size_t>> marks;
+  int64_t launches[FELIS_BATCH_KERNEL_KINDS] = {0};
   int device = 0, sms = 0, dev_smem = 0;
   cudaStream_t st = nullptr;
   std::string err;
@@ -238,7 +251,7 @@ struct felis_batch {
   int steps_cap = 0;
   double *d_he = nullptr, *d_ht = nullptr, *d_hb = nullptr;
   int hist_n = 0;
-  int adi_threads = 128, adi_smem = 0;
+  int adi_smem_max = 0;
   int push_threads = 128, push_smem = 0, adi_ctas = 2;
   bool layout_ready = false;
   int src_valid_it = -1;  // iteration whose solveField source is in the buffers
@@ -261,6 +274,26 @@ felis_status bfail(felis_batch* b, felis_status s, const std::string& m) {
   if (b) b->err = m;
   return s;
 }
+
+struct BatchScope {
+  felis_batch* b;
+  int kind;
+  size_t slot = (size_t)-1;
+  BatchScope(felis_batch* bb, int k) : b(bb), kind(k) {
+    b->launches[k] += 1;
+    if (b->prof && b->ev_used + 2 <= b->ev.size()) {
+      slot = b->ev_used;
+      b->ev_used += 2;
+      cudaEventRecordWithFlags(b->ev[slot], b->st, b->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+    }
+  }
+  ~BatchScope() {
+    if (slot != (size_t)-1) {
+      cudaEventRecordWithFlags(b->ev[slot + 1], b->st, b->capturing ? cudaEventRecordExternal : cudaEventRecordDefault);
+      b->marks.emplace_back(kind, slot);
+    }
+  }
+};
 
 felis_status upload_inst_table(felis_batch* b) {
   std::vector<BInst> h(b->in.size());
@@ -401,21 +434,33 @@ felis_status prepare(felis_batch* b) {
   // work lists, longest items first (the hardware block scheduler then runs a
   // longest-processing-time schedule): ADI planes by their sweep length,
   // slices by their particle count
-  std::vector<int4> adi, push;
-  std::vector<double> ca, cp;
+  std::vector<int4> push;
+  std::vector<double> cp;
+  std::map<std::pair<int, int>, std::vector<int4>> by_grid;
   for (size_t k = 0; k < b->in.size(); ++k) {
     const Inst& I = b->in[k];
     std::vector<int64_t> so(I.p.slice_n + 1);
     BCK(cudaMemcpy(so.data(), I.soff, so.size() * sizeof(int64_t), cudaMemcpyDeviceToHost));
+    std::vector<int4>& g = by_grid[std::make_pair(I.p.nx, I.p.ny)];
     for (int s = 0; s < I.p.slice_n; ++s) {
       push.push_back(make_int4((int)k, s, 0, 0));
       cp.push_back((double)(so[s + 1] - so[s]));
-      for (int hp = 0; hp < 2 * I.p.num_harmony; ++hp) {
-        adi.push_back(make_int4((int)k, s, hp, 0));
-        ca.push_back((double)(I.p.nx + I.p.ny) * I.p.nx);
-      }
+      for (int hp = 0; hp < 2 * I.p.num_harmony; ++hp) g.push_back(make_int4((int)k, s, hp, 0));
     }
   }
+  // largest grids first
+  std::vector<int4> adi;
+  b->adi_classes.clear();
+  for (auto it = by_grid.rbegin(); it != by_grid.rend(); ++it) {
+    AdiClass c{};
+    c.nx = it->first.first;
+    c.ny = it->first.second;
+    c.offset = (int)adi.size();
+    c.count = (int)it->second.size();
+    adi.insert(adi.end(), it->second.begin(), it->second.end());
+    b->adi_classes.push_back(c);
+  }
+  std::vector<double> ca(adi.size(), 0.0);
   auto sorted = [](std::vector<int4>& w, const std::vector<double>& c) {
     std::vector<int> o(w.size());
     for (size_t k = 0; k < o.size(); ++k) o[k] = (int)k;
@@ -424,7 +469,6 @@ felis_status prepare(felis_batch* b) {
     for (size_t k = 0; k < o.size(); ++k) r[k] = w[o[k]];
     w.swap(r);
   };
-  sorted(adi, ca);
   sorted(push, cp);
   b->n_adi = (int)adi.size();
   b->n_push = (int)push.size();
@@ -446,20 +490,27 @@ felis_status prepare(felis_batch* b) {
 // read from global memory); the push holds the accumulators of up to 6144 source
 // cells (larger boxes accumulate in the source buffer in global memory).
 felis_status ensure_launch(felis_batch* b) {
-  const int M32 = ((std::max(b->nx_max, b->ny_max) + 31) / 32) * 32;
-  if (M32 > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
-  b->adi_threads = std::max(M32, 64);
-  const size_t base = batch_adi_smem(b->nx_max, b->ny_max, 0);
-  if ((int)base > b->dev_smem) return bfail(b, FELIS_UNSUPPORTED, "field plane does not fit in shared memory");
-  const size_t per = (size_t)(b->dev_smem / b->adi_ctas - 1024);
-  size_t src_cells = 0;
-  if (base <= per) src_cells = (per - base) / sizeof(float2);
-  else src_cells = ((size_t)b->dev_smem - base) / sizeof(float2);
-  src_cells = std::min(src_cells, (size_t)b->N_max);
-  b->adi_smem = (int)batch_adi_smem(b->nx_max, b->ny_max, (int)src_cells);
+  b->adi_smem_max = 0;
+  for (AdiClass& c : b->adi_classes) {
+    const int M32 = ((std::max(c.nx, c.ny) + 31) / 32) * 32;
+    if (M32 > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
+    c.threads = std::max(M32, 64);
+    // 1 KB of every CTA's share stays for static shared memory
+    const size_t cap = (size_t)b->dev_smem - 1024;
+    const size_t base = batch_adi_smem(c.nx, c.ny, 0);
+    if (base > cap) return bfail(b, FELIS_UNSUPPORTED, "field plane does not fit in shared memory");
+    const size_t per = (size_t)(b->dev_smem / b->adi_ctas - 2048);
+    size_t src_cells = 0;
+    if (base <= per) src_cells = (per - base) / sizeof(float2);
+    else src_cells = (cap - base) / sizeof(float2);
+    src_cells = std::min(src_cells, (size_t)c.nx * c.ny);
+    c.smem = (int)batch_adi_smem(c.nx, c.ny, (int)src_cells);
+    b->adi_smem_max = std::max(b->adi_smem_max, c.smem);
+  }
   const int box = std::min(b->N_max, 6144);
   b->push_smem = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, box);
-  batch_set_smem(b->H_max, b->adi_smem, b->push_smem);
+  if (batch_set_smem(b->H_max, b->adi_smem_max, b->push_smem) != cudaSuccess)
+    return bfail(b, FELIS_UNSUPPORTED, "shared memory of the ensemble launches exceeds the device limit");
   return FELIS_OK;
 }
 
@@ -470,6 +521,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
   const BStep* row_d0 = b->d_steps + (size_t)steps * n;
   if (it0 < b->hist_n) {
     // diagnostics of the state at it0 (row d0 carries the ring offset, no shift)
+    BatchScope ks(b, FELIS_BATCH_KERNEL_REDUCE);
     launch_batch_measure(b->d_inst, row_d0, b->d_push_work, b->n_push, b->st);
     launch_batch_reduce(b->d_inst, n, row_d0, b->d_he + (size_t)it0 * se, b->d_ht + (size_t)it0 * stt,
                         b->d_hb + (size_t)it0 * sb, se * b->hist_n, stt * b->hist_n, sb * b->hist_n, b->st);
@@ -478,20 +530,29 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
     BatchLaunch d{};
     d.inst = b->d_inst; d.step = row_d0; d.work = b->d_push_work; d.nwork = b->n_push;
     d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY;
+    BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
     launch_batch_push(d, b->H_max, b->push_threads, b->st);
   }
   for (int it = it0; it < it1; ++it) {
     const BStep* T = b->d_steps + (size_t)(it - it0) * n;
-    BatchLaunch a{};
-    a.inst = b->d_inst; a.step = T; a.work = b->d_adi_work; a.nwork = b->n_adi; a.smem_bytes = b->adi_smem;
-    launch_batch_adi(a, b->adi_threads, b->st);
-    BatchLaunch p{};
-    p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
-    p.mode = BATCH_PUSH;
-    launch_batch_push(p, b->H_max, b->push_threads, b->st);
-    if (it + 1 < b->hist_n)
+    for (const AdiClass& c : b->adi_classes) {
+      BatchLaunch a{};
+      a.inst = b->d_inst; a.step = T; a.work = b->d_adi_work + c.offset; a.nwork = c.count; a.smem_bytes = c.smem;
+      BatchScope ks(b, FELIS_BATCH_KERNEL_ADI);
+      launch_batch_adi(a, c.threads, b->st);
+    }
+    {
+      BatchLaunch p{};
+      p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
+      p.mode = BATCH_PUSH;
+      BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
+      launch_batch_push(p, b->H_max, b->push_threads, b->st);
+    }
+    if (it + 1 < b->hist_n) {
+      BatchScope ks(b, FELIS_BATCH_KERNEL_REDUCE);
       launch_batch_reduce(b->d_inst, n, T, b->d_he + (size_t)(it + 1) * se, b->d_ht + (size_t)(it + 1) * stt,
                           b->d_hb + (size_t)(it + 1) * sb, se * b->hist_n, stt * b->hist_n, sb * b->hist_n, b->st);
+    }
   }
   BCK(cudaGetLastError());
   return FELIS_OK;
@@ -641,6 +702,7 @@ void felis_batch_destroy(felis_batch* b) {
   void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_he, b->d_ht, b->d_hb};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (b->h_err) cudaFreeHost(b->h_err);
+  for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
   if (b->st) cudaStreamDestroy(b->st);
   delete b;
 }
@@ -786,7 +848,9 @@ felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1) {
   cudaGraph_t graph = nullptr;
   cudaGraphExec_t exec = nullptr;
   BCK(cudaStreamBeginCapture(b->st, cudaStreamCaptureModeThreadLocal));
+  b->capturing = true;
   s = enqueue_run(b, it0, it1, deposit0);
+  b->capturing = false;
   cudaError_t ce = cudaStreamEndCapture(b->st, &graph);
   if (s != FELIS_OK) { if (graph) cudaGraphDestroy(graph); restore(); return s; }
   if (ce != cudaSuccess) { restore(); return bfail(b, FELIS_CUDA_ERROR, std::string("capture: ") + cudaGetErrorString(ce)); }
@@ -852,6 +916,38 @@ felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_
   std::tie(b->push_threads, b->adi_ctas) = pick;
   cache[key] = pick;
   *next_it = it;
+  return FELIS_OK;
+}
+
+felis_status felis_batch_profile(felis_batch* b, int32_t enable, int32_t max_launches) {
+  if (!b || max_launches < 0) return FELIS_BAD_ARG;
+  BCK(cudaStreamSynchronize(b->st));
+  b->prof = enable != 0;
+  b->marks.clear();
+  b->ev_used = 0;
+  for (int k = 0; k < FELIS_BATCH_KERNEL_KINDS; ++k) b->launches[k] = 0;
+  while (b->prof && b->ev.size() < 2 * (size_t)max_launches) {
+    cudaEvent_t e;
+    BCK(cudaEventCreate(&e));
+    b->ev.push_back(e);
+  }
+  return FELIS_OK;
+}
+
+felis_status felis_batch_kernel_stats(felis_batch* b, int32_t kind, int64_t* launches, double* total_ms) {
+  if (!b || kind < -1 || kind >= FELIS_BATCH_KERNEL_KINDS) return FELIS_BAD_ARG;
+  BCK(cudaStreamSynchronize(b->st));
+  int64_t n = 0;
+  if (kind < 0) for (int k = 0; k < FELIS_BATCH_KERNEL_KINDS; ++k) n += b->launches[k];
+  else n = b->launches[kind];
+  double ms = 0.0;
+  for (const auto& m : b->marks) {
+    if (kind >= 0 && m.first != kind) continue;
+    float t = 0.f;
+    if (cudaEventElapsedTime(&t, b->ev[m.second], b->ev[m.second + 1]) == cudaSuccess) ms += t;
+  }
+  if (launches) *launches = n;
+  if (total_ms) *total_ms = ms;
   return FELIS_OK;
 }
 

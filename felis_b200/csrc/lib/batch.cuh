@@ -90,7 +90,7 @@ size_t batch_adi_smem(int nx_max, int ny_max, int src_cells);
 // Shared memory of the push launch with room for the accumulators of
 // `box_cells` source cells of every source plane.
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells);
-void batch_set_smem(int H, int adi_bytes, int push_bytes);
+cudaError_t batch_set_smem(int H, int adi_bytes, int push_bytes);
 // CTAs of each kernel that fit on one SM with this shape.
 int batch_resident_adi(int threads, int smem_bytes);
 int batch_resident_push(int H, int threads, int smem_bytes);

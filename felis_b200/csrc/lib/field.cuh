@@ -32,6 +32,7 @@ struct AdiLaunch {
   const AdiTab* tab;   // [H] (device array of structs)
   double* energy;      // [H][2][S] plane sums of |U|^2 after the solve (may be null)
   int nxp;             // padded row length of the shared-memory plane
+  double2* scratch;    // k_adi_big: one plane per CTA
 };
 
 struct DepositLaunch {
@@ -56,6 +57,9 @@ void deposit_set_smem(size_t bytes);
 void adi_set_smem(size_t bytes);
 void launch_adi(const AdiLaunch& a, cudaStream_t st);
 size_t adi_smem_bytes(int nx, int ny, int nxp);
+// Planes larger than shared memory: `grid` CTAs, each with one scratch plane.
+void launch_adi_big(const AdiLaunch& a, int grid, cudaStream_t st);
+size_t adi_big_smem_bytes(int nx, int ny);
 void launch_energy(const DevGeom& G, const double2* U, int ring_base, double* out_planes, cudaStream_t st);
 void launch_sum_planes(const double* planes, int H, int S, int skip_last, double* out, cudaStream_t st);
 

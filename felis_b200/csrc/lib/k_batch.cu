@@ -860,9 +860,10 @@ size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
   return head + area;
 }
 
-void batch_set_smem(int H, int adi_bytes, int push_bytes) {
-  cudaFuncSetAttribute(k_batch_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, adi_bytes);
-  cudaFuncSetAttribute(push_kernel(H), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
+cudaError_t batch_set_smem(int H, int adi_bytes, int push_bytes) {
+  cudaError_t e = cudaFuncSetAttribute(k_batch_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, adi_bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(push_kernel(H), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
+  return e;
 }
 
 int batch_resident_adi(int threads, int smem_bytes) {

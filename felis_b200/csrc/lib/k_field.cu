@@ -573,6 +573,130 @@ __global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
   }
 }
 
+// ADI of planes too large for shared memory: the same arithmetic in the same
+// order as k_adi, with the plane in global memory.  The x sweep writes its
+// result to a per-CTA scratch plane X (so the rows never wait for one another)
+// and the y sweep reads X and writes U in place; one CTA per plane, planes
+// taken in a grid-stride loop.
+__global__ void __launch_bounds__(256) k_adi_big(AdiLaunch a) {
+  extern __shared__ double2 Atb[];  // recurrence tables of the harmonic
+  __shared__ double red[8];
+  const DevGeom& G = a.G;
+  const int S = G.S, nx = G.nx, ny = G.ny, N = G.N;
+  const int tid = threadIdx.x;
+  double2* X = a.scratch + (size_t)blockIdx.x * N;
+  cd* tx = reinterpret_cast<cd*>(Atb);
+  cd* ty = tx + 4 * nx;
+  double* dx_ = reinterpret_cast<double*>(ty + 4 * ny);
+  double* dy_ = dx_ + 3 * nx;
+  int staged_h = -1;
+  for (int plane = blockIdx.x; plane < S * G.H * 2; plane += gridDim.x) {
+    const int s = plane % S, hp = plane / S, h = hp >> 1, pol = hp & 1;
+    const AdiTab Tg = a.tab[h];
+    if (h != staged_h) {
+      __syncthreads();
+      for (int k = tid; k < nx; k += blockDim.x) {
+        tx[k] = Tg.ax_p[k]; tx[nx + k] = Tg.ax_a[k]; tx[2 * nx + k] = Tg.ax_q[k]; tx[3 * nx + k] = Tg.ax_cc[k];
+        dx_[k] = Tg.ax_pinv[k]; dx_[nx + k] = Tg.ax_qinv[k]; dx_[2 * nx + k] = Tg.ax_ccinv[k];
+      }
+      for (int k = tid; k < ny; k += blockDim.x) {
+        ty[k] = Tg.ay_p[k]; ty[ny + k] = Tg.ay_a[k]; ty[2 * ny + k] = Tg.ay_q[k]; ty[3 * ny + k] = Tg.ay_cc[k];
+        dy_[k] = Tg.ay_pinv[k]; dy_[ny + k] = Tg.ay_qinv[k]; dy_[2 * ny + k] = Tg.ay_ccinv[k];
+      }
+      staged_h = h;
+      __syncthreads();
+    }
+    AdiTab T = Tg;
+    T.ax_p = tx; T.ax_a = tx + nx; T.ax_q = tx + 2 * nx; T.ax_cc = tx + 3 * nx;
+    T.ax_pinv = dx_; T.ax_qinv = dx_ + nx; T.ax_ccinv = dx_ + 2 * nx;
+    T.ay_p = ty; T.ay_a = ty + ny; T.ay_q = ty + 2 * ny; T.ay_cc = ty + 3 * ny;
+    T.ay_pinv = dy_; T.ay_qinv = dy_ + ny; T.ay_ccinv = dy_ + 2 * ny;
+    double2* U = a.U + field_plane(S, h, pol, s, a.ring_base) * N;
+    const double2* Sc = a.Sc + ((size_t)hp * S + s) * N;
+    const int4 bx = a.box[s];
+    const bool src = a.use_source != 0;
+    // ---- x sweep: thread per row j, result in X ----
+    const int j = tid;
+    if (j >= 1 && j <= ny - 2) {
+      const cd rm = T.rx_m[j], r0 = T.rx_0[j], rp = T.rx_p[j];
+      const bool rowin = src && j >= bx.z && j <= bx.w;
+      cd DD = C(0, 0);
+      for (int i = 1; i <= nx - 2; ++i) {
+        const double2 up = U[(j + 1) * nx + i], u0 = U[j * nx + i], um = U[(j - 1) * nx + i];
+        cd t = cmul(rm, C(up.x, up.y));
+        t = cadd(t, cmul(r0, C(u0.x, u0.y)));
+        t = csub(t, cmul(rp, C(um.x, um.y)));
+        if (rowin && i >= bx.x && i <= bx.y) {
+          const double2 sv = Sc[j * nx + i];
+          t = cadd(t, C(sv.x, sv.y));
+        }
+        if (i == 1) {
+          DD = cdiv_inv(t, T.ax_p[1], T.ax_pinv[1]);
+        } else if (i < nx - 2) {
+          DD = csub(cdiv_inv(t, T.ax_p[i], T.ax_pinv[i]), cdiv_inv(cmul(T.ax_a[i], DD), T.ax_q[i], T.ax_qinv[i]));
+        } else {
+          DD = csub(t, cdiv_inv(DD, T.ax_cc[nx - 3], T.ax_ccinv[nx - 3]));
+        }
+        X[j * nx + i] = make_double2(DD.re, DD.im);
+      }
+      cd Uc = cdiv_inv(DD, T.ax_cc[nx - 2], T.ax_ccinv[nx - 2]);
+      X[j * nx + nx - 2] = make_double2(Uc.re, Uc.im);
+      for (int i = nx - 3; i > 0; --i) {
+        const double2 d = X[j * nx + i];
+        Uc = cdiv_inv(csub(C(d.x, d.y), Uc), T.ax_cc[i], T.ax_ccinv[i]);
+        X[j * nx + i] = make_double2(Uc.re, Uc.im);
+      }
+      X[j * nx + 0] = make_double2(0.0, 0.0);
+      X[j * nx + nx - 1] = make_double2(0.0, 0.0);
+    }
+    __syncthreads();
+    // ---- y sweep: thread per column i, reads X, writes U in place ----
+    const int i = tid;
+    if (i >= 1 && i <= nx - 2) {
+      const cd rm = T.ry_m[i], r0 = T.ry_0[i], rp = T.ry_p[i];
+      const bool colin = src && i >= bx.x && i <= bx.y;
+      cd DD = C(0, 0);
+      for (int jr = 1; jr <= ny - 2; ++jr) {
+        const double2 up = X[jr * nx + i + 1], u0 = X[jr * nx + i], um = X[jr * nx + i - 1];
+        cd t = cmul(rm, C(up.x, up.y));
+        t = cadd(t, cmul(r0, C(u0.x, u0.y)));
+        t = csub(t, cmul(rp, C(um.x, um.y)));
+        if (colin && jr >= bx.z && jr <= bx.w) {
+          const double2 sv = Sc[jr * nx + i];
+          t = cadd(t, C(sv.x, sv.y));
+        }
+        if (jr == 1) {
+          DD = cdiv_inv(t, T.ay_p[1], T.ay_pinv[1]);
+        } else if (jr < ny - 2) {
+          DD = csub(cdiv_inv(t, T.ay_p[jr], T.ay_pinv[jr]), cdiv_inv(cmul(T.ay_a[jr], DD), T.ay_q[jr], T.ay_qinv[jr]));
+        } else {
+          DD = csub(t, cdiv_inv(DD, T.ay_cc[ny - 3], T.ay_ccinv[ny - 3]));
+        }
+        U[jr * nx + i] = make_double2(DD.re, DD.im);
+      }
+      cd Un = cdiv_inv(DD, T.ay_cc[ny - 2], T.ay_ccinv[ny - 2]);
+      U[(ny - 2) * nx + i] = make_double2(Un.re, Un.im);
+      for (int jr = ny - 3; jr > 0; --jr) {
+        const double2 d = U[jr * nx + i];
+        Un = cdiv_inv(csub(C(d.x, d.y), Un), T.ay_cc[jr], T.ay_ccinv[jr]);
+        U[jr * nx + i] = make_double2(Un.re, Un.im);
+      }
+    }
+    __syncthreads();
+    // ---- |U|^2 over the plane (edge rows and columns keep their values) ----
+    double e = 0.0;
+    for (int k = tid; k < N; k += blockDim.x) {
+      const double2 v = U[k];
+      e += v.x * v.x + v.y * v.y;
+    }
+    if (a.energy) {
+      const double t = block_sum(e, red);
+      if (tid == 0) a.energy[(size_t)hp * S + s] = t;
+    }
+    __syncthreads();
+  }
+}
+
 // Plane sums of |U|^2 (updateTotalEnergy.cpp:25-33), one block per plane.
 __global__ void __launch_bounds__(256) k_energy(DevGeom G, const double2* U, int ring_base, double* out) {
   __shared__ double red[8];
@@ -625,6 +749,16 @@ void launch_adi(const AdiLaunch& a, cudaStream_t st) {
   const int mx = a.G.nx > a.G.ny ? a.G.nx : a.G.ny;
   const int threads = ((mx + 31) / 32) * 32;
   k_adi<<<a.G.S * a.G.H * 2, threads, adi_smem_bytes(a.G.nx, a.G.ny, a.nxp), st>>>(a);
+}
+
+size_t adi_big_smem_bytes(int nx, int ny) {
+  return (size_t)4 * (nx + ny) * sizeof(double2) + (size_t)3 * (nx + ny) * sizeof(double);
+}
+
+void launch_adi_big(const AdiLaunch& a, int grid, cudaStream_t st) {
+  const int mx = a.G.nx > a.G.ny ? a.G.nx : a.G.ny;
+  const int threads = ((mx + 31) / 32) * 32;
+  k_adi_big<<<grid, threads, adi_big_smem_bytes(a.G.nx, a.G.ny), st>>>(a);
 }
 
 void launch_energy(const DevGeom& G, const double2* U, int ring_base, double* out_planes, cudaStream_t st) {

@@ -311,6 +311,17 @@ felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32
 felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it);
 /* Device time of the last felis_batch_run graph launch. */
 felis_status felis_batch_last_run_ms(felis_batch* b, double* ms);
+/* Kernel kinds of the ensemble, event-timed like felis_profile /
+ * felis_kernel_stats (the measure + reduce pair of a run's first iteration
+ * counts as one REDUCE launch). */
+enum {
+  FELIS_BATCH_KERNEL_ADI = 0,    /* field planes of one grid size */
+  FELIS_BATCH_KERNEL_PUSH = 1,   /* push + next deposit (or the first deposit) */
+  FELIS_BATCH_KERNEL_REDUCE = 2, /* per-instance diagnostics */
+  FELIS_BATCH_KERNEL_KINDS = 4
+};
+felis_status felis_batch_profile(felis_batch* b, int32_t enable, int32_t max_launches);
+felis_status felis_batch_kernel_stats(felis_batch* b, int32_t kind, int64_t* launches, double* total_ms);
 
 /* ---- host-side setup of the reference's input format -------------------- */
 /* Parses a FELIS input file ([Domain], [Save], [Seed], [Undulator], [Quad],

@@ -212,3 +212,28 @@ def test_errors_are_reported(fb, seeded):
         b.run(0, 1)  # no particles uploaded
     with pytest.raises(fb.FelisError):
         b.set_launch(100, 1)
+
+
+def test_grid_classes_and_uneven_instances(fb, tmp_path):
+    """Instances of the three ensemble grid sizes (ADI launch per size, the
+    largest planes filling one SM's shared memory) with uneven slice counts:
+    every instance tracks its own FP64 plain run."""
+    from felis_b200 import analysis
+
+    cases = []
+    for k, (slices, nx) in enumerate(((24, 65), (8, 151), (16, 101))):
+        d = tmp_path / f"g{k}"
+        d.mkdir()
+        cases.append(make_case(fb, d, kind="sase", slices=slices, beamlets=128, nx=nx, total_length=1.0,
+                               seed_power=1e5, energy_mev=1000.0, seed=k + 5))
+    steps = 30
+    b = fb.Batch([c[0].params for c in cases])
+    for k, c in enumerate(cases):
+        _upload(fb, b, k, *c)
+    b.run(0, steps)
+    for k, (cfg, beam, fields) in enumerate(cases):
+        g = _fp64(fb, cfg, beam, fields, steps)
+        P64 = analysis.output_power(g.diagnostics(0, steps + 1)[0])
+        P32 = analysis.output_power(b.diagnostics(k, 0, steps + 1)[0])
+        rel = np.abs(P32 - P64) / P64
+        assert rel.max() < POWER_RTOL, (k, rel.max())

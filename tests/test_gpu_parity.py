@@ -192,3 +192,22 @@ def test_multichunk_deposit_bit_exact(fb, oracle_mod, tmp_path, kw):
     _particles_equal(g, o, "multichunk")
     _fields_equal(g, o, H, "multichunk")
     assert_bits(g.download_ez()[:, 1:-1], o.get_ez()[:, 1:-1], "multichunk Ez")
+
+
+@pytest.mark.parametrize("kw", [
+    dict(slices=3, beamlets=256, nx=151, total_length=1.0, seed_power=1e6),
+    dict(slices=2, beamlets=128, nx=131, total_length=0.6, harmonics=(1, 2), undulator="QuadPolar",
+         polarity=0.5, seed_power=1e6),
+])
+def test_large_grid_adi_bit_exact(fb, oracle_mod, tmp_path, kw):
+    """Grids whose FP64 plane exceeds shared memory take the global-memory ADI
+    (one scratch plane per CTA); results stay bit-identical."""
+    cfg, beam, fields = make_case(fb, tmp_path, kind="sase", **kw)
+    H = cfg.params.num_harmony
+    n = cfg.params.max_step
+    g, o = load_both(fb, oracle_mod, cfg, beam, fields)
+    g.run(0, n)
+    e0, _, _ = o.run(0, n)
+    _particles_equal(g, o, "large grid")
+    _fields_equal(g, o, H, "large grid")
+    np.testing.assert_allclose(g.diagnostics(0, n)[0], e0, rtol=1e-12, atol=1e-300)
