@@ -129,6 +129,17 @@ _sig("felis_batch_tune", C.c_int, _vp, C.c_int32, C.c_int32, _i32p)
 _sig("felis_batch_last_run_ms", C.c_int, _vp, _dp)
 _sig("felis_batch_profile", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_batch_kernel_stats", C.c_int, _vp, C.c_int32, _i64p, _dp)
+_fp = C.POINTER(C.c_float)
+_sig("felis_mlp_create", C.c_int, C.c_int32, C.c_int32, C.c_int32, C.c_uint64, C.POINTER(_vp))
+_sig("felis_mlp_destroy", None, _vp)
+_sig("felis_mlp_last_error", C.c_char_p, _vp)
+_sig("felis_mlp_param_count", C.c_int, _vp, _i64p)
+_sig("felis_mlp_get_params", C.c_int, _vp, _fp)
+_sig("felis_mlp_set_params", C.c_int, _vp, _fp)
+_sig("felis_mlp_forward", C.c_int, _vp, _fp, C.c_int64, _fp)
+_sig("felis_mlp_gradients", C.c_int, _vp, _fp, _fp, C.c_int64, _fp, _dp)
+_sig("felis_mlp_set_data", C.c_int, _vp, _fp, _fp, C.c_int64)
+_sig("felis_mlp_train", C.c_int, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64, _dp)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
 _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
@@ -500,6 +511,89 @@ class Batch:
         ms = C.c_double(0)
         self._ck(_lib.felis_batch_kernel_stats(self._b, kind, C.byref(n), C.byref(ms)))
         return n.value, ms.value
+
+
+def _f32(a) -> np.ndarray:
+    return np.ascontiguousarray(a, dtype=np.float32)
+
+
+def _pf(a: np.ndarray):
+    return a.ctypes.data_as(_fp)
+
+
+class MLP:
+    """felis_mlp: the taper-surrogate network (4 linear layers, GELU, BF16
+    tensor-core forward and backward, FP32 AdamW)."""
+
+    def __init__(self, n_in: int, width: int, n_out: int, seed: int = 1):
+        h = _vp()
+        st = _lib.felis_mlp_create(n_in, width, n_out, seed, C.byref(h))
+        if st != OK:
+            raise FelisError(st, "felis_mlp_create failed (see stderr)")
+        self._m = h
+        self.n_in, self.width, self.n_out = n_in, width, n_out
+        c = C.c_int64(0)
+        _lib.felis_mlp_param_count(h, C.byref(c))
+        self.n_params = c.value
+
+    def close(self):
+        if getattr(self, "_m", None):
+            _lib.felis_mlp_destroy(self._m)
+            self._m = None
+
+    def __del__(self):
+        self.close()
+
+    def _ck(self, st: int):
+        if st != OK:
+            raise FelisError(st, _lib.felis_mlp_last_error(self._m).decode())
+
+    def params(self) -> np.ndarray:
+        out = np.zeros(self.n_params, dtype=np.float32)
+        self._ck(_lib.felis_mlp_get_params(self._m, _pf(out)))
+        return out
+
+    def set_params(self, p):
+        p = _f32(p)
+        assert p.size == self.n_params
+        self._ck(_lib.felis_mlp_set_params(self._m, _pf(p)))
+
+    def unflatten(self, p: np.ndarray) -> list:
+        """[(W1, b1), ..., (W4, b4)] views of a flat parameter vector."""
+        dims = [(self.width, self.n_in), (self.width, self.width), (self.width, self.width), (self.n_out, self.width)]
+        out, k = [], 0
+        for r, c in dims:
+            W = p[k:k + r * c].reshape(r, c)
+            k += r * c
+            b = p[k:k + r]
+            k += r
+            out.append((W, b))
+        return out
+
+    def forward(self, x) -> np.ndarray:
+        x = _f32(x).reshape(-1, self.n_in)
+        y = np.zeros((x.shape[0], self.n_out), dtype=np.float32)
+        self._ck(_lib.felis_mlp_forward(self._m, _pf(x), x.shape[0], _pf(y)))
+        return y
+
+    def gradients(self, x, t) -> tuple[np.ndarray, float]:
+        x = _f32(x).reshape(-1, self.n_in)
+        t = _f32(t).reshape(-1, self.n_out)
+        g = np.zeros(self.n_params, dtype=np.float32)
+        loss = C.c_double(0)
+        self._ck(_lib.felis_mlp_gradients(self._m, _pf(x), _pf(t), x.shape[0], _pf(g), C.byref(loss)))
+        return g, loss.value
+
+    def set_data(self, x, t):
+        x = _f32(x).reshape(-1, self.n_in)
+        t = _f32(t).reshape(-1, self.n_out)
+        self._ck(_lib.felis_mlp_set_data(self._m, _pf(x), _pf(t), x.shape[0]))
+
+    def train(self, epochs: int, batch: int = 512, lr: float = 1e-3, weight_decay: float = 1e-4,
+              seed: int = 1) -> np.ndarray:
+        hist = np.zeros(epochs)
+        self._ck(_lib.felis_mlp_train(self._m, epochs, batch, lr, weight_decay, seed, _p(hist)))
+        return hist
 
 
 def device_info() -> tuple[str, int]:

@@ -33,6 +33,8 @@ UNITS = [
     ("lib/k_sort.cu", []),
     ("lib/batch.cu", []),
     ("lib/k_batch.cu", ["--use_fast_math"]),
+    ("lib/mlp.cu", []),
+    ("lib/k_mlp.cu", []),
     ("host/config.cpp", []),
 ]
 

@@ -1,0 +1,58 @@
+// Taper-surrogate MLP: tensor-core GEMM and the elementwise kernels of its
+// forward pass, backward pass and AdamW update.
+#pragma once
+
+#include <cuda_bf16.h>
+#include <cuda_runtime.h>
+#include <stdint.h>
+
+namespace felis {
+
+typedef __nv_bfloat16 bf16;
+
+// C[M][N] = A[M][K] . B[N][K]^T on the 5th-generation tensor cores (BF16
+// operands, FP32 accumulation in tensor memory), with an optional epilogue:
+//   z = C + bias[n]                (bias may be null)
+//   out_f32[m][n] = z              (may be null)
+//   out_bf16[m][n] = gelu ? GELU(z) : z   (may be null)
+// A and B are row-major with leading dimensions lda, ldb (elements, multiples
+// of 8); M is a multiple of 128, N a multiple of 16, K a multiple of 16.
+// Columns n >= n_valid of the outputs are written as 0.  err (may be null)
+// receives 1 when a tensor-core wait ran out.
+struct GemmArgs {
+  const bf16* A;
+  const bf16* B;
+  int M, N, K, lda, ldb;
+  const float* bias;
+  float* out_f32;
+  bf16* out_bf16;
+  int ldc;       // leading dimension of both outputs
+  int n_valid;
+  int gelu;
+  int* err;
+};
+void launch_gemm_tc(const GemmArgs& g, cudaStream_t st);
+// Shared-memory limit of the GEMM kernel (call once per device before use).
+cudaError_t gemm_tc_prepare();
+
+// Elementwise and reduction helpers (row-major [rows][cols] unless stated).
+void launch_f32_to_bf16(const float* in, bf16* out, int64_t n, cudaStream_t st);
+// out[c][r] = in[r][c] for r < rows, c < cols; rows_pad / cols_pad zero padding
+// of the destination ([cols_pad][rows_pad])
+void launch_transpose_bf16(const bf16* in, int rows, int cols, int ld_in, bf16* out, int rows_pad, int cols_pad,
+                           cudaStream_t st);
+// dz = g * GELU'(z), written as BF16
+void launch_gelu_backward(const float* z, const float* g, bf16* dz, int64_t n, cudaStream_t st);
+// dy = scale * (y - t) on real rows / columns, 0 elsewhere (y, t, dy all
+// [rows][cols_pad]); loss_part[b] = sum of (y - t)^2 of block b, blocks =
+// mse_blocks(rows)
+int mse_blocks(int rows);
+void launch_mse_grad(const float* y, const float* t, int rows, int rows_real, int cols_pad, int cols_real,
+                     float scale, bf16* dy, double* loss_part, cudaStream_t st);
+// column sums of a BF16 [rows][cols] matrix into FP32 out[cols] (fixed order)
+void launch_col_sum(const bf16* in, int rows, int cols, float* out, cudaStream_t st);
+// AdamW on n FP32 parameters; writes the BF16 copy
+void launch_adamw(float* w, const float* g, float* m, float* v, bf16* w_bf16, int64_t n, float lr, float b1,
+                  float b2, float eps, float wd, float bc1, float bc2, cudaStream_t st);
+
+}  // namespace felis

@@ -323,6 +323,38 @@ enum {
 felis_status felis_batch_profile(felis_batch* b, int32_t enable, int32_t max_launches);
 felis_status felis_batch_kernel_stats(felis_batch* b, int32_t kind, int64_t* launches, double* total_ms);
 
+/* ---- taper surrogate network ---------------------------------------------
+ * No counterpart in the reference.  A multilayer perceptron of four linear
+ * layers (n_in -> width -> width -> width -> n_out, GELU after the first
+ * three) that learns per-segment power and bandwidth from taper and beam
+ * parameters, trained on runs of the ensemble engine.  Forward and backward
+ * passes run on the tensor cores (BF16 weights and activations, FP32
+ * accumulation); FP32 master parameters with AdamW.  width is 128 or 256;
+ * n_in <= 256, n_out <= width.  Inputs and outputs are row-major FP32 host
+ * arrays, [n][n_in] and [n][n_out]; the loss is the mean squared error over
+ * all outputs (normalise the targets beforehand). */
+typedef struct felis_mlp felis_mlp;
+felis_status felis_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64_t seed, felis_mlp** out);
+void felis_mlp_destroy(felis_mlp* m);
+const char* felis_mlp_last_error(const felis_mlp* m);
+/* Parameters flattened as W1 [width][n_in], b1, W2, b2, W3, b3, W4 [n_out][width], b4. */
+felis_status felis_mlp_param_count(const felis_mlp* m, int64_t* count);
+felis_status felis_mlp_get_params(felis_mlp* m, float* out);
+/* Sets the parameters and resets the optimiser state. */
+felis_status felis_mlp_set_params(felis_mlp* m, const float* in);
+felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y);
+/* Gradient of the loss over n <= 65536 samples, in the parameter layout, and
+ * the loss itself. */
+felis_status felis_mlp_gradients(felis_mlp* m, const float* x, const float* t, int64_t n, float* grads,
+                                 double* loss);
+/* Training set kept on the device for felis_mlp_train. */
+felis_status felis_mlp_set_data(felis_mlp* m, const float* x, const float* t, int64_t n);
+/* Shuffled minibatches (batch a multiple of 128, at most 65536) with AdamW
+ * (beta 0.9 / 0.999, weight decay on the weights only); writes the mean loss
+ * of every epoch. */
+felis_status felis_mlp_train(felis_mlp* m, int32_t epochs, int32_t batch, float lr, float weight_decay,
+                             uint64_t seed, double* loss_per_epoch);
+
 /* ---- host-side setup of the reference's input format -------------------- */
 /* Parses a FELIS input file ([Domain], [Save], [Seed], [Undulator], [Quad],
  * [EBeam], [Wake_field], [Bessel_table], [Phase_shifter] blocks;

@@ -1,0 +1,144 @@
+"""Taper-surrogate network (felis_mlp_*) against a CPU computation of the same
+network.
+
+The GPU computes with BF16 weights and activations on the tensor cores and
+accumulates in FP32.  The CPU side (numpy, FP64) rounds to BF16 at the same
+places -- inputs, weights, hidden activations, and the backward operands dz
+-- so the forward outputs agree to accumulation-order rounding and the
+gradients to a few BF16 ulps in norm.
+"""
+import numpy as np
+import pytest
+from scipy.special import erf
+
+pytestmark = pytest.mark.gpu
+
+N_IN, WIDTH, N_OUT = 38, 256, 33
+FWD_ATOL = 2e-3      # forward, relative to the largest |output|
+GRAD_RTOL = 1e-2     # gradient blocks, relative in norm
+
+
+def bf16(a):
+    a = np.ascontiguousarray(a, dtype=np.float32)
+    u = a.view(np.uint32).astype(np.uint64)
+    u = (u + 0x7FFF + ((u >> 16) & 1)) & 0xFFFF0000
+    return u.astype(np.uint32).view(np.float32).astype(np.float64)
+
+
+def gelu(z):
+    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+
+
+def gelu_grad(z):
+    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+
+
+def cpu_forward(layers, x):
+    a = bf16(x)
+    zs, acts = [], [a]
+    for k, (W, b) in enumerate(layers):
+        z = a @ bf16(W).T + b.astype(np.float64)
+        zs.append(z)
+        if k < len(layers) - 1:
+            a = bf16(gelu(z))
+            acts.append(a)
+    return zs, acts
+
+
+def cpu_gradients(layers, x, t):
+    zs, acts = cpu_forward(layers, x)
+    n, n_out = t.shape
+    y = zs[-1]
+    loss = np.mean((y - t) ** 2)
+    dz = bf16(2.0 / (n * n_out) * (y - t))
+    grads = [None] * len(layers)
+    for k in range(len(layers) - 1, -1, -1):
+        W, _ = layers[k]
+        gW = dz.T @ acts[k]
+        gb = dz.sum(axis=0)
+        grads[k] = (gW, gb)
+        if k == 0:
+            break
+        da = dz @ bf16(W)
+        dz = bf16(da * gelu_grad(zs[k - 1]))
+    return grads, loss, y
+
+
+def random_params(m, rng, scale=1.0):
+    p = []
+    for (W, b) in m.unflatten(np.zeros(m.n_params, dtype=np.float32)):
+        fan_in = W.shape[1]
+        p.append(rng.normal(0, scale * np.sqrt(2.0 / fan_in), W.shape).ravel())
+        p.append(rng.normal(0, 0.1, b.shape))
+    return np.concatenate(p).astype(np.float32)
+
+
+@pytest.fixture
+def net(fb):
+    m = fb.MLP(N_IN, WIDTH, N_OUT, seed=3)
+    yield m
+    m.close()
+
+
+def test_forward_matches_cpu(net):
+    rng = np.random.default_rng(11)
+    p = random_params(net, rng)
+    net.set_params(p)
+    for n in (1, 300, 1024):
+        x = rng.normal(0, 1, (n, N_IN)).astype(np.float32)
+        y = net.forward(x)
+        zs, _ = cpu_forward(net.unflatten(p), x)
+        ref = zs[-1]
+        np.testing.assert_allclose(y, ref, rtol=0, atol=FWD_ATOL * np.abs(ref).max())
+
+
+def test_gradients_match_cpu(net):
+    rng = np.random.default_rng(12)
+    p = random_params(net, rng)
+    net.set_params(p)
+    x = rng.normal(0, 1, (384, N_IN)).astype(np.float32)
+    t = rng.normal(0, 1, (384, N_OUT)).astype(np.float32)
+    g, loss = net.gradients(x, t)
+    ref, ref_loss, _ = cpu_gradients(net.unflatten(p), x, t)
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-3)
+    for k, ((gW, gb), (rW, rb)) in enumerate(zip(net.unflatten(g), ref)):
+        ew = np.linalg.norm(gW - rW) / np.linalg.norm(rW)
+        eb = np.linalg.norm(gb - rb) / np.linalg.norm(rb)
+        assert ew < GRAD_RTOL, (k, "W", ew)
+        assert eb < GRAD_RTOL, (k, "b", eb)
+
+
+def test_gradients_ragged_batch(net):
+    """A batch that is not a multiple of 128: the padding rows carry no loss."""
+    rng = np.random.default_rng(13)
+    p = random_params(net, rng)
+    net.set_params(p)
+    x = rng.normal(0, 1, (200, N_IN)).astype(np.float32)
+    t = rng.normal(0, 1, (200, N_OUT)).astype(np.float32)
+    g, loss = net.gradients(x, t)
+    ref, ref_loss, _ = cpu_gradients(net.unflatten(p), x, t)
+    np.testing.assert_allclose(loss, ref_loss, rtol=1e-3)
+    gW, _ = net.unflatten(g)[0]
+    assert np.linalg.norm(gW - ref[0][0]) / np.linalg.norm(ref[0][0]) < GRAD_RTOL
+
+
+def test_training_fits_a_smooth_map(fb):
+    """AdamW on the device fits a smooth 38 -> 33 map: the loss falls by an
+    order of magnitude and held-out samples follow."""
+    rng = np.random.default_rng(14)
+    A = rng.normal(0, 1, (N_IN, 8)) / np.sqrt(N_IN)
+    B = rng.normal(0, 1, (8, N_OUT))
+
+    def f(x):
+        return np.tanh(x @ A) @ B / 2.0
+
+    x = rng.normal(0, 1, (8192, N_IN)).astype(np.float32)
+    y = f(x).astype(np.float32)
+    m = fb.MLP(N_IN, WIDTH, N_OUT, seed=5)
+    m.set_data(x, y)
+    hist = m.train(epochs=40, batch=512, lr=1e-3, weight_decay=1e-4)
+    assert hist[-1] < 0.1 * hist[0], hist
+    xt = rng.normal(0, 1, (1000, N_IN)).astype(np.float32)
+    err = np.mean((m.forward(xt) - f(xt)) ** 2) / np.mean(f(xt) ** 2)
+    assert err < 0.1, err
+    m.close()
