@@ -959,14 +959,22 @@ felis_status felis_batch_last_run_ms(felis_batch* b, double* ms) {
 
 felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t it0, int32_t it1, double* energy,
                                          double* twiss, double* bfactor) {
-  if (!b || inst < 0 || inst >= (int)b->in.size() || it0 < 0 || it1 < it0 || it1 > b->hist_n) return bfail(b, FELIS_BAD_ARG, "bad range");
+  if (!b || inst < 0 || inst >= (int)b->in.size() || it0 < 0 || it1 < it0 || it1 > b->hist_n)
+    return bfail(b, FELIS_BAD_ARG, "bad range");
+  if (it1 == it0) return FELIS_OK;
   BCK(cudaStreamSynchronize(b->st));
   const int H = b->in[inst].p.num_harmony, se = 2 * b->H_max, sb = 2 * b->H_max;
-  for (int it = it0; it < it1; ++it) {
-    if (energy) BCK(cudaMemcpy(energy + (size_t)(it - it0) * 2 * H, b->d_he + (size_t)inst * se * b->hist_n + (size_t)it * se, 2 * H * sizeof(double), cudaMemcpyDeviceToHost));
-    if (twiss) BCK(cudaMemcpy(twiss + (size_t)(it - it0) * 6, b->d_ht + (size_t)inst * 6 * b->hist_n + (size_t)it * 6, 6 * sizeof(double), cudaMemcpyDeviceToHost));
-    if (bfactor) BCK(cudaMemcpy(bfactor + (size_t)(it - it0) * 2 * H, b->d_hb + (size_t)inst * sb * b->hist_n + (size_t)it * sb, 2 * H * sizeof(double), cudaMemcpyDeviceToHost));
-  }
+  const size_t rows = (size_t)(it1 - it0);
+  // history rows of one instance are contiguous: one strided copy per array
+  if (energy)
+    BCK(cudaMemcpy2D(energy, 2 * H * sizeof(double), b->d_he + (size_t)inst * se * b->hist_n + (size_t)it0 * se,
+                     se * sizeof(double), 2 * H * sizeof(double), rows, cudaMemcpyDeviceToHost));
+  if (twiss)
+    BCK(cudaMemcpy(twiss, b->d_ht + (size_t)inst * 6 * b->hist_n + (size_t)it0 * 6, rows * 6 * sizeof(double),
+                   cudaMemcpyDeviceToHost));
+  if (bfactor)
+    BCK(cudaMemcpy2D(bfactor, 2 * H * sizeof(double), b->d_hb + (size_t)inst * sb * b->hist_n + (size_t)it0 * sb,
+                     sb * sizeof(double), 2 * H * sizeof(double), rows, cudaMemcpyDeviceToHost));
   return FELIS_OK;
 }
 

@@ -1,0 +1,231 @@
+"""Learned taper proposal.
+
+A network (`felis_b200.MLP`: 4 linear layers of width 256, GELU, BF16 tensor
+cores) learns, from runs that the batched engine itself generates, how the
+per-segment power of a FELIS run depends on the undulator taper and on six beam
+parameters.  It then ranks many candidate tapers for a given beam; the best
+ones are re-run by the plain FP64 method, which judges the network's error and
+takes over as a plain scan where that error exceeds 5 %.
+
+Runs.  Steady-state (Static) FELIS runs: 1 GeV class beam, 4096 quiet-start
+particles, 32 undulator segments of 40 periods (lambda_u 2.6 cm, no gaps,
+33.3 m, 1280 iterations), a Gaussian seed, grid key nx = 65.  Taper: per
+segment K_i = K0 (1 - a max(0, z_i - z0)^2) + N(0, 1e-4), z_i the segment's
+start, a in [0, 2e-4], z0 in [5, 30] m.  Beam parameters: peak current,
+relative energy spread, normalised emittance, matched beta, beam energy (the
+undulator stays resonant at the segment-0 K), seed power.
+
+Features (38): the 32 K_i / K0 - 1 and the 6 beam parameters (seed power as
+log10).  Targets (33): log10 of the field energy at the end of each segment
+(the per-iteration power sums of updateTotalEnergy.cpp:25-36, unscaled) and
+the final bunching |b1| (a steady-state run has one slice, hence no spectrum;
+the bunching stands in for the spectral bandwidth of a time-dependent run).
+"""
+from __future__ import annotations
+
+import os
+import tempfile
+import time
+
+import numpy as np
+
+SEGMENTS = 32
+PERIODS = 40
+LAMBDA_U_CM = 2.6
+SEG_LEN = PERIODS * LAMBDA_U_CM / 100.0
+K0 = 2.6
+STEPS = SEGMENTS * PERIODS
+N_FEATURES = SEGMENTS + 6
+N_TARGETS = SEGMENTS + 1
+
+BEAM_RANGES = {
+    "current": (2000.0, 4000.0),       # A
+    "spread": (0.5e-4, 2.0e-4),        # relative rms energy spread
+    "emit_um": (0.3, 0.6),             # normalised emittance
+    "beta": (10.0, 30.0),              # m
+    "energy_mev": (950.0, 1050.0),
+    "log_seed_w": (4.0, 6.0),          # log10 seed power [W]
+}
+BEAM_KEYS = list(BEAM_RANGES)
+
+
+def random_beam(rng) -> dict:
+    return {k: float(rng.uniform(*BEAM_RANGES[k])) for k in BEAM_KEYS}
+
+
+def random_taper(rng) -> np.ndarray:
+    """K of the 32 segments for a in [0, 2e-4], z0 in [5, 30] m, jitter 1e-4."""
+    a = rng.uniform(0.0, 2e-4)
+    z0 = rng.uniform(5.0, 30.0)
+    z = np.arange(SEGMENTS) * SEG_LEN
+    return K0 * (1.0 - a * np.maximum(0.0, z - z0) ** 2) + rng.normal(0.0, 1e-4, SEGMENTS)
+
+
+def random_tapers(rng, n: int) -> np.ndarray:
+    """n tapers at once, [n, 32] (same distribution as random_taper)."""
+    a = rng.uniform(0.0, 2e-4, (n, 1))
+    z0 = rng.uniform(5.0, 30.0, (n, 1))
+    z = np.arange(SEGMENTS)[None, :] * SEG_LEN
+    return K0 * (1.0 - a * np.maximum(0.0, z - z0) ** 2) + rng.normal(0.0, 1e-4, (n, SEGMENTS))
+
+
+def features(beam: dict, k: np.ndarray) -> np.ndarray:
+    return np.concatenate([np.asarray(k) / K0 - 1.0, [beam[key] for key in BEAM_KEYS]]).astype(np.float32)
+
+
+def _input(beam: dict, k: np.ndarray, path: str) -> str:
+    from felis_b200 import workloads
+
+    return workloads.write_input(
+        path, kind="static", beamlets=1024, per_beamlet=4, nx=65, total_length=(STEPS + 0.5) * LAMBDA_U_CM / 100.0,
+        energy_mev=beam["energy_mev"], spread_pct=beam["spread"] * 100.0, emit_um=beam["emit_um"],
+        beta=beam["beta"], current=beam["current"], K0=K0, lambda_u_cm=LAMBDA_U_CM, units=SEGMENTS,
+        unit_len=SEG_LEN, und_len=SEG_LEN, seed_power=10.0 ** beam["log_seed_w"], in_air=False, k_list=k)
+
+
+def _targets(energy: np.ndarray, bfac: np.ndarray) -> np.ndarray:
+    """energy[it, 2] (Ux, Uy sums), bfac[it, 2] -> the 33 targets."""
+    p = energy[:, 0] + energy[:, 1]
+    seg = p[np.arange(1, SEGMENTS + 1) * PERIODS]
+    return np.concatenate([np.log10(np.maximum(seg, 1e-300)), [np.hypot(bfac[-1, 0], bfac[-1, 1])]])
+
+
+def simulate(cases: list, chunk: int = 4096, workdir: str | None = None) -> np.ndarray:
+    """Full simulations of (beam, taper) cases on the batched mixed-precision
+    engine, `chunk` instances per ensemble; returns targets [n, 33]."""
+    import felis_b200 as fb
+
+    d = workdir or tempfile.mkdtemp(prefix="felis_taper_")
+    out = np.zeros((len(cases), N_TARGETS))
+    for c0 in range(0, len(cases), chunk):
+        part = cases[c0:c0 + chunk]
+        cfgs = [fb.Config(_input(b, k, os.path.join(d, f"c{c0 + i}.inp"))) for i, (b, k) in enumerate(part)]
+        ens = fb.Batch([c.params for c in cfgs])
+        for i, c in enumerate(cfgs):
+            beam = c.load_beam(0, seed=1)
+            ux, uy = c.load_seed(0)
+            ens.upload_particles(i, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
+                                 beam["offsets"], beam["weights"])
+            ens.upload_field(i, 0, 0, ux)
+            ens.upload_field(i, 0, 1, uy)
+        ens.run(0, STEPS)
+        for i in range(len(part)):
+            e, _, bf = ens.diagnostics(i, 0, STEPS + 1)
+            out[c0 + i] = _targets(e, bf)
+        ens.close()
+        for c in cfgs:
+            c.close()
+    return out
+
+
+def simulate_plain(beam: dict, k: np.ndarray, workdir: str | None = None) -> np.ndarray:
+    """The plain FP64 method (felis_create / felis_run) on one case."""
+    import felis_b200 as fb
+
+    d = workdir or tempfile.mkdtemp(prefix="felis_taper_")
+    c = fb.Config(_input(beam, k, os.path.join(d, "plain.inp")))
+    h = fb.Handle(c.params)
+    b = c.load_beam(0, seed=1)
+    ux, uy = c.load_seed(0)
+    h.upload_particles(0, b["x"], b["y"], b["px"], b["py"], b["theta"], b["gamma"], b["offsets"], b["weights"])
+    h.upload_field(0, 0, ux)
+    h.upload_field(0, 1, uy)
+    h.run(0, STEPS)
+    e, _, bf = h.diagnostics(0, STEPS + 1)
+    h.close()
+    c.close()
+    return _targets(e, bf)
+
+
+class Surrogate:
+    """The network with its input / output normalisation."""
+
+    def __init__(self, width: int = 256, seed: int = 1):
+        import felis_b200 as fb
+
+        self.net = fb.MLP(N_FEATURES, width, N_TARGETS, seed=seed)
+        self.xm = self.xs = self.ym = self.ys = None
+
+    def fit(self, X: np.ndarray, Y: np.ndarray, epochs: int = 200, batch: int = 512, lr: float = 1e-3,
+            weight_decay: float = 1e-4, seed: int = 1) -> np.ndarray:
+        self.xm, self.xs = X.mean(0), X.std(0) + 1e-12
+        self.ym, self.ys = Y.mean(0), Y.std(0) + 1e-12
+        self.net.set_data((X - self.xm) / self.xs, (Y - self.ym) / self.ys)
+        return self.net.train(epochs, batch=batch, lr=lr, weight_decay=weight_decay, seed=seed)
+
+    def predict(self, X: np.ndarray) -> np.ndarray:
+        y = self.net.forward((np.asarray(X) - self.xm) / self.xs)
+        return y * self.ys + self.ym
+
+    def close(self):
+        self.net.close()
+
+
+def dataset(n: int, seed: int = 1, chunk: int = 4096) -> tuple[np.ndarray, np.ndarray, list]:
+    rng = np.random.default_rng(seed)
+    cases = [(random_beam(rng), random_taper(rng)) for _ in range(n)]
+    X = np.stack([features(b, k) for b, k in cases])
+    Y = simulate(cases, chunk=chunk)
+    return X, Y, cases
+
+
+def propose(model: Surrogate, beam: dict, n_candidates: int, top: int, seed: int = 7):
+    """Rank n_candidates random tapers for `beam` by predicted final power;
+    returns the `top` tapers and their predicted targets."""
+    rng = np.random.default_rng(seed)
+    ks = random_tapers(rng, n_candidates)
+    X = np.concatenate([ks / K0 - 1.0, np.tile([beam[k] for k in BEAM_KEYS], (n_candidates, 1))], axis=1)
+    pred = model.predict(X.astype(np.float32))
+    order = np.argsort(-pred[:, SEGMENTS - 1])[:top]
+    return ks[order], pred[order]
+
+
+def search(model: Surrogate, beam: dict, n_candidates: int = 1_000_000, top: int = 64, tol: float = 0.05,
+           fallback_runs: int = 64, seed: int = 7) -> dict:
+    """Surrogate-guided taper search for one beam.  The proposed winners are
+    re-run by the plain FP64 method; where the surrogate's error on the final
+    power exceeds `tol`, a plain random scan of `fallback_runs` tapers takes
+    over.  Returns the best verified taper and the bookkeeping."""
+    t0 = time.perf_counter()
+    ks, pred = propose(model, beam, n_candidates, top, seed)
+    t_rank = time.perf_counter() - t0
+    verified = np.stack([simulate_plain(beam, k) for k in ks])
+    p_pred = 10.0 ** pred[:, SEGMENTS - 1]
+    p_true = 10.0 ** verified[:, SEGMENTS - 1]
+    err = np.abs(p_pred - p_true) / p_true
+    best = int(np.argmax(p_true))
+    res = {"best_power": float(p_true[best]), "best_taper": ks[best], "runs": top, "rank_seconds": t_rank,
+           "surrogate_error_max": float(err.max()), "surrogate_error_best": float(err[best]), "fallback": False}
+    if err[best] > tol:
+        rng = np.random.default_rng(seed + 1)
+        scan = list(random_tapers(rng, fallback_runs))
+        ps = np.array([10.0 ** simulate_plain(beam, k)[SEGMENTS - 1] for k in scan])
+        res["fallback"] = True
+        res["runs"] += fallback_runs
+        if ps.max() > res["best_power"]:
+            res["best_power"] = float(ps.max())
+            res["best_taper"] = scan[int(np.argmax(ps))]
+    return res
+
+
+def compare_with_scan(model: Surrogate, beam: dict, n_candidates: int, top: int, scan_runs: int,
+                      seed: int = 7) -> dict:
+    """What the network gains over the method without it, for one beam, in
+    full simulations of one simulator (the batched engine): the best final
+    power of the network's `top` proposals against the running best of a
+    plain random scan of `scan_runs` tapers, and how many scan runs it takes
+    to reach the network's best (None: not within the scan)."""
+    ks, pred = propose(model, beam, n_candidates, top, seed)
+    rng = np.random.default_rng(seed + 2)
+    scan = random_tapers(rng, scan_runs)
+    Y = simulate([(beam, k) for k in list(ks) + list(scan)])
+    p_sur = 10.0 ** Y[:top, SEGMENTS - 1]
+    p_scan = 10.0 ** Y[top:, SEGMENTS - 1]
+    running = np.maximum.accumulate(p_scan)
+    best = float(p_sur.max())
+    reach = np.flatnonzero(running >= best)
+    pred_best = 10.0 ** pred[int(np.argmax(p_sur)), SEGMENTS - 1]
+    return {"surrogate_best": best, "surrogate_runs": top, "scan_best": float(p_scan.max()),
+            "scan_best_at_equal_runs": float(running[min(top, scan_runs) - 1]),
+            "scan_runs_to_reach": int(reach[0]) + 1 if reach.size else None, "scan_runs": scan_runs,
+            "surrogate_error_at_best": float(abs(pred_best - best) / best)}

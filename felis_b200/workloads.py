@@ -42,13 +42,14 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
                unit_len: float = 4.0, und_len: float = 3.4, seed_power: float = 1e6, seed_sigma_um: float = 30.0,
                noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
                linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
-               in_air: bool = True) -> str:
+               in_air: bool = True, k_list=None) -> str:
     static = kind == "static"
     if noise is None:
         noise = not static
     photon = resonant_photon_energy(energy_mev, lambda_u_cm, K0)
     lam0_um = PLANCK_H * C_LIGHT / photon * 1e6
     minZ, maxZ = 0.0, (slices + 0.5) * lam0_um
+    k_line = "" if k_list is None else " K0_list=" + ",".join(repr(float(k)) for k in k_list) + "\n"
     harm = "\n".join(f" harmony{i} = {h}" for i, h in enumerate(harmonics))
     zspan = 1.0e-3
     quad_block = ""
@@ -117,7 +118,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  undulator_start=0.0
  undulator_end={und_len}
  K0={K0}
-
+{k_line}
 [Wake_field]
  activate={'ON' if wake else 'OFF'}
  shape=Circular
