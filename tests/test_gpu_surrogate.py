@@ -21,7 +21,7 @@ def trained():
 
     X, Y, _ = sg.dataset(TRAIN_RUNS, seed=21)
     model = sg.Surrogate(seed=2)
-    hist = model.fit(X, Y, epochs=150, batch=256, lr=1e-3)
+    hist = model.fit(X, Y, schedule=((100, 1.0), (50, 0.3)), batch=256, lr=1e-3)
     yield sg, model, hist
     model.close()
 
