@@ -94,7 +94,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload(name: str, rank: int = 0, slices: int | None = None):
+def make_workload(name: str, rank: int = 0, slices: int | None = None, grid: int | None = None):
     import felis_b200 as fb
     from felis_b200 import workloads
 
@@ -102,6 +102,8 @@ def make_workload(name: str, rank: int = 0, slices: int | None = None):
     kw = dict(workloads.WORKLOADS[name])
     if slices and name == "sase":
         kw["slices"] = slices
+    if grid:
+        kw["nx"] = grid
     path = workloads.write_input(os.path.join(d, f"{name}.inp"), **kw)
     cfg = fb.Config(path)
     beam = cfg.load_beam(0, seed=2 if name == "sase" else 1)
@@ -197,7 +199,7 @@ def run_felis(args, dist, rank, world):
 
     import felis_b200 as fb
 
-    cfg, beam, fields = make_workload(args.workload, rank, args.slices)
+    cfg, beam, fields = make_workload(args.workload, rank, args.slices, args.grid)
     p = cfg.params
     P = int(beam["offsets"][-1])
     cells = p.slice_n * p.nx * p.ny * 2 * p.num_harmony
@@ -555,6 +557,7 @@ def main():
     ap.add_argument("--e2e-steps", type=int, default=100)
     ap.add_argument("--no-cpu-baseline", action="store_true")
     ap.add_argument("--slices", type=int, default=None, help="smaller sase bunch (profiling captures)")
+    ap.add_argument("--grid", type=int, default=None, help="grid key nx = ny of the workload (profiling captures)")
     ap.add_argument("--ensemble", type=int, default=96, help="instances of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
@@ -581,7 +584,7 @@ def main():
     dist, rank, world = dist_init()
     line = run_felis(args, dist, rank, world)
     if not args.fp64_only:
-        cfg, beam, fields = make_workload(args.workload, rank, args.slices)
+        cfg, beam, fields = make_workload(args.workload, rank, args.slices, args.grid)
         fp64 = dict(line)
         e64 = fp64.pop("_energy")
         mixed = run_mixed(args, cfg, beam, fields, dist, world, e64)
