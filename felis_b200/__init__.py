@@ -106,6 +106,10 @@ for _n in ("felis_solve_field", "felis_transverse_push", "felis_push_theta_gamma
            "felis_periodic_particles", "felis_shift_field", "felis_step"):
     _sig(_n, C.c_int, _vp, C.c_int32)
 _sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_set_slice_exchange", C.c_int, _vp, C.c_int32)
+_sig("felis_get_first_planes", C.c_int, _vp, _dp)
+_sig("felis_set_first_planes", C.c_int, _vp, _dp)
+_sig("felis_diagnostic_sums", C.c_int, _vp, C.c_int32, _dp)
 _sig("felis_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, _dp, _dp, _dp)
 _sig("felis_edge_deposit_count", C.c_int, _vp, _i64p)
 _sig("felis_sort_by_slice", C.c_int, _i32p, C.c_int64, _i64p)
@@ -375,6 +379,24 @@ class Handle:
         b = np.zeros(n * 2 * self.H)
         self._ck(_lib.felis_get_diagnostics(self._h, it0, it1, _p(e), _p(t), _p(b)))
         return e.reshape(n, 2 * self.H), t.reshape(n, 6 * self.species), b.reshape(n, 2 * self.H)
+
+    def set_slice_exchange(self, enable: bool):
+        self._ck(_lib.felis_set_slice_exchange(self._h, 1 if enable else 0))
+
+    def first_planes(self) -> np.ndarray:
+        """[H][2][ny][nx] complex planes of the block's first slice."""
+        buf = np.zeros(2 * self.H * 2 * self.nx * self.ny)
+        self._ck(_lib.felis_get_first_planes(self._h, _p(buf)))
+        return (buf[0::2] + 1j * buf[1::2]).reshape(self.H, 2, self.ny, self.nx)
+
+    def set_first_planes(self, planes: np.ndarray):
+        buf = _cplx_to_interleaved(planes)
+        self._ck(_lib.felis_set_first_planes(self._h, _p(buf)))
+
+    def diagnostic_sums(self, it: int = 0) -> np.ndarray:
+        out = np.zeros(7 * self.species + 2 * self.H + 1)
+        self._ck(_lib.felis_diagnostic_sums(self._h, it, _p(out)))
+        return out
 
     def edge_deposit_count(self) -> int:
         c = C.c_int64(0)

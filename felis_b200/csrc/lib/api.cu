@@ -117,6 +117,9 @@ struct felis_handle {
   bool diag_valid = false;        // hist row for the next iteration already written
   int diag_iter = -1;
   bool capturing = false;
+  // slice sharding across processes: the shift leaves the plane that becomes
+  // the first slice holding the old last slice, for the caller to exchange
+  bool exchange = false;
 };
 
 namespace {
@@ -492,6 +495,7 @@ felis_status do_shift(felis_handle* h) {
   const int S = h->p.slice_n;
   h->ring_base = ((h->ring_base - 1) % S + S) % S;
   const size_t N = (size_t)h->p.nx * h->p.ny;
+  if (h->exchange) return FELIS_OK;  // fieldShareZ.cpp:39-78 fills it
   KernelScope ks(h, FELIS_KERNEL_SHIFT);
   for (int hh = 0; hh < h->p.num_harmony; ++hh)
     for (int pol = 0; pol < 2; ++pol)
@@ -1219,6 +1223,64 @@ felis_status felis_kernel_stats(felis_handle* h, int32_t kind, int64_t* launches
   }
   if (launches) *launches = n;
   if (total_ms) *total_ms = ms;
+  return FELIS_OK;
+}
+
+felis_status felis_set_slice_exchange(felis_handle* h, int32_t enable) {
+  if (!h) return FELIS_BAD_ARG;
+  h->exchange = enable != 0;
+  h->diag_valid = false;
+  return FELIS_OK;
+}
+
+// The first slice's planes of every harmonic and polarisation, [H][2][ny*nx]
+// interleaved complex: after a shift in exchange mode, the slice that leaves
+// this process's block (the packed slot of fieldShareZ.cpp:39-78).
+felis_status felis_get_first_planes(felis_handle* h, double* out) {
+  if (!h || !out) return FELIS_BAD_ARG;
+  const int S = h->p.slice_n, H = h->p.num_harmony;
+  const size_t N = (size_t)h->p.nx * h->p.ny;
+  CK(cudaStreamSynchronize(h->st));
+  for (int hh = 0; hh < H; ++hh)
+    for (int pol = 0; pol < 2; ++pol)
+      CK(cudaMemcpy(out + 2 * ((size_t)(hh * 2 + pol) * N), h->U + field_plane(S, hh, pol, 0, h->ring_base) * N,
+                    N * sizeof(double2), cudaMemcpyDeviceToHost));
+  return FELIS_OK;
+}
+
+// Sets the first slice's planes (the slice received from the previous
+// process; zeros on the first process).
+felis_status felis_set_first_planes(felis_handle* h, const double* in) {
+  if (!h || !in) return FELIS_BAD_ARG;
+  const int S = h->p.slice_n, H = h->p.num_harmony;
+  const size_t N = (size_t)h->p.nx * h->p.ny;
+  CK(cudaStreamSynchronize(h->st));
+  for (int hh = 0; hh < H; ++hh)
+    for (int pol = 0; pol < 2; ++pol)
+      CK(cudaMemcpy(h->U + field_plane(S, hh, pol, 0, h->ring_base) * N, in + 2 * ((size_t)(hh * 2 + pol) * N),
+                    N * sizeof(double2), cudaMemcpyHostToDevice));
+  h->diag_valid = false;
+  return FELIS_OK;
+}
+
+// Unfinished diagnostic sums of the current state, for reductions across
+// processes (twiss.cpp:46-64, saveFile.cpp:126-137): per species sum x^2,
+// y^2, x'^2, y'^2, x x', y y', count; then per harmonic sum w cos(H theta),
+// sum w sin(H theta); then sum w.
+felis_status felis_diagnostic_sums(felis_handle* h, int32_t it, double* out) {
+  if (!h || !out) return FELIS_BAD_ARG;
+  (void)it;
+  felis_status s = diag_now(h, h->d_tmp, h->d_tmp + 6 * FELIS_MAX_SPECIES);
+  if (s != FELIS_OK) return s;
+  const int nq = 7 * h->p.num_species + 2 * h->p.num_harmony + 1;
+  std::vector<double> l1((size_t)h->l1_blocks * nq);
+  CK(cudaMemcpyAsync(l1.data(), h->d_l1, l1.size() * sizeof(double), cudaMemcpyDeviceToHost, h->st));
+  CK(cudaStreamSynchronize(h->st));
+  for (int k = 0; k < nq; ++k) {
+    double t = 0.0;
+    for (int b = 0; b < h->l1_blocks; ++b) t += l1[(size_t)b * nq + k];
+    out[k] = t;
+  }
   return FELIS_OK;
 }
 

@@ -234,6 +234,24 @@ felis_status felis_kernel_stats(felis_handle* h, int32_t kind, int64_t* launches
 /* Device time of the last felis_run graph launch (CUDA events around it). */
 felis_status felis_last_run_ms(felis_handle* h, double* ms);
 
+/* ---- slices sharded across processes (boundary.cpp:33-46, fieldShareZ.cpp:39-78)
+ * A process holds slices [min_i, min_i + slice_n) of global_slice_n.  In
+ * exchange mode the slippage shift leaves the plane that becomes this
+ * block's first slice holding the block's old last slice; the caller sends
+ * those planes to the next process (felis_get_first_planes) and writes the
+ * planes received from the previous one in their place
+ * (felis_set_first_planes; zeros on the first process), as MPI_Transfer1F_Zplus
+ * does.  Call it between iterations (felis_step, or the per-function loop). */
+felis_status felis_set_slice_exchange(felis_handle* h, int32_t enable);
+/* [H][2][ny*nx] interleaved complex, host buffers. */
+felis_status felis_get_first_planes(felis_handle* h, double* out);
+felis_status felis_set_first_planes(felis_handle* h, const double* in);
+/* Unfinished sums of the current state for reductions across processes
+ * (twiss.cpp:46-64 per species: sum x^2, y^2, x'^2, y'^2, x x', y y', count;
+ * then saveFile.cpp:126-137 per harmonic: sum w cos(H theta), sum w
+ * sin(H theta); then sum w): 7 * num_species + 2 * num_harmony + 1 values. */
+felis_status felis_diagnostic_sums(felis_handle* h, int32_t it, double* out);
+
 /* ---- slice sort (the slice binning of restoreParticleHDF.cpp:166-214 and
  * the slice-major write order of saveParticleHDF.cpp:95-109) -------------
  * Stable sort of n particles by integer slice key on the GPU: perm[k] is the

@@ -937,6 +937,41 @@ static void bfactor(orc* D, double* out) {
   }
 }
 
+// The unfinished sums behind twiss() and bfactor(), for reductions across
+// processes (twiss.cpp:46-64 before MPI_Allreduce; saveFile.cpp:126-137):
+// per species sum x^2, y^2, x'^2, y'^2, x x', y y', count; per harmonic
+// sum w cos(H theta), sum w sin(H theta); sum w.
+static void diagnostic_sums(orc* D, double* out) {
+  int k = 0;
+  for (int s = 0; s < D->nSpecies; ++s) {
+    Species& P = D->sp[s];
+    double a[7] = {0, 0, 0, 0, 0, 0, 0};
+    const int64_t n1 = P.off[D->subSliceN];
+    for (int64_t n = 0; n < n1; ++n) {
+      const double x = P.x[n], y = P.y[n], invGam = 1.0 / P.gamma[n];
+      const double xPrime = P.px[n] * invGam, yPrime = P.py[n] * invGam;
+      a[0] += x * x; a[1] += y * y; a[2] += xPrime * xPrime; a[3] += yPrime * yPrime;
+      a[4] += x * xPrime; a[5] += y * yPrime; a[6] += 1.0;
+    }
+    for (int j = 0; j < 7; ++j) out[k++] = a[j];
+  }
+  double totalN = 0.0;
+  for (int h = 0; h < D->numHarmony; ++h) {
+    cd b = C(0, 0);
+    for (int sl = 0; sl < D->subSliceN; ++sl)
+      for (int s = 0; s < D->nSpecies; ++s) {
+        Species& P = D->sp[s];
+        for (int64_t n = P.off[sl]; n < P.off[sl + 1]; ++n) {
+          b = cadd(b, cscale(cexpi(D->harmony[h] * P.theta[n]), P.weight[sl]));
+          if (h == 0) totalN += P.weight[sl];
+        }
+      }
+    out[k++] = b.re;
+    out[k++] = b.im;
+  }
+  out[k] = totalN;
+}
+
 extern "C" {
 
 orc* orc_create(const felis_params* p, int threads) {
@@ -1094,6 +1129,7 @@ int orc_shift_field(orc* D) { ORC_CALL(shift_field(D)); }
 void orc_total_energy(orc* D, double* out) { total_energy(D, out); }
 void orc_twiss(orc* D, double* out) { twiss(D, out); }
 void orc_bfactor(orc* D, double* out) { bfactor(D, out); }
+void orc_diagnostic_sums(orc* D, double* out) { diagnostic_sums(D, out); }
 
 // main.cpp:117-155 for iterations [it0, it1).  Diagnostics per iteration are
 // written when the pointers are non-null (2H energy, 6*species twiss, 2H bfactor).

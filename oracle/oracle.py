@@ -64,6 +64,7 @@ def load(variant: str = "strict", out_dir: str | None = None) -> C.CDLL:
         "orc_total_energy": (None, [vp, _dp]),
         "orc_twiss": (None, [vp, _dp]),
         "orc_bfactor": (None, [vp, _dp]),
+        "orc_diagnostic_sums": (None, [vp, _dp]),
         "orc_run": (C.c_int, [vp, C.c_int, C.c_int, _dp, _dp, _dp]),
         "orc_build_flags": (C.c_int, []),
     }
@@ -188,6 +189,11 @@ class Oracle:
     def bfactor(self) -> np.ndarray:
         out = np.zeros(2 * self.H)
         self.lib.orc_bfactor(self.h, _p(out))
+        return out
+
+    def diagnostic_sums(self) -> np.ndarray:
+        out = np.zeros(7 * self.species + 2 * self.H + 1)
+        self.lib.orc_diagnostic_sums(self.h, _p(out))
         return out
 
     def run(self, it0: int, it1: int, diagnostics: bool = True):
