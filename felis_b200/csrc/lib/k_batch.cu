@@ -149,8 +149,9 @@ __global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
     bi0 = b.x; bi1 = b.y; bj0 = b.z; bj1 = b.w;
     bw = bi1 - bi0 + 1;
     const int cells = (bw > 0 && bj1 >= bj0) ? bw * (bj1 - bj0 + 1) : 0;
+    // the deposit packs the slice's source planes back to back, `cells` each
     const int p = I.src_plane[h] + ((I.harmony[h] & 1) ? 0 : pol);
-    const float2* g = I.src + ((size_t)s * I.nsrc + p) * N;
+    const float2* g = I.src + (size_t)s * I.nsrc * N + (size_t)p * cells;
     const size_t used = ((size_t)ny * nxp + 6 * (size_t)Mx) * sizeof(float2);
     if (cells > 0 && used + (size_t)cells * sizeof(float2) <= (size_t)a.smem_bytes) {
       for (int k = tid; k < cells; k += nt) cp_async8(ssrc + k, g + k);

@@ -20,6 +20,7 @@ laser_alpha = -1 it would land in Uy and never interact.
 """
 from __future__ import annotations
 
+import math
 import os
 import tempfile
 
@@ -42,7 +43,15 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
                unit_len: float = 4.0, und_len: float = 3.4, seed_power: float = 1e6, seed_sigma_um: float = 30.0,
                noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
                linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
-               in_air: bool = True, k_list=None) -> str:
+               in_air: bool = True, k_list=None, sigma_slices: float | None = None, profile_nodes: int = 65,
+               K_und: float | None = None) -> str:
+    """Input text of one workload.  `sigma_slices` switches the flat-top
+    current to a Gaussian of that rms length (in slices) centred on the bunch,
+    written as a `profile_nodes`-node Polygon so that the energy-spread nodes
+    still apply (loadBeam.cpp's Gaussian load type has no spread).  `K0` sets
+    the photon energy by the planar resonance; `K_und` (default K0) is the
+    undulator's K, e.g. K0 / sqrt(1 + polarity^2) for an elliptical undulator
+    on the same resonance (parameterSetting.cpp's default K0)."""
     static = kind == "static"
     if noise is None:
         noise = not static
@@ -52,6 +61,16 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
     k_line = "" if k_list is None else " K0_list=" + ",".join(repr(float(k)) for k in k_list) + "\n"
     harm = "\n".join(f" harmony{i} = {h}" for i, h in enumerate(harmonics))
     zspan = 1.0e-3
+    if sigma_slices is None:
+        z_nodes = f" z_nodes=2\n z0={-zspan}\n z1={zspan}\n z_n0=1\n z_n1=1"
+    else:
+        lam0 = lam0_um * 1e-6
+        centre, sig = 0.5 * slices * lam0, sigma_slices * lam0
+        zs = [(-1.0 + (slices + 2.0) * k / (profile_nodes - 1)) * lam0 for k in range(profile_nodes)]
+        lines = [f" z_nodes={profile_nodes}"]
+        lines += [f" z{k}={z!r}" for k, z in enumerate(zs)]
+        lines += [f" z_n{k}={math.exp(-0.5 * ((z - centre) / sig) ** 2)!r}" for k, z in enumerate(zs)]
+        z_nodes = "\n".join(lines)
     quad_block = ""
     if quads:
         quad_block = """
@@ -117,7 +136,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  unit_end={unit_len}
  undulator_start=0.0
  undulator_end={und_len}
- K0={K0}
+ K0={K0 if K_und is None else K_und}
 {k_line}
 [Wake_field]
  activate={'ON' if wake else 'OFF'}
@@ -141,11 +160,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  alpha_y=0
  beamlets_in_bucket={beamlets}
  number_in_beamlet={per_beamlet}
- z_nodes=2
- z0={-zspan}
- z1={zspan}
- z_n0=1
- z_n1=1
+{z_nodes}
  energy_nodes=2
  energy_z0={-zspan}
  energy_z1={zspan}
@@ -176,7 +191,15 @@ def write_input(path: str | None = None, kind: str = "sase", **kw) -> str:
 
 WORKLOADS = {
     "static": dict(kind="static"),
-    "sase": dict(kind="sase"),
+    "sase": dict(kind="sase", seed_power=0.0),
+    # mixed-precision long run: QuadPolar (polarity 0.5), harmonics 1 and 3,
+    # Gaussian current (rms 600 slices, peak 4 kA, 16384 particles per slice
+    # at the peak), copper AC wake in a 5 mm pipe, 151 x 151 grid, 60 m with
+    # a linear taper to K = 0.99 K0 in the last of 15 units
+    "gaussian_taper": dict(kind="sase", slices=4096, sigma_slices=600.0, current=4000.0, beamlets=4096,
+                           per_beamlet=4, nx=151, harmonics=(1, 3), undulator="QuadPolar", polarity=0.5,
+                           wake=True, units=15, total_length=60.0, seed_power=0.0,
+                           K_und=2.6 / math.sqrt(1.25), linear_taper=-0.01 * 2.6 / math.sqrt(1.25) * math.sqrt(2.0) / 14.0),
 }
 
 

@@ -96,6 +96,31 @@ def test_mixed_vs_fp64_figures_of_merit(fb, seeded):
                                rtol=BUNCHING_RTOL)
 
 
+def test_mixed_vs_fp64_every_harmonic_and_polarisation(fb, tmp_path):
+    """An elliptical undulator (QuadPolar, polarity 0.5) with harmonics 1, 2
+    and 3: each harmonic and polarisation has its own source plane (odd
+    harmonics one shared plane, even harmonics one per polarisation), and the
+    power of every one of the 2 H planes follows FP64."""
+    import math
+
+    cfg, beam, fields = make_case(fb, tmp_path, kind="sase", **dict(
+        SEEDED, slices=96, harmonics=(1, 2, 3), undulator="QuadPolar", polarity=0.5, K_und=2.6 / math.sqrt(1.25)))
+    p = cfg.params
+    steps = p.max_step
+    g = _fp64(fb, cfg, beam, fields, steps)
+    b = fb.Batch([p])
+    _upload(fb, b, 0, cfg, beam, fields)
+    b.run(0, steps)
+    e64, _, _ = g.diagnostics(0, steps + 1)
+    e32, _, _ = b.diagnostics(0, 0, steps + 1)
+    for col in range(2 * p.num_harmony):
+        P64, P32 = e64[:, col], e32[:, col]
+        assert P64[-1] > 0 and P32[-1] > 0, f"plane {col}: no field"
+        sel = P64 > 1e-6 * P64.max()
+        rel = np.abs(P32[sel] - P64[sel]) / P64[sel]
+        assert rel.max() < POWER_RTOL, f"plane {col} (harmonic {p.harmony[col // 2]}, pol {col % 2}): {rel.max():.3e}"
+
+
 def test_initial_diagnostics_match_fp64(fb, seeded):
     cfg, beam, fields = seeded
     g = _fp64(fb, cfg, beam, fields, 1)
