@@ -13,6 +13,7 @@
 #include <string.h>
 
 #include <algorithm>
+#include <complex>
 #include <map>
 #include <string>
 #include <tuple>
@@ -56,6 +57,7 @@ struct Inst {
   int4* sbox = nullptr;
   int nsrc = 0;
   int src_plane[FELIS_MAX_HARMONY] = {0};
+  int cx[5] = {0}, cy[5] = {0};  // ADI chunks of the interior columns / rows
   double* part_e = nullptr;
   double* part_b = nullptr;
   int* err = nullptr;
@@ -186,38 +188,79 @@ void transverse_maps(const Inst& I, const felis_lattice& l0, const felis_lattice
 // solveField.cpp:138-180 rewritten with reciprocals): per direction p = 1/aP
 // (last row 1), m = a/(aP CC[i-1]) (first row 0, last row 1/CC[i-1]),
 // r = 1/CC, and the right-hand-side coefficients.
-void adi_tables(const felis_params& p, int hidx, int M, std::vector<float2>& out) {
-  typedef double2 d2;
-  auto C2 = [](double r, double i) { return make_double2(r, i); };
-  auto mul = [&](d2 a, d2 b) { return C2(a.x * b.x - a.y * b.y, a.x * b.y + a.y * b.x); };
-  auto inv = [&](d2 b) { const double n = b.x * b.x + b.y * b.y; return C2(b.x / n, -b.y / n); };
-  auto sub = [&](d2 a, d2 b) { return C2(a.x - b.x, a.y - b.y); };
-  auto add = [&](d2 a, d2 b) { return C2(a.x + b.x, a.y + b.y); };
+// Four chunks of an interior line of m points, for the partitioned
+// recurrences of the ADI: starts with residues 0, 4, 8, 12 (mod 16) in some
+// order, so that the lanes of a quad walking the four chunks of one line, four
+// lines per half-warp, hit 16 distinct 8-byte shared-memory words when the
+// row pitch is odd; among those, the split with the shortest longest chunk.
+void adi_chunks(int m, int out[5]) {
+  static const int perm[6][3] = {{4, 8, 12}, {4, 12, 8}, {8, 4, 12}, {8, 12, 4}, {12, 4, 8}, {12, 8, 4}};
+  int best = 1 << 30;
+  out[0] = 0; out[4] = m;
+  for (int q = 1; q < 4; ++q) out[q] = q * m / 4;
+  for (const auto& rs : perm) {
+    int cand[3][2];
+    for (int q = 0; q < 3; ++q) {
+      const int ideal = (q + 1) * m / 4, r = rs[q];
+      const int lo = ideal - (((ideal - r) % 16) + 16) % 16;
+      cand[q][0] = lo;
+      cand[q][1] = lo + 16;
+    }
+    for (int a = 0; a < 8; ++a) {
+      const int s1 = cand[0][a & 1], s2 = cand[1][(a >> 1) & 1], s3 = cand[2][(a >> 2) & 1];
+      if (!(0 < s1 && s1 < s2 && s2 < s3 && s3 < m)) continue;
+      const int len = std::max(std::max(s1, s2 - s1), std::max(s3 - s2, m - s3));
+      if (len < best) { best = len; out[1] = s1; out[2] = s2; out[3] = s3; }
+    }
+  }
+}
+
+// Complex tables of the ADI of harmonic hidx (solveField.cpp:80-185), indexed
+// by interior point c = i - 1, 16 tables of M entries:
+//   0-4   x sweep: 1/alphaP (last: 1), alpha/(alphaP CC[i-1]) (first 0, last
+//         1/CC[n-3]), 1/CC, and the chunk products
+//         G_c = prod_{k = chunk start}^{c} (-m_k),  Q_c = prod_{k = c}^{chunk end} (-1/CC_k)
+//         of the forward and backward recurrences (chunks cx)
+//   5-9   the same for the y sweep (chunks cy)
+//   10-12 right-hand side of the x sweep by row: -betaP, H+betaP+beta, beta
+//   13-15 right-hand side of the y sweep by column: -alphaP, H+alphaP+alpha, alpha
+void adi_tables(const felis_params& p, int hidx, int M, const int cx[5], const int cy[5], std::vector<float2>& out) {
+  typedef std::complex<double> cd;
   const double H = p.harmony[hidx];
-  out.assign((size_t)12 * M, make_float2(0.f, 0.f));
-  auto put = [&](int t, int k, d2 v) { out[(size_t)t * M + k] = make_float2((float)v.x, (float)v.y); };
+  out.assign((size_t)16 * M, make_float2(0.f, 0.f));
+  auto put = [&](int t, int k, cd v) { out[(size_t)t * M + k] = make_float2((float)v.real(), (float)v.imag()); };
   for (int dir = 0; dir < 2; ++dir) {
-    const int n = dir == 0 ? p.nx : p.ny;
+    const int n = dir == 0 ? p.nx : p.ny, m = n - 2;
+    const int* ch = dir == 0 ? cx : cy;
     const double* A = dir == 0 ? p.abc_alpha : p.abc_beta;
     const double* AP = dir == 0 ? p.abc_alpha_p : p.abc_beta_p;
-    std::vector<d2> al(n), ap(n), CC(n);
-    for (int i = 0; i < n; ++i) { al[i] = C2(A[2 * i], A[2 * i + 1]); ap[i] = C2(AP[2 * i], AP[2 * i + 1]); }
-    CC[1] = mul(sub(sub(C2(H, 0), ap[1]), al[1]), inv(ap[1]));
-    for (int i = 2; i < n - 2; ++i)
-      CC[i] = sub(mul(sub(sub(C2(H, 0), ap[i]), al[i]), inv(ap[i])), mul(al[i], inv(mul(ap[i], CC[i - 1]))));
-    CC[n - 2] = sub(sub(sub(C2(H, 0), ap[n - 2]), al[n - 2]), inv(CC[n - 3]));
-    const int tp = dir == 0 ? 0 : 3;
+    std::vector<cd> al(n), ap(n), CC(n), fw(m), rc(m);
+    for (int i = 0; i < n; ++i) { al[i] = cd(A[2 * i], A[2 * i + 1]); ap[i] = cd(AP[2 * i], AP[2 * i + 1]); }
+    CC[1] = (H - ap[1] - al[1]) / ap[1];
+    for (int i = 2; i < n - 2; ++i) CC[i] = (H - ap[i] - al[i]) / ap[i] - al[i] / (ap[i] * CC[i - 1]);
+    CC[n - 2] = H - ap[n - 2] - al[n - 2] - 1.0 / CC[n - 3];
+    const int tp = dir == 0 ? 0 : 5;
     for (int i = 1; i < n - 1; ++i) {
-      put(tp + 0, i, i < n - 2 ? inv(ap[i]) : C2(1, 0));
-      put(tp + 1, i, i == 1 ? C2(0, 0) : (i < n - 2 ? mul(al[i], inv(mul(ap[i], CC[i - 1]))) : inv(CC[n - 3])));
-      put(tp + 2, i, inv(CC[i]));
+      const int c = i - 1;
+      const cd a = i < n - 2 ? 1.0 / ap[i] : cd(1.0, 0.0);
+      fw[c] = i == 1 ? cd(0.0, 0.0) : (i < n - 2 ? al[i] / (ap[i] * CC[i - 1]) : 1.0 / CC[n - 3]);
+      rc[c] = 1.0 / CC[i];
+      put(tp + 0, c, a);
+      put(tp + 1, c, fw[c]);
+      put(tp + 2, c, rc[c]);
     }
-    // rhs of the other sweep uses this direction's coefficients
-    const int tr = dir == 0 ? 9 : 6;
+    for (int q = 0; q < 4; ++q) {
+      cd g(1.0, 0.0);
+      for (int c = ch[q]; c < ch[q + 1]; ++c) { g *= -fw[c]; put(tp + 3, c, g); }
+      g = cd(1.0, 0.0);
+      for (int c = ch[q + 1] - 1; c >= ch[q]; --c) { g *= -rc[c]; put(tp + 4, c, g); }
+    }
+    // right-hand side of the other sweep
+    const int tr = dir == 0 ? 13 : 10;
     for (int i = 1; i < n - 1; ++i) {
-      put(tr + 0, i, C2(-ap[i].x, -ap[i].y));
-      put(tr + 1, i, add(add(C2(H, 0), ap[i]), al[i]));
-      put(tr + 2, i, al[i]);
+      put(tr + 0, i - 1, -ap[i]);
+      put(tr + 1, i - 1, H + ap[i] + al[i]);
+      put(tr + 2, i - 1, al[i]);
     }
   }
 }
@@ -302,7 +345,9 @@ felis_status upload_inst_table(felis_batch* b) {
     BInst& D = h[k];
     const felis_params& p = I.p;
     D.S = p.slice_n; D.nx = p.nx; D.ny = p.ny; D.N = p.nx * p.ny; D.H = p.num_harmony; D.L = p.scl_mode;
-    D.F = p.scf_mode; D.nr = p.nr; D.nxp = p.nx | 1; D.bn = p.bessel_rows; D.bcols = p.bessel_cols;
+    D.F = p.scf_mode; D.nr = p.nr; D.bn = p.bessel_rows; D.bcols = p.bessel_cols;
+    D.pitch = (p.nx - 2) | 1;
+    for (int q = 0; q < 5; ++q) { D.cx[q] = I.cx[q]; D.cy[q] = I.cy[q]; }
     D.numSlice = p.num_slice; D.minI = p.min_i; D.wakeOn = p.wake_on;
     D.nsrc = I.nsrc;
     for (int i = 0; i < FELIS_MAX_HARMONY; ++i) {
@@ -485,16 +530,16 @@ felis_status prepare(felis_batch* b) {
   return FELIS_OK;
 }
 
-// Shared memory of both launches: the ADI holds its plane, 6 tables and as
+// Shared memory of both launches: the ADI holds its interior plane, 16 tables and as
 // much of the source box as fits beside adi_ctas CTAs per SM (more cells are
 // read from global memory); the push holds the accumulators of up to 6144 source
 // cells (larger boxes accumulate in the source buffer in global memory).
 felis_status ensure_launch(felis_batch* b) {
   b->adi_smem_max = 0;
   for (AdiClass& c : b->adi_classes) {
-    const int M32 = ((std::max(c.nx, c.ny) + 31) / 32) * 32;
-    if (M32 > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
-    c.threads = std::max(M32, 64);
+    if (std::max(c.nx, c.ny) > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
+    // four threads per interior row (x sweep) and per interior column (y sweep)
+    c.threads = ((4 * (std::max(c.nx, c.ny) - 2) + 31) / 32) * 32;
     // 1 KB of every CTA's share stays for static shared memory
     const size_t cap = (size_t)b->dev_smem - 1024;
     const size_t base = batch_adi_smem(c.nx, c.ny, 0);
@@ -598,7 +643,7 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
   for (int k = 0; k < n; ++k) {
     const felis_params* p = instances[k];
     if (!p || p->abi_version != FELIS_ABI_VERSION || p->dimension != 3 || p->num_species != 1 || p->slice_n < 1 ||
-        p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY || p->nx < 4 || p->ny < 4 || p->scl_mode < 1 ||
+        p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY || p->nx < 6 || p->ny < 6 || p->scl_mode < 1 ||
         p->scl_mode > 4 || p->scf_mode < 1 || p->scl_mode * p->scf_mode > 16 || !p->bessel || !p->abc_alpha)
       return bad(FELIS_BAD_ARG, "instance parameters rejected (one species, 3D, L <= 4)");
     Inst& I = b->in[k];
@@ -659,10 +704,12 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
     if (p->wake_e) std::copy(p->wake_e, p->wake_e + p->global_slice_n, wk.begin());
     if (e == cudaSuccess) e = cudaMalloc(&I.wake, wk.size() * sizeof(double));
     if (e == cudaSuccess) e = cudaMemcpy(I.wake, wk.data(), wk.size() * sizeof(double), cudaMemcpyHostToDevice);
+    adi_chunks(p->nx - 2, I.cx);
+    adi_chunks(p->ny - 2, I.cy);
     std::vector<float2> tabs;
     for (int h = 0; h < H; ++h) {
       std::vector<float2> t;
-      adi_tables(*p, h, M, t);
+      adi_tables(*p, h, M, I.cx, I.cy, t);
       tabs.insert(tabs.end(), t.begin(), t.end());
     }
     if (e == cudaSuccess) e = cudaMalloc(&I.adi, tabs.size() * sizeof(float2));

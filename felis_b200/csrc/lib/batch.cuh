@@ -15,7 +15,11 @@ typedef int acc_t;
 // per-step energy exchange, while dg (of the size of the energy spread)
 // resolves it to 1e-7.
 struct BInst {
-  int S, nx, ny, N, H, L, F, nr, nxp, bn, bcols, numSlice, minI, wakeOn;
+  int S, nx, ny, N, H, L, F, nr, bn, bcols, numSlice, minI, wakeOn;
+  // ADI: row pitch of the shared-memory plane of interior cells (odd, >= nx - 2)
+  // and the four chunks each interior row / column is split into (starts,
+  // then the interior count): cx over the nx - 2 columns, cy over the rows
+  int pitch, cx[5], cy[5];
   int nsrc;                             // source planes per slice
   int harmony[FELIS_MAX_HARMONY];
   int src_plane[FELIS_MAX_HARMONY];     // first source plane of each harmonic
@@ -30,7 +34,7 @@ struct BInst {
   int4* sbox;            // [S] cell box of that source (bi0, bi1, bj0, bj1)
   const float* bessel;   // [bn][bcols]
   const double* wakeE;   // global slices
-  const float2* adi_c;   // per harmonic: 12 complex tables of max(nx, ny) (batch.cu)
+  const float2* adi_c;   // per harmonic: 16 complex tables of max(nx, ny), interior index (batch.cu)
   double* part_e;        // [S][H*2] plane energies of the last ADI
   double* part_b;        // [S][7 + 2H + 1] beam partial sums of the last push
   int* err;              // [ERR_SLOTS]

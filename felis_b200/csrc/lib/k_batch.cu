@@ -2,8 +2,9 @@
 //
 //   k_batch_adi   one CTA per field plane (instance, slice, harmonic,
 //                 polarisation): the ADI of solveField.cpp:80-185 in FP32 with
-//                 the plane, the recurrence tables and the slice's source box
-//                 staged in shared memory; emits the plane's |U|^2 sum.
+//                 the interior plane, the recurrence tables and the slice's
+//                 source box in shared memory, four threads per line
+//                 (partitioned recurrences); emits the plane's |U|^2 sum.
 //   k_batch_push  one CTA per (instance, slice): both transverse half-pushes,
 //                 push_theta_gamma or the drift, the theta wrap, the beam
 //                 partial sums (particlePush.cpp, rearrangeParticles.cpp,
@@ -119,26 +120,74 @@ __device__ __forceinline__ float quantum(float bound) {
 }
 
 // ============================================================================
-// ADI (solveField.cpp:80-185), one CTA per plane, thread per row / column.
+// ADI (solveField.cpp:80-185), one CTA per plane.
+//
+// Each sweep is a forward and a backward first-order linear recurrence along
+// every interior row (x) or column (y), with data-independent coefficients.
+// Four threads (a lane quad) share a line, one chunk each: a thread runs the
+// recurrence over its chunk from a zero start, the quad composes the chunks'
+// affine carry maps with two shuffles (a scan over four elements), and the
+// thread corrects its chunk by the carry times the chunk product of the
+// coefficients (host tables G, Q).  Exact in real arithmetic; in FP32 the
+// rounding differs from the serial order by a few ulps.
+//
+// The right-hand side of each sweep reads the neighbouring lines, which other
+// threads overwrite: the x sweep's is formed in place in the staged plane
+// (thread per column chunk, rows in registers, the rows either side of the
+// chunk read before a barrier), the y sweep's while the x sweep's result is
+// finished (thread per row chunk).  Four barriers per plane; the final values
+// go straight to global memory (edge cells keep their values: the ADI never
+// writes them).
 // ============================================================================
-__global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
+__device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
+  return make_float2(__shfl_up_sync(0xffffffffu, v.x, d, 4), __shfl_up_sync(0xffffffffu, v.y, d, 4));
+}
+__device__ __forceinline__ float2 shfl_down2(float2 v, int d) {
+  return make_float2(__shfl_down_sync(0xffffffffu, v.x, d, 4), __shfl_down_sync(0xffffffffu, v.y, d, 4));
+}
+// Carry into chunk q of the forward recurrence x_c = L_c + G_c x_{start-1}:
+// the composition of the maps of chunks 0..q-1 applied to zero.
+__device__ __forceinline__ float2 carry_fwd(float2 g, float2 l, int q) {
+#pragma unroll
+  for (int d = 1; d < 4; d <<= 1) {
+    const float2 gp = shfl_up2(g, d), lp = shfl_up2(l, d);
+    if (q >= d) { l = cad(l, cm(g, lp)); g = cm(g, gp); }
+  }
+  const float2 ex = shfl_up2(l, 1);
+  return q == 0 ? make_float2(0.f, 0.f) : ex;
+}
+// Carry into chunk q of the backward recurrence x_c = B_c + Q_c x_{end+1}.
+__device__ __forceinline__ float2 carry_bwd(float2 g, float2 l, int q) {
+#pragma unroll
+  for (int d = 1; d < 4; d <<= 1) {
+    const float2 gp = shfl_down2(g, d), lp = shfl_down2(l, d);
+    if (q + d < 4) { l = cad(l, cm(g, lp)); g = cm(g, gp); }
+  }
+  const float2 ex = shfl_down2(l, 1);
+  return q == 3 ? make_float2(0.f, 0.f) : ex;
+}
+
+__global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ double redd[8];
+  __shared__ double redd[32];
   const int4 wi = a.work[blockIdx.x];
   const BInst& I = a.inst[wi.x];
   const BStep& T = a.step[wi.x];
   const int s = wi.y, hp = wi.z, h = hp >> 1, pol = hp & 1;
-  const int S = I.S, nx = I.nx, ny = I.ny, N = I.N, nxp = I.nxp, Mx = nx > ny ? nx : ny;
+  const int S = I.S, nx = I.nx, ny = I.ny, P = I.pitch, Mx = nx > ny ? nx : ny;
+  const int mx = nx - 2, my = ny - 2;
   const int tid = threadIdx.x, nt = blockDim.x;
-  float2* U = I.U + ((size_t)hp * S + (s + T.ring_base) % S) * N;
-  const float2* ad = I.adi_c + (size_t)h * 12 * Mx;
-  float2* pl = reinterpret_cast<float2*>(sm);
-  float2* tb = pl + (size_t)ny * nxp;  // 6 recurrence tables of Mx complex
-  float2* ssrc = tb + 6 * Mx;
-  const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
-  for (int k = tid; k < 6 * Mx; k += nt) cp_async8(tb + k, ad + k);
-  for (int r = warp; r < ny; r += nwarp)
-    for (int c = lane; c < nx; c += 32) cp_async8(pl + r * nxp + c, U + r * nx + c);
+  float2* U = I.U + ((size_t)hp * S + (s + T.ring_base) % S) * I.N;
+  const float2* ad = I.adi_c + (size_t)h * 16 * Mx;
+  float2* pl = reinterpret_cast<float2*>(sm);  // interior cells, [my][P]
+  float2* tb = pl + (size_t)my * P;            // 16 tables of Mx
+  float2* ssrc = tb + 16 * Mx;
+  for (int k = tid; k < 16 * Mx; k += nt) cp_async8(tb + k, ad + k);
+  {
+    const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
+    for (int r = warp; r < my; r += nwarp)
+      for (int c = lane; c < mx; c += 32) cp_async8(pl + r * P + c, U + (size_t)(r + 1) * nx + c + 1);
+  }
   // source of this plane: odd harmonic -eta f m (one plane m for both
   // polarisations), even harmonic its own plane
   int bi0 = 1, bi1 = 0, bj0 = 1, bj1 = 0, bw = 0;
@@ -151,8 +200,8 @@ __global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
     const int cells = (bw > 0 && bj1 >= bj0) ? bw * (bj1 - bj0 + 1) : 0;
     // the deposit packs the slice's source planes back to back, `cells` each
     const int p = I.src_plane[h] + ((I.harmony[h] & 1) ? 0 : pol);
-    const float2* g = I.src + (size_t)s * I.nsrc * N + (size_t)p * cells;
-    const size_t used = ((size_t)ny * nxp + 6 * (size_t)Mx) * sizeof(float2);
+    const float2* g = I.src + (size_t)s * I.nsrc * I.N + (size_t)p * cells;
+    const size_t used = ((size_t)my * P + 16 * (size_t)Mx) * sizeof(float2);
     if (cells > 0 && used + (size_t)cells * sizeof(float2) <= (size_t)a.smem_bytes) {
       for (int k = tid; k < cells; k += nt) cp_async8(ssrc + k, g + k);
       Sc = ssrc;
@@ -165,86 +214,164 @@ __global__ void __launch_bounds__(256) k_batch_adi(BatchLaunch a) {
   const bool src = Sc != nullptr;
   cp_async_wait_all();
   __syncthreads();
-  const float2* px_ = tb;             // 1/alphaP (last: 1)
-  const float2* mx_ = tb + Mx;        // alpha / (alphaP CC[i-1])
-  const float2* rx_ = tb + 2 * Mx;    // 1/CC
-  const float2* py_ = tb + 3 * Mx;
-  const float2* my_ = tb + 4 * Mx;
-  const float2* ry_ = tb + 5 * Mx;
-  // x sweep (thread per row), one barrier per column so that every row has
-  // read column i of U before any row overwrites it
-  const int j = tid;
-  const bool row = j >= 1 && j <= ny - 2;
-  float2 DD = make_float2(0.f, 0.f);
-  float2 ra = make_float2(0, 0), rb = ra, rc = ra, edge0 = ra, edge1 = ra;
-  if (row) {
-    ra = ad[6 * Mx + j]; rb = ad[7 * Mx + j]; rc = ad[8 * Mx + j];  // -betaP, H+betaP+beta, beta
-    edge0 = pl[j * nxp]; edge1 = pl[j * nxp + nx - 1];             // the ADI keeps the edge columns
-  }
-  const bool rowin = row && src && j >= bj0 && j <= bj1;
-  for (int i = 1; i <= nx - 2; ++i) {
-    float2 up = make_float2(0, 0), u0 = up, um = up, sv = up;
-    if (row) {
-      up = pl[(j + 1) * nxp + i]; u0 = pl[j * nxp + i]; um = pl[(j - 1) * nxp + i];
-      if (rowin && i >= bi0 && i <= bi1) sv = cm(sfac, Sc[(j - bj0) * bw + (i - bi0)]);
-    }
-    __syncthreads();
-    if (row) {
-      const float2 t = cad(cad(cm(ra, up), cm(rb, u0)), csb(sv, cm(rc, um)));
-      DD = csb(cm(t, px_[i]), cm(mx_[i], DD));
-      pl[j * nxp + i] = DD;
-    }
-  }
-  if (row) {
-    float2 Uc = cm(DD, rx_[nx - 2]);
-    pl[j * nxp + nx - 2] = Uc;
-    for (int i = nx - 3; i > 0; --i) {
-      Uc = cm(csb(pl[j * nxp + i], Uc), rx_[i]);
-      pl[j * nxp + i] = Uc;
-    }
-    pl[j * nxp] = make_float2(0.f, 0.f);
-    pl[j * nxp + nx - 1] = make_float2(0.f, 0.f);
-  }
-  __syncthreads();
-  // y sweep (thread per column), one barrier per row
-  const int i = tid;
-  const bool col = i >= 1 && i <= nx - 2;
-  if (col) { ra = ad[9 * Mx + i]; rb = ad[10 * Mx + i]; rc = ad[11 * Mx + i]; }  // -alphaP, H+alphaP+alpha, alpha
-  const bool colin = col && src && i >= bi0 && i <= bi1;
-  DD = make_float2(0.f, 0.f);
-  for (int jr = 1; jr <= ny - 2; ++jr) {
-    float2 up = make_float2(0, 0), u0 = up, um = up, sv = up;
-    if (col) {
-      up = pl[jr * nxp + i + 1]; u0 = pl[jr * nxp + i]; um = pl[jr * nxp + i - 1];
-      if (colin && jr >= bj0 && jr <= bj1) sv = cm(sfac, Sc[(jr - bj0) * bw + (i - bi0)]);
-    }
-    __syncthreads();
-    if (col) {
-      const float2 t = cad(cad(cm(ra, up), cm(rb, u0)), csb(sv, cm(rc, um)));
-      DD = csb(cm(t, py_[jr]), cm(my_[jr], DD));
-      pl[jr * nxp + i] = DD;
-    }
-  }
-  if (col) {
-    float2 Un = cm(DD, ry_[ny - 2]);
-    pl[(ny - 2) * nxp + i] = Un;
-    for (int jr = ny - 3; jr > 0; --jr) {
-      Un = cm(csb(pl[jr * nxp + i], Un), ry_[jr]);
-      pl[jr * nxp + i] = Un;
-    }
-  }
-  __syncthreads();
-  if (row) { pl[j * nxp] = edge0; pl[j * nxp + nx - 1] = edge1; }
-  __syncthreads();
-  // write the plane back and sum |U|^2 over it (edge rows and columns keep
-  // their old values: the ADI never writes them)
+  const float2 zero = make_float2(0.f, 0.f);
+  auto source = [&](int j, int i) -> float2 {
+    if (src && i >= bi0 && i <= bi1 && j >= bj0 && j <= bj1) return cm(sfac, Sc[(j - bj0) * bw + (i - bi0)]);
+    return zero;
+  };
+  // ---- x sweep right-hand side: thread (column, row chunk), in place in the
+  // staged plane; the rows either side of the chunk are read first
   double e = 0.0;
-  for (int r = warp; r < ny; r += nwarp)
-    for (int c = lane; c < nx; c += 32) {
-      const float2 v = pl[r * nxp + c];
-      U[r * nx + c] = v;
+  {
+    const int c = tid % mx, qc = tid / mx;
+    const bool valid = qc < 4;
+    const int r0 = valid ? I.cy[qc] : 0, r1 = valid ? I.cy[qc + 1] : 0, i = c + 1;
+    float2 um = zero, ul = zero;
+    if (valid) {
+      um = r0 == 0 ? U[i] : pl[(r0 - 1) * P + c];
+      ul = r1 == my ? U[(size_t)(ny - 1) * nx + i] : pl[r1 * P + c];
+    }
+    // |U|^2 of the edge cells, which keep their values
+    const int ne = 2 * nx + 2 * my;
+    for (int k = tid; k < ne; k += nt) {
+      float2 v;
+      if (k < nx) v = U[k];
+      else if (k < 2 * nx) v = U[(size_t)(ny - 1) * nx + (k - nx)];
+      else v = U[(size_t)(((k - 2 * nx) >> 1) + 1) * nx + (((k - 2 * nx) & 1) ? nx - 1 : 0)];
       e += (double)(v.x * v.x + v.y * v.y);
     }
+    __syncthreads();
+    // every loop below loads the next step's operands before it stores: the
+    // compiler cannot move a shared-memory load above a store to the same array
+    if (valid) {
+      const float2* ra = tb + 10 * Mx;
+      const float2* rb = tb + 11 * Mx;
+      const float2* rc = tb + 12 * Mx;
+      float2 u0 = pl[r0 * P + c];
+      float2 up = r0 + 1 < r1 ? pl[(r0 + 1) * P + c] : ul;
+      float2 ka = ra[r0], kb = rb[r0], kc = rc[r0], sv = source(r0 + 1, i);
+      for (int r = r0; r < r1; ++r) {
+        const int rn = r + 1 < r1 ? r + 1 : r;
+        const float2 upn = r + 2 < r1 ? pl[(r + 2) * P + c] : ul;
+        const float2 kan = ra[rn], kbn = rb[rn], kcn = rc[rn], svn = source(rn + 1, i);
+        pl[r * P + c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
+        um = u0;
+        u0 = up;
+        up = upn;
+        ka = kan; kb = kbn; kc = kcn; sv = svn;
+      }
+    }
+  }
+  __syncthreads();
+  const int q = tid & 3, line = tid >> 2;
+  // ---- x sweep: thread (row, column chunk)
+  {
+    const float2* pa = tb;
+    const float2* pm = tb + Mx;
+    const float2* pr = tb + 2 * Mx;
+    const float2* pG = tb + 3 * Mx;
+    const float2* pQ = tb + 4 * Mx;
+    const bool valid = line < my;
+    const int c0 = I.cx[q], c1 = I.cx[q + 1];
+    float2* row = pl + (valid ? line : 0) * P;
+    float2 L = zero;
+    if (valid) {
+      float2 v = row[c0], ka = pa[c0], km = pm[c0];
+      for (int c = c0; c < c1; ++c) {
+        const int cn = c + 1 < c1 ? c + 1 : c;
+        const float2 vn = row[cn], kan = pa[cn], kmn = pm[cn];
+        L = csb(cm(v, ka), cm(km, L));
+        row[c] = L;
+        v = vn; ka = kan; km = kmn;
+      }
+    }
+    const float2 din = carry_fwd(pG[c1 - 1], L, q);
+    float2 B = zero, Blast = zero;
+    if (valid) {
+      float2 v = row[c1 - 1], kg = pG[c1 - 1], kr = pr[c1 - 1];
+      for (int c = c1 - 1; c >= c0; --c) {
+        const int cn = c > c0 ? c - 1 : c;
+        const float2 vn = row[cn], kgn = pG[cn], krn = pr[cn];
+        B = cm(csb(cad(v, cm(kg, din)), B), kr);
+        row[c] = B;
+        if (c == c1 - 1) Blast = B;
+        v = vn; kg = kgn; kr = krn;
+      }
+    }
+    const float2 uin = carry_bwd(pQ[c0], B, q);
+    // x sweep result at the chunk's last point, and from the quad's previous
+    // thread at the point left of the chunk (zero left of the first column)
+    const float2 uend = cad(Blast, cm(pQ[c1 - 1], uin));
+    const float2 uprev = shfl_up2(uend, 1);
+    // ---- finish the x sweep and form the y sweep's right-hand side
+    if (valid) {
+      const float2* ra = tb + 13 * Mx;
+      const float2* rb = tb + 14 * Mx;
+      const float2* rc = tb + 15 * Mx;
+      const int j = line + 1;
+      float2 um = q == 0 ? zero : uprev;
+      float2 u0 = cad(row[c0], cm(pQ[c0], uin));
+      float2 up = c0 + 1 < c1 ? cad(row[c0 + 1], cm(pQ[c0 + 1], uin)) : uin;
+      float2 ka = ra[c0], kb = rb[c0], kc = rc[c0], sv = source(j, c0 + 1);
+      for (int c = c0; c < c1; ++c) {
+        const int cn = c + 1 < c1 ? c + 1 : c, c2 = c + 2 < c1 ? c + 2 : c;
+        const float2 b2 = row[c2], q2 = pQ[c2];
+        const float2 kan = ra[cn], kbn = rb[cn], kcn = rc[cn], svn = source(j, cn + 1);
+        row[c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
+        um = u0;
+        u0 = up;
+        up = c + 2 < c1 ? cad(b2, cm(q2, uin)) : uin;
+        ka = kan; kb = kbn; kc = kcn; sv = svn;
+      }
+    }
+  }
+  __syncthreads();
+  // ---- y sweep: thread (column, row chunk); results to global memory
+  {
+    const float2* pa = tb + 5 * Mx;
+    const float2* pm = tb + 6 * Mx;
+    const float2* pr = tb + 7 * Mx;
+    const float2* pG = tb + 8 * Mx;
+    const float2* pQ = tb + 9 * Mx;
+    const bool valid = line < mx;
+    const int c = valid ? line : 0;
+    const int r0 = I.cy[q], r1 = I.cy[q + 1];
+    float2 L = zero;
+    if (valid) {
+      float2 v = pl[r0 * P + c], ka = pa[r0], km = pm[r0];
+      for (int r = r0; r < r1; ++r) {
+        const int rn = r + 1 < r1 ? r + 1 : r;
+        const float2 vn = pl[rn * P + c], kan = pa[rn], kmn = pm[rn];
+        L = csb(cm(v, ka), cm(km, L));
+        pl[r * P + c] = L;
+        v = vn; ka = kan; km = kmn;
+      }
+    }
+    const float2 din = carry_fwd(pG[r1 - 1], L, q);
+    float2 B = zero;
+    if (valid) {
+      float2 v = pl[(r1 - 1) * P + c], kg = pG[r1 - 1], kr = pr[r1 - 1];
+      for (int r = r1 - 1; r >= r0; --r) {
+        const int rn = r > r0 ? r - 1 : r;
+        const float2 vn = pl[rn * P + c], kgn = pG[rn], krn = pr[rn];
+        B = cm(csb(cad(v, cm(kg, din)), B), kr);
+        pl[r * P + c] = B;
+        v = vn; kg = kgn; kr = krn;
+      }
+    }
+    const float2 uin = carry_bwd(pQ[r0], B, q);
+    if (valid) {
+      float2 v = pl[r0 * P + c], kq = pQ[r0];
+      for (int r = r0; r < r1; ++r) {
+        const int rn = r + 1 < r1 ? r + 1 : r;
+        const float2 vn = pl[rn * P + c], kqn = pQ[rn];
+        const float2 o = cad(v, cm(kq, uin));
+        U[(size_t)(r + 1) * nx + c + 1] = o;
+        e += (double)(o.x * o.x + o.y * o.y);
+        v = vn; kq = kqn;
+      }
+    }
+  }
   const double et = block_sum_d(e, redd);
   if (tid == 0) I.part_e[(size_t)s * 2 * I.H + hp] = et;
 }
@@ -849,7 +976,7 @@ PushKernel push_kernel(int H) {
 
 size_t batch_adi_smem(int nx_max, int ny_max, int src_cells) {
   const int M = nx_max > ny_max ? nx_max : ny_max;
-  return ((size_t)ny_max * (nx_max | 1) + 6 * (size_t)M + (size_t)src_cells) * sizeof(float2);
+  return ((size_t)(ny_max - 2) * ((nx_max - 2) | 1) + 16 * (size_t)M + (size_t)src_cells) * sizeof(float2);
 }
 
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
