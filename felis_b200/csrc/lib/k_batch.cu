@@ -626,6 +626,27 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     const float dzf = (float)dz;
     const float2* __restrict__ Ubase = I.U + (size_t)plane * N;
     const size_t hpstride = (size_t)S * N;
+    // the slice's field around the beam, staged in the area the deposit
+    // uses afterwards: the cell box of the last deposit (where the particles
+    // were after the last push) with a margin of 3 cells; a particle outside
+    // it reads global memory.  Same values, so the same results.
+    int fi0 = 0, fi1 = -1, fj0 = 0, fj1 = -1, fbw = 1, fcells = 0;
+    const float2* sF = reinterpret_cast<const float2*>(area);
+    {
+      const int4 b = I.sbox[s];
+      if (b.y >= b.x && b.w >= b.z) {
+        const int i0 = max(0, b.x - 3), i1 = min(nx - 1, b.y + 3), j0 = max(0, b.z - 3), j1 = min(ny - 1, b.w + 3);
+        const int w = i1 - i0 + 1, cells = w * (j1 - j0 + 1);
+        if ((size_t)2 * H * cells * sizeof(float2) <= area_bytes) {
+          fi0 = i0; fi1 = i1; fj0 = j0; fj1 = j1; fbw = w; fcells = cells;
+          float2* dst = reinterpret_cast<float2*>(area);
+          for (int hp = 0; hp < 2 * H; ++hp)
+            for (int k = tid; k < cells; k += nt)
+              cp_async8(dst + (size_t)hp * cells + k, Ubase + hp * hpstride + (size_t)(j0 + k / w) * nx + i0 + k % w);
+        }
+      }
+      cp_async_wait_all();
+    }
     __syncthreads();
     const float4* m4 = reinterpret_cast<const float4*>(smap);
     double acc7[7] = {0, 0, 0, 0, 0, 0, 0};
@@ -668,13 +689,17 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
         const float wx1 = gx - ii, wy1 = gy - jj, wx0 = 1.f - wx1, wy0 = 1.f - wy1;
         float2 Ux[HM], Uy[HM];
         float sumU2 = 0.f;
+        const bool staged = ii >= fi0 && ii < fi1 && jj >= fj0 && jj < fj1;
+        const float2* fb = staged ? sF + (jj - fj0) * fbw + (ii - fi0) : Ubase + jj * nx + ii;
+        const size_t fps = staged ? (size_t)fcells : hpstride;
+        const int frs = staged ? fbw : nx;
 #pragma unroll
         for (int h = 0; h < HM; ++h) {
           if (h >= H) break;
-          const float2* Px = Ubase + (2 * h) * hpstride + jj * nx + ii;
-          const float2* Py = Px + hpstride;
-          Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[nx], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[nx + 1], wx1 * wy1)));
-          Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[nx], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[nx + 1], wx1 * wy1)));
+          const float2* Px = fb + (2 * h) * fps;
+          const float2* Py = Px + fps;
+          Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[frs], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[frs + 1], wx1 * wy1)));
+          Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[frs], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[frs + 1], wx1 * wy1)));
           const float Hh = (float)hh[h];
           sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
         }
