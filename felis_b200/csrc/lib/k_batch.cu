@@ -579,12 +579,16 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
   acc_t* sR = reinterpret_cast<acc_t*>(sm + o1);
   unsigned char* area = sm + o2;
   const size_t area_bytes = (size_t)a.smem_bytes - o2;
-  // deposit statistics of the (pushed) beam: cell box and fixed-point bounds
+  // deposit statistics of the (pushed) beam: cell box and fixed-point bounds.
+  // The bounds are conservative and free of per-particle divisions: the 2-D
+  // term |w mc| / weight <= max(wm fb) / min|g| per thread; the radial term
+  // (1 + |wr1|) / max(ir, 1) <= 1.625 (|wr1| <= 5/8 for ir >= 1), counted when
+  // a particle may lie inside the radial grid.
   int ci0 = 1 << 30, ci1 = -(1 << 30), cj0 = 1 << 30, cj1 = -(1 << 30);
-  float bmax = 0.f, rmax = 0.f;
-  auto stats = [&](float x, float y, float px, float py, float g) {
-    const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
-    const int ii = (int)gx, jj = (int)gy;
+  float wfmax = 0.f, gmin = 3.0e38f;
+  int rin = 0;
+  const float rlim2 = ((float)nr + 0.5f) * dr * ((float)nr + 0.5f) * dr;
+  auto stats = [&](float gx, float gy, int ii, int jj, float x, float y, float px, float py, float g) {
     if (ii >= 0 && ii < nx && jj >= 0 && jj < ny) {
       ci0 = min(ci0, ii); ci1 = max(ci1, ii); cj0 = min(cj0, jj); cj1 = max(cj1, jj);
       const float w1 = gx - ii, v1 = gy - jj;
@@ -596,14 +600,10 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
         pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
         fb = fmaxf(fb, 2.f * xi2 * Hmax);
       }
-      bmax = fmaxf(bmax, wm * fb / fabsf(g));
+      wfmax = fmaxf(wfmax, wm * fb);
+      gmin = fminf(gmin, fabsf(g));
     }
-    const float r = sqrtf(x * x + y * y);
-    const int ir = (int)(r / dr + 0.5f);
-    if (ir >= 0 && ir < nr) {
-      const float wr1 = ir > 0 ? fabsf((r * r * idr2 - (float)(ir * ir)) / (2.f * ir)) : 0.f;
-      rmax = fmaxf(rmax, (1.f + wr1) / (ir > 0 ? (float)ir : 1.f));
-    }
+    rin |= (x * x + y * y < rlim2) ? 1 : 0;
   };
   // ================= pass 1: push (particlePush.cpp) =================
   if (push) {
@@ -800,7 +800,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
         bre[h] += (double)e.x;
         bim[h] += (double)e.y;
       }
-      if (dep) stats(x, y, px, py, gRf + dg);
+      if (dep) stats(gx, gy, ii, jj, x, y, px, py, gRf + dg);
     }
     wsum = (double)weight * (double)max(0, (P - tid + nt - 1) / nt);
     if (bad_over) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
@@ -831,7 +831,8 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
   } else if (dep) {
     for (int q = tid; q < P; q += nt) {
       const int64_t n = p0 + q;
-      stats(xs[n], ys[n], has_even ? pxs[n] : 0.f, has_even ? pys[n] : 0.f, gRf + dgs[n]);
+      const float x = xs[n], y = ys[n], gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+      stats(gx, gy, (int)gx, (int)gy, x, y, has_even ? pxs[n] : 0.f, has_even ? pys[n] : 0.f, gRf + dgs[n]);
     }
   }
   if (!dep) return;
@@ -841,6 +842,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
   // bounds: |w mc| <= wm H weight coef_U / g for odd harmonics, times |f| <=
   // 2 xi2 H for even ones (|eta| <= 1, |e| = 1); radial |w c| <= coef_Ez L
   // weight (1 + |wr1|) / max(ir, 1)
+  const float bmax = wfmax > 0.f ? wfmax / gmin : 0.f, rmax = rin ? 1.625f : 0.f;
   const float bnd = block_max_f(bmax, redf) * 1.0625f * Hmax * weight * fabsf(D.coef_U) * (float)P;
   const float rbnd = block_max_f(rmax, redf) * 1.0625f * L * weight * fabsf(D.coef_Ez) * (float)P;
   // interior targets a particle can reach
