@@ -215,10 +215,6 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   cp_async_wait_all();
   __syncthreads();
   const float2 zero = make_float2(0.f, 0.f);
-  auto source = [&](int j, int i) -> float2 {
-    if (src && i >= bi0 && i <= bi1 && j >= bj0 && j <= bj1) return cm(sfac, Sc[(j - bj0) * bw + (i - bi0)]);
-    return zero;
-  };
   // ---- x sweep right-hand side: thread (column, row chunk), in place in the
   // staged plane; the rows either side of the chunk are read first
   double e = 0.0;
@@ -249,11 +245,17 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       const float2* rc = tb + 12 * Mx;
       float2 u0 = pl[r0 * P + c];
       float2 up = r0 + 1 < r1 ? pl[(r0 + 1) * P + c] : ul;
-      float2 ka = ra[r0], kb = rb[r0], kc = rc[r0], sv = source(r0 + 1, i);
+      // the source term of this column: one range test per column, one per row
+      const bool scol = src && i >= bi0 && i <= bi1;
+      const float2* sc = scol ? Sc + (i - bi0) : Sc;
+      auto srow = [&](int j) -> float2 {
+        return (scol && j >= bj0 && j <= bj1) ? cm(sfac, sc[(j - bj0) * bw]) : zero;
+      };
+      float2 ka = ra[r0], kb = rb[r0], kc = rc[r0], sv = srow(r0 + 1);
       for (int r = r0; r < r1; ++r) {
         const int rn = r + 1 < r1 ? r + 1 : r;
         const float2 upn = r + 2 < r1 ? pl[(r + 2) * P + c] : ul;
-        const float2 kan = ra[rn], kbn = rb[rn], kcn = rc[rn], svn = source(rn + 1, i);
+        const float2 kan = ra[rn], kbn = rb[rn], kcn = rc[rn], svn = srow(rn + 1);
         pl[r * P + c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
         um = u0;
         u0 = up;
@@ -278,7 +280,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
     if (valid) {
       float2 v = row[c0], ka = pa[c0], km = pm[c0];
       for (int c = c0; c < c1; ++c) {
-        const int cn = c + 1 < c1 ? c + 1 : c;
+        const int cn = c + 1;  // one past the chunk stays inside the plane or the tables
         const float2 vn = row[cn], kan = pa[cn], kmn = pm[cn];
         L = csb(cm(v, ka), cm(km, L));
         row[c] = L;
@@ -312,11 +314,14 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       float2 um = q == 0 ? zero : uprev;
       float2 u0 = cad(row[c0], cm(pQ[c0], uin));
       float2 up = c0 + 1 < c1 ? cad(row[c0 + 1], cm(pQ[c0 + 1], uin)) : uin;
-      float2 ka = ra[c0], kb = rb[c0], kc = rc[c0], sv = source(j, c0 + 1);
+      const bool srw = src && j >= bj0 && j <= bj1;
+      const float2* sr = srw ? Sc + (j - bj0) * bw : Sc;
+      auto scolv = [&](int i) -> float2 { return (srw && i >= bi0 && i <= bi1) ? cm(sfac, sr[i - bi0]) : zero; };
+      float2 ka = ra[c0], kb = rb[c0], kc = rc[c0], sv = scolv(c0 + 1);
       for (int c = c0; c < c1; ++c) {
-        const int cn = c + 1 < c1 ? c + 1 : c, c2 = c + 2 < c1 ? c + 2 : c;
+        const int cn = c + 1, c2 = c + 2;  // past the chunk: read, not used
         const float2 b2 = row[c2], q2 = pQ[c2];
-        const float2 kan = ra[cn], kbn = rb[cn], kcn = rc[cn], svn = source(j, cn + 1);
+        const float2 kan = ra[cn], kbn = rb[cn], kcn = rc[cn], svn = scolv(cn + 1);
         row[c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
         um = u0;
         u0 = up;
@@ -340,7 +345,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
     if (valid) {
       float2 v = pl[r0 * P + c], ka = pa[r0], km = pm[r0];
       for (int r = r0; r < r1; ++r) {
-        const int rn = r + 1 < r1 ? r + 1 : r;
+        const int rn = r + 1;
         const float2 vn = pl[rn * P + c], kan = pa[rn], kmn = pm[rn];
         L = csb(cm(v, ka), cm(km, L));
         pl[r * P + c] = L;
@@ -363,7 +368,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
     if (valid) {
       float2 v = pl[r0 * P + c], kq = pQ[r0];
       for (int r = r0; r < r1; ++r) {
-        const int rn = r + 1 < r1 ? r + 1 : r;
+        const int rn = r + 1;
         const float2 vn = pl[rn * P + c], kqn = pQ[rn];
         const float2 o = cad(v, cm(kq, uin));
         U[(size_t)(r + 1) * nx + c + 1] = o;
