@@ -1,7 +1,9 @@
 """One process of the sharded slice loop on CPU (gloo), driven by test_shard.py.
 
 argv: input file, iterations it0 it1, output .npz, engine ("oracle": the CPU
-restatement; "gpu": a felis_b200.Handle on cuda:0).  RANK, WORLD_SIZE,
+restatement; "gpu": a felis_b200.Handle on cuda:0), and optionally a
+directory for a checkpoint of the end state written by all processes
+together (felis_b200.checkpoint).  RANK, WORLD_SIZE,
 MASTER_ADDR and MASTER_PORT come from the environment.  The initial state is
 the single-process beam and seed field cut into this process's slice block,
 so the blocks together start from exactly the state of the single-process run.
@@ -20,13 +22,14 @@ sys.path.insert(0, os.path.join(ROOT, "oracle"))
 def main():
     path, it0, it1, out = sys.argv[1], int(sys.argv[2]), int(sys.argv[3]), sys.argv[4]
     engine = sys.argv[5] if len(sys.argv) > 5 else "oracle"
+    ckpt = sys.argv[6] if len(sys.argv) > 6 else None
     rank, world = int(os.environ["RANK"]), int(os.environ["WORLD_SIZE"])
 
     import torch.distributed as dist
 
     import felis_b200 as fb
     import oracle
-    from felis_b200 import shard
+    from felis_b200 import checkpoint, shard
 
     dist.init_process_group("gloo", rank=rank, world_size=world, timeout=datetime.timedelta(seconds=60))
     try:
@@ -61,6 +64,9 @@ def main():
             for pol in (0, 1):
                 res[f"U{h}{pol}"] = get_field(h, pol)[1:-1]
         np.savez(out, **res)
+        if ckpt:
+            checkpoint.save_field(o, p, ckpt, it1, dist=dist)
+            checkpoint.save_particles(o, p, [(b["offsets"], b["weights"])], ckpt, it1, dist=dist)
         dist.barrier()
     finally:
         dist.destroy_process_group()

@@ -28,7 +28,7 @@ def _free_port() -> int:
         return s.getsockname()[1]
 
 
-def _run_ranks(path, world, tmp_path, engine="oracle"):
+def _run_ranks(path, world, tmp_path, engine="oracle", ckpt=None):
     port = _free_port()
     procs, outs = [], []
     for r in range(world):
@@ -36,7 +36,7 @@ def _run_ranks(path, world, tmp_path, engine="oracle"):
         env = dict(os.environ, RANK=str(r), WORLD_SIZE=str(world), MASTER_ADDR="127.0.0.1", MASTER_PORT=str(port),
                    OMP_NUM_THREADS="1")
         procs.append(subprocess.Popen([sys.executable, os.path.join(HERE, "shard_worker.py"), path, str(IT0), str(IT1),
-                                       out, engine], env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
+                                       out, engine] + ([ckpt] if ckpt else []), env=env, stdout=subprocess.PIPE, stderr=subprocess.STDOUT))
         outs.append(out)
     logs = []
     for p in procs:
@@ -79,6 +79,11 @@ def single(fb, oracle_mod, tmp_path_factory):
     res.update(o.get_particles(0))
     res["fields"] = {(h, pol): o.get_field(h, pol)[1:-1] for h in range(p.num_harmony) for pol in (0, 1)}
     res["offsets"] = beam["offsets"]
+    from felis_b200 import checkpoint
+
+    res["ckpt"] = str(tmp)
+    checkpoint.save_field(o, p, str(tmp), IT1)
+    checkpoint.save_particles(o, p, [(beam["offsets"], beam["weights"])], str(tmp), IT1)
     return res
 
 
@@ -108,6 +113,24 @@ def test_sharded_loop_equals_single_process(single, world, tmp_path):
     # the bunching factor is per block; its sums reassemble the whole-bunch value
     tot = sum(r["bsums"] for r in ranks)
     np.testing.assert_allclose(tot[:, :-1] / tot[:, -1:], single["B"], rtol=1e-11, atol=1e-14)
+
+
+def test_sharded_checkpoint_equals_single_process(single, tmp_path):
+    """Two processes write one checkpoint of their blocks (rank 0 gathers,
+    as the reference's collective HDF5 writes assemble one file); it equals
+    the single-process checkpoint of the same state entry for entry, except
+    the per-process particle counts."""
+    d = tmp_path / "ck"
+    d.mkdir()
+    _run_ranks(single["path"], 2, tmp_path, ckpt=str(d))
+    for name in (f"field{IT1}.npz", f"particle{IT1}.npz"):
+        with np.load(d / name) as a, np.load(os.path.join(single["ckpt"], name)) as b:
+            assert set(a.files) == set(b.files)
+            for k in a.files:
+                if k.endswith("/cntP"):
+                    assert a[k].sum() == b[k].sum() and len(a[k]) == 2
+                else:
+                    assert_bits(a[k], b[k], f"{name}:{k}")
 
 
 @pytest.mark.gpu
