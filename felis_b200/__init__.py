@@ -149,6 +149,7 @@ _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
 _sig("felis_config_error", C.c_char_p)
 _sig("felis_config_load_beam", C.c_int, _vp, C.c_int32, C.c_uint64, _i64p, _dp, _dp, _dp, _dp, _dp, _dp, _dp)
+_sig("felis_config_load_beam_device", C.c_int, _vp, C.c_int32, C.c_uint64, _i64p, _dp, _dp, _dp, _dp, _dp, _dp, _dp)
 _sig("felis_config_load_seed", C.c_int, _vp, C.c_int32, _dp, _dp)
 _sig("felis_config_wake", C.c_int, _vp, _dp, _dp)
 _sig("felis_detmath_sincos", None, C.c_double, _dp, _dp)
@@ -170,6 +171,18 @@ def _f64(a) -> np.ndarray:
     return np.ascontiguousarray(a, dtype=np.float64)
 
 
+def _arr64(a):
+    """(owner, double*) of a host array or of a torch CUDA tensor (whose data
+    the uploads copy device to device)."""
+    if getattr(a, "is_cuda", False):
+        import torch
+
+        t = a.to(torch.float64).contiguous()
+        return t, C.cast(C.c_void_p(t.data_ptr()), _dp)
+    h = _f64(a)
+    return h, _p(h)
+
+
 class Config:
     """A parsed FELIS input file (felis_config_load) and its setup tables."""
 
@@ -182,7 +195,7 @@ class Config:
         self.params = _lib.felis_config_params(h).contents
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and _lib is not None:  # (interpreter teardown)
             _lib.felis_config_free(self._h)
             self._h = None
 
@@ -220,6 +233,34 @@ class Config:
         w = np.zeros(S)
         st = _lib.felis_config_load_beam(self._h, species, seed, counts.ctypes.data_as(_i64p),
                                          *(_p(arrs[k]) for k in ("x", "y", "px", "py", "theta", "gamma")), _p(w))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        off = np.zeros(S + 1, dtype=np.int64)
+        off[1:] = np.cumsum(counts)
+        arrs["offsets"] = off
+        arrs["weights"] = w
+        return arrs
+
+    def load_beam_device(self, species: int = 0, seed: int = 0, device: int = 0) -> dict:
+        """load_beam with the per-beamlet work on the GPU: x .. gamma as torch
+        CUDA tensors (float64), offsets and weights as host arrays."""
+        import torch
+
+        S = self.params.slice_n
+        counts = np.zeros(S, dtype=np.int64)
+        st = _lib.felis_config_load_beam_device(self._h, species, seed, counts.ctypes.data_as(_i64p), *([None] * 7))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        n = int(counts.sum())
+        dev = torch.device("cuda", device)
+        arrs = {k: torch.empty(max(n, 1), dtype=torch.float64, device=dev)[:n]
+                for k in ("x", "y", "px", "py", "theta", "gamma")}
+        w = np.zeros(S)
+        with torch.cuda.device(dev):
+            st = _lib.felis_config_load_beam_device(
+                self._h, species, seed, counts.ctypes.data_as(_i64p),
+                *(C.cast(C.c_void_p(arrs[k].data_ptr()), _dp) for k in ("x", "y", "px", "py", "theta", "gamma")),
+                _p(w))
         if st != OK:
             raise FelisError(st, _lib.felis_config_error().decode())
         off = np.zeros(S + 1, dtype=np.int64)
@@ -273,7 +314,7 @@ class Handle:
         self._counts = [0] * self.species
 
     def close(self):
-        if getattr(self, "_h", None):
+        if getattr(self, "_h", None) and _lib is not None:  # (interpreter teardown)
             _lib.felis_destroy(self._h)
             self._h = None
 
@@ -286,10 +327,11 @@ class Handle:
 
     # ---- data in / out ----
     def upload_particles(self, species: int, x, y, px, py, theta, gamma, offsets, weights):
-        arrs = [_f64(a) for a in (x, y, px, py, theta, gamma)]
+        """Host arrays or torch CUDA tensors (Config.load_beam_device)."""
+        arrs = [_arr64(a) for a in (x, y, px, py, theta, gamma)]
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         w = _f64(weights)
-        self._ck(_lib.felis_upload_particles(self._h, species, *(_p(a) for a in arrs), off.ctypes.data_as(_i64p), _p(w)))
+        self._ck(_lib.felis_upload_particles(self._h, species, *(p for _, p in arrs), off.ctypes.data_as(_i64p), _p(w)))
         self._counts[species] = int(off[-1])
 
     def download_particles(self, species: int = 0) -> dict:
@@ -460,7 +502,7 @@ class Batch:
         self._counts = [0] * self.n
 
     def close(self):
-        if getattr(self, "_b", None):
+        if getattr(self, "_b", None) and _lib is not None:  # (interpreter teardown)
             _lib.felis_batch_destroy(self._b)
             self._b = None
 
@@ -472,10 +514,11 @@ class Batch:
             raise FelisError(st, _lib.felis_batch_last_error(self._b).decode())
 
     def upload_particles(self, inst: int, x, y, px, py, theta, gamma, offsets, weights):
-        arrs = [_f64(a) for a in (x, y, px, py, theta, gamma)]
+        """Host arrays or torch CUDA tensors (Config.load_beam_device)."""
+        arrs = [_arr64(a) for a in (x, y, px, py, theta, gamma)]
         off = np.ascontiguousarray(offsets, dtype=np.int64)
         w = _f64(weights)
-        self._ck(_lib.felis_batch_upload_particles(self._b, inst, *(_p(a) for a in arrs),
+        self._ck(_lib.felis_batch_upload_particles(self._b, inst, *(p for _, p in arrs),
                                                    off.ctypes.data_as(_i64p), _p(w)))
         self._counts[inst] = int(off[-1])
 
@@ -559,7 +602,7 @@ class MLP:
         self.n_params = c.value
 
     def close(self):
-        if getattr(self, "_m", None):
+        if getattr(self, "_m", None) and _lib is not None:  # (interpreter teardown)
             _lib.felis_mlp_destroy(self._m)
             self._m = None
 

@@ -30,6 +30,7 @@
 #include <vector>
 
 #include "../../../include/felis_b200.h"
+#include "../lib/load.cuh"
 
 namespace {
 
@@ -722,6 +723,63 @@ felis_status felis_config_load(const char* path, int32_t num_ranks, int32_t rank
 void felis_config_free(felis_config* c) { delete c; }
 const felis_params* felis_config_params(const felis_config* c) { return c ? &c->p : nullptr; }
 
+}  // extern "C"
+
+namespace {
+
+// Per-slice quantities of loadBeam.cpp (current profile, energy, spread, the
+// matched transverse sizes, beamlet count and macro weight) for slice sl;
+// gamma0 carries over from the previous slice when the profile sets none, as
+// in the reference's loop.
+struct SliceLoad {
+  double dGam, sigX, sigY, sigXPrime, sigYPrime, delTX, delTY, remacro, eNumbers, ESn0;
+  int beamlets;
+};
+
+SliceLoad slice_load(const felis_params& p, const Beam& LL, int sl, double macro, double& gamma0) {
+  SliceLoad L{};
+  const double bucketZ = p.lambda0 * p.num_slice;
+  double n0 = 0.0, En0 = 0.0, ESn0 = 0.0;
+  const double posZ = (sl + p.min_i) * bucketZ + p.min_z;
+  if (LL.type == 1) {
+    for (size_t l = 0; l + 1 < LL.zpoint.size(); ++l)
+      if (posZ >= LL.zpoint[l] && posZ < LL.zpoint[l + 1])
+        n0 = (LL.zn[l + 1] - LL.zn[l]) / (LL.zpoint[l + 1] - LL.zpoint[l]) * (posZ - LL.zpoint[l]) + LL.zn[l];
+    for (size_t l = 0; l + 1 < LL.Epoint.size(); ++l)
+      if (posZ >= LL.Epoint[l] && posZ < LL.Epoint[l + 1])
+        En0 = (LL.En[l + 1] - LL.En[l]) / (LL.Epoint[l + 1] - LL.Epoint[l]) * (posZ - LL.Epoint[l]) + LL.En[l];
+    gamma0 = LL.energy * En0 / kMc2 + 1.0;
+    for (size_t l = 0; l + 1 < LL.ESpoint.size(); ++l)
+      if (posZ >= LL.ESpoint[l] && posZ < LL.ESpoint[l + 1])
+        ESn0 = (LL.ESn[l + 1] - LL.ESn[l]) / (LL.ESpoint[l + 1] - LL.ESpoint[l]) * (posZ - LL.ESpoint[l]) + LL.ESn[l];
+  } else if (LL.type == 2) {
+    const double phase = pow((posZ - LL.posZ) / LL.sigZ, LL.gaussPower);
+    n0 = exp(-phase);
+    gamma0 = (LL.energy + LL.Echirp * (posZ - LL.posZ)) / kMc2 + 1.0;
+  }
+  L.ESn0 = ESn0;
+  L.dGam = LL.spread * gamma0 * ESn0;
+  const double emitX = LL.emitX / gamma0, emitY = LL.emitY / gamma0;
+  const double gammaX = (1 + LL.alphaX * LL.alphaX) / LL.betaX;
+  const double gammaY = (1 + LL.alphaY * LL.alphaY) / LL.betaY;
+  L.sigX = sqrt(emitX / gammaX); L.sigY = sqrt(emitY / gammaY);
+  L.sigXPrime = sqrt(emitX * gammaX); L.sigYPrime = sqrt(emitY * gammaY);
+  const double distanceX = sqrt(fabs((LL.betaX - 1.0 / gammaX) / gammaX));
+  const double distanceY = sqrt(fabs((LL.betaY - 1.0 / gammaY) / gammaY));
+  const double vz = sqrt(gamma0 * gamma0 - 1.0) / gamma0;
+  L.delTX = distanceX / vz; L.delTY = distanceY / vz;
+  if (vz == 0.0) L.delTX = L.delTY = 0.0;
+  L.beamlets = LL.numBeamlet * n0;
+  L.remacro = (L.beamlets > 0) ? macro * (double)LL.numBeamlet / (double)L.beamlets * n0 : 0.0;
+  L.eNumbers = L.remacro * LL.numInBeamlet;
+  if (L.eNumbers < 10) L.eNumbers = 10;
+  return L;
+}
+
+}  // namespace
+
+extern "C" {
+
 // loadBeam.cpp:28-269 (3D).  Counts first (arrays NULL), then the particles.
 felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t seed, int64_t* counts, double* xo,
                                     double* yo, double* pxo, double* pyo, double* tho, double* gao, double* wo) {
@@ -749,39 +807,10 @@ felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t s
   for (int ii = 0; ii < c->rank; ++ii) q1.next(v1);  // randskip = myrank
   int64_t out_idx = 0;
   for (int sl = 0; sl < p.slice_n; ++sl) {
-    double n0 = 0.0, En0 = 0.0, ESn0 = 0.0;
-    const double posZ = (sl + p.min_i) * bucketZ + p.min_z;
-    if (LL.type == 1) {
-      for (size_t l = 0; l + 1 < LL.zpoint.size(); ++l)
-        if (posZ >= LL.zpoint[l] && posZ < LL.zpoint[l + 1])
-          n0 = (LL.zn[l + 1] - LL.zn[l]) / (LL.zpoint[l + 1] - LL.zpoint[l]) * (posZ - LL.zpoint[l]) + LL.zn[l];
-      for (size_t l = 0; l + 1 < LL.Epoint.size(); ++l)
-        if (posZ >= LL.Epoint[l] && posZ < LL.Epoint[l + 1])
-          En0 = (LL.En[l + 1] - LL.En[l]) / (LL.Epoint[l + 1] - LL.Epoint[l]) * (posZ - LL.Epoint[l]) + LL.En[l];
-      gamma0 = LL.energy * En0 / kMc2 + 1.0;
-      for (size_t l = 0; l + 1 < LL.ESpoint.size(); ++l)
-        if (posZ >= LL.ESpoint[l] && posZ < LL.ESpoint[l + 1])
-          ESn0 = (LL.ESn[l + 1] - LL.ESn[l]) / (LL.ESpoint[l + 1] - LL.ESpoint[l]) * (posZ - LL.ESpoint[l]) + LL.ESn[l];
-    } else if (LL.type == 2) {
-      const double phase = pow((posZ - LL.posZ) / LL.sigZ, LL.gaussPower);
-      n0 = exp(-phase);
-      gamma0 = (LL.energy + LL.Echirp * (posZ - LL.posZ)) / kMc2 + 1.0;
-    }
-    const double dGam = LL.spread * gamma0 * ESn0;
-    const double emitX = LL.emitX / gamma0, emitY = LL.emitY / gamma0;
-    const double gammaX = (1 + LL.alphaX * LL.alphaX) / LL.betaX;
-    const double gammaY = (1 + LL.alphaY * LL.alphaY) / LL.betaY;
-    const double sigX = sqrt(emitX / gammaX), sigY = sqrt(emitY / gammaY);
-    const double sigXPrime = sqrt(emitX * gammaX), sigYPrime = sqrt(emitY * gammaY);
-    const double distanceX = sqrt(fabs((LL.betaX - 1.0 / gammaX) / gammaX));
-    const double distanceY = sqrt(fabs((LL.betaY - 1.0 / gammaY) / gammaY));
-    const double vz = sqrt(gamma0 * gamma0 - 1.0) / gamma0;
-    double delTX = distanceX / vz, delTY = distanceY / vz;
-    if (vz == 0.0) delTX = delTY = 0.0;
-    const int beamlets = LL.numBeamlet * n0;
-    const double remacro = (beamlets > 0) ? macro * (double)LL.numBeamlet / (double)beamlets * n0 : 0.0;
-    double eNumbers = remacro * numInBeamlet;
-    if (eNumbers < 10) eNumbers = 10;
+    const SliceLoad L = slice_load(p, LL, sl, macro, gamma0);
+    const double dGam = L.dGam, sigX = L.sigX, sigY = L.sigY, sigXPrime = L.sigXPrime, sigYPrime = L.sigYPrime;
+    const double delTX = L.delTX, delTY = L.delTY, remacro = L.remacro, eNumbers = L.eNumbers, ESn0 = L.ESn0;
+    const int beamlets = L.beamlets;
     const int64_t total = (int64_t)beamlets * numInBeamlet;
     if (!fill) {
       counts[sl] = total;
@@ -834,6 +863,84 @@ felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t s
         tho[k] = theta + noise * noiseONOFF;
       }
     }
+  }
+  return FELIS_OK;
+}
+
+// felis_config_load_beam with the per-beamlet work on the device (k_load.cu):
+// the host computes the per-slice setup and draws the noise amplitudes from
+// the same random stream in the same order.
+felis_status felis_config_load_beam_device(felis_config* c, int32_t species, uint64_t seed, int64_t* counts,
+                                           double* xo, double* yo, double* pxo, double* pyo, double* tho,
+                                           double* gao, double* wo) {
+  if (!c || species < 0 || species >= (int)c->beams.size() || !counts) {
+    g_err = "felis_config_load_beam_device: bad argument";
+    return FELIS_BAD_ARG;
+  }
+  const felis_params& p = c->p;
+  if (p.dimension != 3) { g_err = "only the 3D loader is implemented"; return FELIS_UNSUPPORTED; }
+  const Beam& LL = c->beams[species];
+  const int maxH = p.harmony[p.num_harmony - 1];
+  const int numInBeamlet = LL.numInBeamlet;
+  double gamma0 = LL.energy / kMc2 + 1;
+  const double bucketZ = p.lambda0 * p.num_slice;
+  const int ptclCnt = numInBeamlet * LL.numBeamlet;
+  const double macro = LL.peakCurrent / kECharge / kVelocityC * bucketZ / (double)ptclCnt;
+  const bool fill = xo != nullptr;
+  if (fill && (!yo || !pxo || !pyo || !tho || !gao || !wo)) {
+    g_err = "felis_config_load_beam_device: null array";
+    return FELIS_BAD_ARG;
+  }
+  std::vector<felis::LoadSlice> ls(p.slice_n);
+  std::vector<double> eN(p.slice_n);
+  int64_t beamlets_total = 0;
+  for (int sl = 0; sl < p.slice_n; ++sl) {
+    const SliceLoad L = slice_load(p, LL, sl, macro, gamma0);
+    const int64_t total = (int64_t)L.beamlets * numInBeamlet;
+    if (!fill) {
+      counts[sl] = total;
+      continue;
+    }
+    if (counts[sl] != total) { g_err = "felis_config_load_beam_device: counts changed"; return FELIS_BAD_ARG; }
+    wo[sl] = L.remacro;
+    ls[sl] = felis::LoadSlice{gamma0, L.dGam, L.sigX, L.sigY, L.sigXPrime, L.sigYPrime, L.delTX, L.delTY, L.ESn0,
+                              beamlets_total, L.beamlets, 0};
+    eN[sl] = L.eNumbers;
+    beamlets_total += L.beamlets;
+  }
+  if (!fill) return FELIS_OK;
+  // the noise amplitudes in the host loader's draw order
+  GslRng ran(seed);
+  std::vector<double> noise((size_t)std::max<int64_t>(beamlets_total, 1) * 2 * maxH);
+  size_t q = 0;
+  for (int sl = 0; sl < p.slice_n; ++sl)
+    for (int b = 0; b < ls[sl].beamlets; ++b)
+      for (int m = 1; m <= maxH; ++m) {
+        const double sigma = sqrt(2.0 / eN[sl] / (1.0 * m * m));
+        noise[q++] = ran.gaussian(sigma);
+        noise[q++] = ran.gaussian(sigma);
+      }
+  felis::LoadSlice* d_ls = nullptr;
+  double* d_noise = nullptr;
+  cudaError_t e = cudaMalloc(&d_ls, ls.size() * sizeof(felis::LoadSlice));
+  if (e == cudaSuccess) e = cudaMalloc(&d_noise, noise.size() * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpy(d_ls, ls.data(), ls.size() * sizeof(felis::LoadSlice), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = cudaMemcpy(d_noise, noise.data(), noise.size() * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) {
+    felis::LoadArgs a{};
+    a.slices = d_ls; a.noise = d_noise; a.S = p.slice_n; a.maxH = maxH; a.num_in_beamlet = numInBeamlet;
+    a.trans_flat = LL.transFlat ? 1 : 0; a.noise_on = LL.noise ? 1.0 : 0.0;
+    a.dPhi = 2.0 * M_PI * p.num_slice; a.div = 2.0 * M_PI / (1.0 * numInBeamlet);
+    a.halton0 = (uint64_t)c->rank;  // randskip = myrank
+    a.x = xo; a.y = yo; a.px = pxo; a.py = pyo; a.theta = tho; a.gamma = gao;
+    e = felis::launch_load_beam(a, 0);
+  }
+  if (e == cudaSuccess) e = cudaDeviceSynchronize();
+  if (d_ls) cudaFree(d_ls);
+  if (d_noise) cudaFree(d_noise);
+  if (e != cudaSuccess) {
+    g_err = std::string("felis_config_load_beam_device: ") + cudaGetErrorString(e);
+    return FELIS_CUDA_ERROR;
   }
   return FELIS_OK;
 }

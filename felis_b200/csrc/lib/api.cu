@@ -848,8 +848,9 @@ felis_status felis_upload_particles(felis_handle* h, int32_t species, const doub
   const int64_t b = h->soff[(size_t)species * (S + 1)];
   const double* src[6] = {x, y, px, py, theta, gamma};
   double* dst[6] = {h->x, h->y, h->px, h->py, h->th, h->ga};
+  // host or device arrays (felis_config_load_beam_device writes device ones)
   for (int k = 0; k < 6; ++k)
-    if (cnt > 0) CK(cudaMemcpyAsync(dst[k] + b, src[k], cnt * sizeof(double), cudaMemcpyHostToDevice, h->st));
+    if (cnt > 0) CK(cudaMemcpyAsync(dst[k] + b, src[k], cnt * sizeof(double), cudaMemcpyDefault, h->st));
   for (int s = 0; s < S; ++s) h->weight[(size_t)species * S + s] = weights[s];
   if (!h->d_weight) CK(cudaMalloc(&h->d_weight, (size_t)ns * S * sizeof(double)));
   CK(cudaMemcpyAsync(h->d_weight, h->weight.data(), (size_t)ns * S * sizeof(double), cudaMemcpyHostToDevice, h->st));

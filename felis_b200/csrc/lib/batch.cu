@@ -783,13 +783,23 @@ felis_status felis_batch_upload_particles(felis_batch* b, int32_t inst, const do
   b->src_valid_it = -1;       // the next run deposits first
   const double* src[5] = {x, y, px, py, gamma};
   float* dst[5] = {I.x, I.y, I.px, I.py, I.dg};
-  std::vector<float> tmp(n);
-  for (int k = 0; k < 5; ++k) {
-    const double off = k == 4 ? I.p.gam_r : 0.0;  // gamma is stored as gamma - gamR
-    for (int64_t i = 0; i < n; ++i) tmp[i] = (float)(src[k][i] - off);
-    if (n) BCK(cudaMemcpy(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  // host arrays are rounded on the host, device arrays (the device beam
+  // loader's) on the device; gamma is stored as gamma - gamR
+  cudaPointerAttributes at{};
+  const bool on_device = n > 0 && cudaPointerGetAttributes(&at, x) == cudaSuccess && at.type == cudaMemoryTypeDevice;
+  if (on_device) {
+    for (int k = 0; k < 5; ++k) BCK(launch_f64_to_f32(src[k], dst[k], n, k == 4 ? I.p.gam_r : 0.0, b->st));
+    BCK(cudaMemcpyAsync(I.th, theta, n * sizeof(double), cudaMemcpyDeviceToDevice, b->st));
+    BCK(cudaStreamSynchronize(b->st));
+  } else {
+    std::vector<float> tmp(n);
+    for (int k = 0; k < 5; ++k) {
+      const double off = k == 4 ? I.p.gam_r : 0.0;
+      for (int64_t i = 0; i < n; ++i) tmp[i] = (float)(src[k][i] - off);
+      if (n) BCK(cudaMemcpy(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+    }
+    if (n) BCK(cudaMemcpy(I.th, theta, n * sizeof(double), cudaMemcpyHostToDevice));
   }
-  if (n) BCK(cudaMemcpy(I.th, theta, n * sizeof(double), cudaMemcpyHostToDevice));
   BCK(cudaMemcpy(I.soff, slice_offsets, (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
   std::vector<float> w(weights, weights + S);
   BCK(cudaMemcpy(I.weight, w.data(), S * sizeof(float), cudaMemcpyHostToDevice));

@@ -84,6 +84,8 @@ struct BatchLaunch {
 enum { BATCH_PUSH = 0, BATCH_DEPOSIT_ONLY = 1 };
 
 void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st);
+// dst[i] = (float)(src[i] - off) on the device (uploads of device arrays).
+cudaError_t launch_f64_to_f32(const double* src, float* dst, int64_t n, double off, cudaStream_t st);
 // H: the largest harmonic count of the ensemble (selects the kernel instance).
 void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st);
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);

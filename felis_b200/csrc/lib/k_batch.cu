@@ -1038,6 +1038,20 @@ int batch_resident_push(int H, int threads, int smem_bytes) {
   return n;
 }
 
+namespace {
+__global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__ dst, int64_t n, double off) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = (float)(src[i] - off);
+}
+}  // namespace
+
+cudaError_t launch_f64_to_f32(const double* src, float* dst, int64_t n, double off, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = (n + 255) / 256;
+  k_f64_to_f32<<<(int)(blocks < 4736 ? blocks : 4736), 256, 0, st>>>(src, dst, n, off);
+  return cudaGetLastError();
+}
+
 void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st) {
   if (a.nwork > 0) k_batch_adi<<<a.nwork, threads, a.smem_bytes, st>>>(a);
 }

@@ -45,11 +45,12 @@ def prepare(workload: str = "gaussian_taper", slices: int | None = None, length:
     d = tempfile.mkdtemp(prefix="felis_longrun_")
     path = workloads.write_input(os.path.join(d, f"{workload}.inp"), **kw)
     cfg = fb.Config(path)
-    beam = cfg.load_beam(0, seed=seed)
+    beam = cfg.load_beam_device(0, seed=seed)  # the per-beamlet work on the GPU
     if cfg.params.wake_on:
         # wakeField.cpp:9-50 from this beam's slice charge (makeDensity)
         cfg.wake(beam["weights"] * np.diff(beam["offsets"]))
-    fields = [cfg.load_seed(h) for h in range(cfg.params.num_harmony)]
+    # without a seed laser both engines start from their zeroed fields
+    fields = None if kw.get("seed_power", 1.0) == 0.0 else [cfg.load_seed(h) for h in range(cfg.params.num_harmony)]
     return cfg, beam, fields, kw
 
 
@@ -83,7 +84,7 @@ def run_fp64(cfg, beam, fields, steps: int, chunk: int) -> dict:
     try:
         h.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
                            beam["offsets"], beam["weights"])
-        for k, (ux, uy) in enumerate(fields):
+        for k, (ux, uy) in enumerate(fields or []):
             h.upload_field(k, 0, ux)
             h.upload_field(k, 1, uy)
         ms = 0.0
@@ -106,7 +107,7 @@ def run_mixed(cfg, beam, fields, steps: int, chunk: int, tune_steps: int = 4) ->
         b = fb.Batch([p])
         b.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
                            beam["offsets"], beam["weights"])
-        for k, (ux, uy) in enumerate(fields):
+        for k, (ux, uy) in enumerate(fields or []):
             b.upload_field(0, k, 0, ux)
             b.upload_field(0, k, 1, uy)
         return b
@@ -170,7 +171,7 @@ def main(argv=None):
     cfg, beam, fields, kw = prepare(a.workload, a.slices, a.length)
     p = cfg.params
     steps = a.steps if a.steps is not None else p.max_step
-    P = int(beam["offsets"][-1])
+    P = int(beam["offsets"][-1])  # (the beam's device arrays stay referenced until the runs are done)
     cells = p.slice_n * p.nx * p.ny * 2 * p.num_harmony
     harmonics = [p.harmony[i] for i in range(p.num_harmony)]
     dz = p.dz if p.dz > 0 else kw.get("lambda_u_cm", 2.6) * 0.01

@@ -204,7 +204,7 @@ WORKLOADS = {
 
 
 def ensemble(n: int = 96, seed: int = 20240601) -> list[dict]:
-    """The batched SASE ensemble: n instances with beam seeds 1..n, slice
+    """The batched SASE ensemble (shot noise, no seed laser): n instances with beam seeds 1..n, slice
     counts uniform in {128, 256, 512, 1024, 2048}, grid keys nx = ny from
     {65, 101, 151}, 1024 beamlets x 4 = 4096 particles per slice, peak current
     uniform in [2, 4] kA and relative energy spread uniform in [0.5, 2]e-4.
@@ -214,7 +214,7 @@ def ensemble(n: int = 96, seed: int = 20240601) -> list[dict]:
     rng = random.Random(seed)
     out = []
     for k in range(n):
-        out.append(dict(kind="sase", slices=rng.choice([128, 256, 512, 1024, 2048]), beamlets=1024,
+        out.append(dict(kind="sase", seed_power=0.0, slices=rng.choice([128, 256, 512, 1024, 2048]), beamlets=1024,
                         per_beamlet=4, nx=rng.choice([65, 101, 151]), current=rng.uniform(2000.0, 4000.0),
                         spread_pct=rng.uniform(0.5e-4, 2e-4) * 100.0, beam_seed=k + 1))
     return out

@@ -392,6 +392,17 @@ felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t s
                                     int64_t* counts, double* x, double* y,
                                     double* px, double* py, double* theta,
                                     double* gamma, double* weights);
+/* The same particles computed on the device (loadBeam.cpp:28-269): x .. gamma
+ * are device pointers (beamlet-major, the order of felis_config_load_beam),
+ * counts and weights host arrays; counts first when x is NULL.  The host
+ * keeps the per-slice setup and the sequential noise stream; one kernel
+ * computes the Halton points, the transverse and energy transforms and the
+ * mirrored phases.  Equal to felis_config_load_beam up to the last bits of
+ * log / sin / cos (the device's against the host C library's). */
+felis_status felis_config_load_beam_device(felis_config* c, int32_t species, uint64_t seed,
+                                           int64_t* counts, double* x, double* y,
+                                           double* px, double* py, double* theta,
+                                           double* gamma, double* weights);
 /* Initial seed field (loadSeed.cpp:25-80), reference layout, both pols. */
 felis_status felis_config_load_seed(felis_config* c, int32_t harmonic_index,
                                     double* ux, double* uy);
