@@ -24,7 +24,7 @@ _lib = C.CDLL(LIB_PATH)
 
 MAX_HARMONY = 8
 MAX_SPECIES = 8
-ABI_VERSION = 1
+ABI_VERSION = 2
 
 OK, BAD_ARG, CUDA_ERROR, THETA_OVERFLOW, OUT_OF_RANGE, NAN, TIMEOUT, UNSUPPORTED, NO_DEVICE, IO, NOT_FOUND = range(11)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA_ERROR", 3: "THETA_OVERFLOW", 4: "OUT_OF_RANGE", 5: "NAN",
@@ -70,6 +70,7 @@ class Params(C.Structure):
         ("abc_alpha", _dp), ("abc_alpha_p", _dp), ("abc_beta", _dp), ("abc_beta_p", _dp),
         ("bessel", _dp), ("wake_e", _dp),
         ("undulators", C.POINTER(Undulator)), ("quads", C.POINTER(Quad)),
+        ("beam_area", C.c_double * 8),
     ]
 
 

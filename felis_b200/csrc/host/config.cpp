@@ -158,6 +158,36 @@ struct Halton7 {
   }
 };
 
+// Three-dimensional Sobol points in Gray-code order (Antonov & Saleev 1979;
+// direction numbers of Bratley & Fox 1988, ACM TOMS 14:88): dimension 1 the
+// van der Corput sequence, dimension 2 the primitive polynomial x + 1 with
+// m1 = 1, dimension 3 x^2 + x + 1 with m1 = 1, m2 = 3; 30-bit integers, so
+// point n is its numerator times 2^-30.  The first point is (1/2, 1/2, 1/2).
+struct Sobol3 {
+  static constexpr int kBits = 30;
+  uint32_t v[kBits + 1][3] = {};
+  uint32_t x[3] = {0, 0, 0};
+  unsigned long count = 0;
+  Sobol3() {
+    uint32_t m[kBits + 1][3] = {};
+    for (int k = 1; k <= kBits; ++k) {
+      m[k][0] = 1;
+      m[k][1] = k == 1 ? 1 : (2 * m[k - 1][1]) ^ m[k - 1][1];
+      m[k][2] = k == 1 ? 1 : (k == 2 ? 3 : (2 * m[k - 1][2]) ^ (4 * m[k - 2][2]) ^ m[k - 2][2]);
+      for (int d = 0; d < 3; ++d) v[k][d] = m[k][d] << (kBits - k);
+    }
+  }
+  void next(double out[3]) {
+    int c = 1;  // 1-based position of the rightmost zero bit of count
+    for (unsigned long n = count; n & 1ul; n >>= 1) ++c;
+    for (int d = 0; d < 3; ++d) {
+      x[d] ^= v[c][d];
+      out[d] = (double)x[d] / (double)(1ul << kBits);
+    }
+    ++count;
+  }
+};
+
 struct GslRng {
   std::mt19937 mt;
   explicit GslRng(unsigned long seed) : mt((uint32_t)(seed == 0 ? 4357 : seed)) {}
@@ -570,6 +600,15 @@ felis_status load_config(felis_config* c) {
   p.num_species = (int)c->beams.size();
   if (p.num_species < 1 || p.num_species > FELIS_MAX_SPECIES) { g_err = "no [EBeam] block"; return FELIS_NOT_FOUND; }
   p.gamma0 = c->beams[0].gamma0;
+  // 1D model: each species' matched spot area (solveField.cpp:455-462)
+  for (int s = 0; s < p.num_species; ++s) {
+    const Beam& LL = c->beams[s];
+    const double emitX = LL.emitX / p.gamma0, emitY = LL.emitY / p.gamma0;
+    const double gammaX = (1 + LL.alphaX * LL.alphaX) / LL.betaX;
+    const double gammaY = (1 + LL.alphaY * LL.alphaY) / LL.betaY;
+    const double sigX = sqrt(emitX / gammaX), sigY = sqrt(emitY / gammaY);
+    p.beam_area[s] = 2.0 * M_PI * sigX * sigY;
+  }
   for (int rank = 1;; ++rank) {
     UndBlock UB;
     bool found;
@@ -776,6 +815,63 @@ SliceLoad slice_load(const felis_params& p, const Beam& LL, int sl, double macro
   return L;
 }
 
+// loadBeam.cpp:271-446 (1D): the same per-slice setup; per beamlet a Sobol
+// point (phase, energy by Box-Muller) and the noise amplitudes; no
+// transverse coordinates.  Counts first (arrays NULL), then the particles.
+felis_status load_beam_1d(felis_config* c, int species, uint64_t seed, int64_t* counts, double* xo, double* yo,
+                          double* pxo, double* pyo, double* tho, double* gao, double* wo) {
+  const felis_params& p = c->p;
+  const Beam& LL = c->beams[species];
+  const int maxH = p.harmony[p.num_harmony - 1];
+  const int numInBeamlet = LL.numInBeamlet;
+  double gamma0 = LL.energy / kMc2 + 1;
+  const double bucketZ = p.lambda0 * p.num_slice;
+  const int ptclCnt = numInBeamlet * LL.numBeamlet;
+  const double dPhi = 2.0 * M_PI * p.num_slice;
+  const double div = 2.0 * M_PI / (1.0 * numInBeamlet);
+  const double noiseONOFF = LL.noise ? 1.0 : 0.0;
+  const double macro = LL.peakCurrent / kECharge / kVelocityC * bucketZ / (double)ptclCnt;
+  const bool fill = xo != nullptr;
+  GslRng ran(seed);
+  Sobol3 q1;
+  double v1[3] = {0.0, 0.0, 0.0};
+  for (int ii = 0; ii < c->rank; ++ii) q1.next(v1);  // randskip = myrank
+  int64_t out_idx = 0;
+  for (int sl = 0; sl < p.slice_n; ++sl) {
+    const SliceLoad L = slice_load(p, LL, sl, macro, gamma0);
+    const int64_t total = (int64_t)L.beamlets * numInBeamlet;
+    if (!fill) {
+      counts[sl] = total;
+      continue;
+    }
+    if (counts[sl] != total) { g_err = "felis_config_load_beam: counts changed"; return FELIS_BAD_ARG; }
+    wo[sl] = L.remacro;
+    std::vector<double> an(maxH + 1, 0.0), bn(maxH + 1, 0.0);
+    for (int b = 0; b < L.beamlets; ++b) {
+      q1.next(v1);
+      const double th = v1[0];
+      double gam = (v1[1] == 0.0) ? 1e-10 : v1[1];
+      const double tmp = sqrt(-2.0 * log(gam)) * cos(v1[2] * 2.0 * M_PI);
+      gam = gamma0 + L.dGam * tmp;
+      const double theta0 = th * dPhi;
+      for (int m = 1; m <= maxH; ++m) {
+        const double sigma = sqrt(2.0 / L.eNumbers / (1.0 * m * m));
+        an[m] = ran.gaussian(sigma);
+        bn[m] = ran.gaussian(sigma);
+      }
+      for (int n = 0; n < numInBeamlet; ++n) {
+        const int64_t k = out_idx++;
+        xo[k] = 0.0; yo[k] = 0.0; pxo[k] = 0.0; pyo[k] = 0.0; gao[k] = gam;
+        const double theta = theta0 + n * div;
+        double noise = 0.0;
+        for (int m = 1; m <= maxH; ++m) noise += an[m] * cos(m * theta) + bn[m] * sin(m * theta);
+        tho[k] = theta + noise * noiseONOFF;
+      }
+    }
+  }
+  return FELIS_OK;
+}
+
 }  // namespace
 
 extern "C" {
@@ -788,7 +884,8 @@ felis_status felis_config_load_beam(felis_config* c, int32_t species, uint64_t s
     return FELIS_BAD_ARG;
   }
   const felis_params& p = c->p;
-  if (p.dimension != 3) { g_err = "only the 3D loader is implemented"; return FELIS_UNSUPPORTED; }
+  if (p.dimension == 1) return load_beam_1d(c, species, seed, counts, xo, yo, pxo, pyo, tho, gao, wo);
+  if (p.dimension != 3) { g_err = "dimension must be 1 or 3"; return FELIS_UNSUPPORTED; }
   const Beam& LL = c->beams[species];
   const int maxH = p.harmony[p.num_harmony - 1];
   const int numInBeamlet = LL.numInBeamlet;
@@ -878,7 +975,7 @@ felis_status felis_config_load_beam_device(felis_config* c, int32_t species, uin
     return FELIS_BAD_ARG;
   }
   const felis_params& p = c->p;
-  if (p.dimension != 3) { g_err = "only the 3D loader is implemented"; return FELIS_UNSUPPORTED; }
+  if (p.dimension != 3) { g_err = "the device loader is 3D only (felis_config_load_beam loads 1D beams)"; return FELIS_UNSUPPORTED; }
   const Beam& LL = c->beams[species];
   const int maxH = p.harmony[p.num_harmony - 1];
   const int numInBeamlet = LL.numInBeamlet;
@@ -950,13 +1047,28 @@ felis_status felis_config_load_beam_device(felis_config* c, int32_t species, uin
 felis_status felis_config_load_seed(felis_config* c, int32_t hidx, double* ux, double* uy) {
   if (!c || !ux || !uy) return FELIS_BAD_ARG;
   const felis_params& p = c->p;
-  if (p.dimension != 3) return FELIS_UNSUPPORTED;
+  if (p.dimension != 3 && p.dimension != 1) return FELIS_UNSUPPORTED;
   int h_pick = 0;
   for (int h = 0; h < p.num_harmony; ++h)
     if (p.harmony[h] == c->loadH) h_pick = h;
   const size_t N = (size_t)p.nx * p.ny, total = (size_t)(p.slice_n + 2) * N;
   for (size_t k = 0; k < 2 * total; ++k) { ux[k] = 0.0; uy[k] = 0.0; }
   if (hidx != h_pick) return FELIS_OK;
+  if (p.dimension == 1) {
+    // loadSeed.cpp:82-111: one amplitude per slice (z from minZ itself)
+    const double bucketZ1 = p.lambda0 * p.num_slice, sigmaZ1 = c->duration * kVelocityC;
+    const double invSigma21 = 1.0 / sigmaZ1 / sigmaZ1;
+    const double factor = sqrt(1.0 + c->polarity * c->polarity) * 0.5;
+    const std::complex<double> ph = std::exp(std::complex<double>(0.0, 1.0) * c->laserPsi);
+    for (int sl = 0; sl < p.slice_n; ++sl) {
+      const double z = (sl + p.min_i) * bucketZ1 + p.min_z;
+      const double amp = factor * c->a0 * exp(-0.25 * z * z * invSigma21);
+      const std::complex<double> vx = amp * (1.0 + c->laserAlpha * ph), vy = amp * (-1.0 + c->laserAlpha * ph);
+      ux[2 * (sl + 1)] = vx.real(); ux[2 * (sl + 1) + 1] = vx.imag();
+      uy[2 * (sl + 1)] = vy.real(); uy[2 * (sl + 1) + 1] = vy.imag();
+    }
+    return FELIS_OK;
+  }
   const double a0 = c->a0, dx = p.dx, dy = p.dy;
   const int nx = p.nx, ny = p.ny;
   const double bucketZ = p.lambda0 * p.num_slice;

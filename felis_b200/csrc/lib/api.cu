@@ -23,6 +23,7 @@
 #include <vector>
 
 #include "field.cuh"
+#include "oned.cuh"
 #include "particles.cuh"
 
 using namespace felis;
@@ -620,14 +621,21 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
   if (!p || !out) return FELIS_BAD_ARG;
   *out = nullptr;
   if (p->abi_version != FELIS_ABI_VERSION) return FELIS_BAD_ARG;
-  if (p->dimension != 3) return FELIS_UNSUPPORTED;
+  if (p->dimension != 3 && p->dimension != 1) return FELIS_UNSUPPORTED;
   if (p->precision != FELIS_FP64) return FELIS_UNSUPPORTED;
+  const bool one_d = p->dimension == 1;
   if (p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY || p->num_species < 1 ||
-      p->num_species > FELIS_MAX_SPECIES || p->slice_n < 1 || p->nx < 4 || p->ny < 4 || p->nr < 3 ||
-      p->scl_mode < 1 || p->scf_mode < 1 || p->scl_mode * p->scf_mode > 16 || p->scl_mode > 4 ||
-      p->bessel_rows < 2 || p->bessel_cols < 1 || !p->bessel || !p->abc_alpha || !p->abc_alpha_p ||
-      !p->abc_beta || !p->abc_beta_p || p->num_undulators < 0 || (p->num_undulators > 0 && !p->undulators))
+      p->num_species > FELIS_MAX_SPECIES || p->slice_n < 1 || p->scl_mode < 1 || p->scf_mode < 1 ||
+      p->scl_mode * p->scf_mode > 16 || p->scl_mode > 4 || p->bessel_rows < 2 || p->bessel_cols < 1 ||
+      !p->bessel || p->num_undulators < 0 || (p->num_undulators > 0 && !p->undulators))
     return FELIS_BAD_ARG;
+  if (one_d ? (p->nx != 1 || p->ny != 1 || p->nr != 1 || p->scf_mode != 1)
+            : (p->nx < 4 || p->ny < 4 || p->nr < 3 || !p->abc_alpha || !p->abc_alpha_p || !p->abc_beta ||
+               !p->abc_beta_p))
+    return FELIS_BAD_ARG;
+  if (one_d)
+    for (int s = 0; s < p->num_species; ++s)
+      if (!(p->beam_area[s] > 0.0)) return FELIS_BAD_ARG;
   int ndev = 0;
   if (cudaGetDeviceCount(&ndev) != cudaSuccess || ndev == 0) return FELIS_NO_DEVICE;
   felis_handle* h = new felis_handle();
@@ -715,8 +723,13 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
   if (ce != cudaSuccess) {
     bail(FELIS_CUDA_ERROR, cudaGetErrorString(ce));
   }
-  // ADI tables
-  if (st == FELIS_OK) {
+  // ADI tables (3D; the 1D field has no transverse operator)
+  if (st == FELIS_OK && one_d) {
+    if (cudaMemsetAsync(h->box, 0, (size_t)S * sizeof(int4), h->st) != cudaSuccess ||
+        cudaMemsetAsync(h->Sc, 0, (size_t)H * 2 * S * sizeof(double2), h->st) != cudaSuccess)
+      bail(FELIS_CUDA_ERROR, "1D buffers");
+  }
+  if (st == FELIS_OK && !one_d) {
     std::vector<cd> al(nx), alP(nx), be(ny), beP(ny);
     for (int i = 0; i < nx; ++i) { al[i] = C(p->abc_alpha[2 * i], p->abc_alpha[2 * i + 1]); alP[i] = C(p->abc_alpha_p[2 * i], p->abc_alpha_p[2 * i + 1]); }
     for (int j = 0; j < ny; ++j) { be[j] = C(p->abc_beta[2 * j], p->abc_beta[2 * j + 1]); beP[j] = C(p->abc_beta_p[2 * j], p->abc_beta_p[2 * j + 1]); }
@@ -994,9 +1007,74 @@ felis_status felis_bfactor(felis_handle* h, int32_t it, double* out) {
   return FELIS_OK;
 }
 
+// Scalars of one 1D call (solveField.cpp:428-470, particlePush.cpp:390-436),
+// formed on the host in the restatement's order.
+static bool oned_setup(const felis_handle* h, const felis_lattice& L, OneDLaunch* a) {
+  *a = OneDLaunch{};
+  a->G = h->G;
+  a->ns = h->p.num_species;
+  a->ring_base = h->ring_base;
+  a->soff = h->d_soff; a->weight = h->d_weight; a->th = h->th; a->ga = h->ga;
+  a->U = h->U; a->Sc = h->Sc; a->Ez = h->Ez; a->err = h->d_err;
+  if (!polarisation(L, &a->Phi, &a->etaX, &a->etaY)) return false;
+  const double K0 = L.K0, ue = L.ue, ks = h->p.ks, dz = h->p.dz;
+  const double bucket = h->p.lambda0 * h->p.num_slice;
+  a->K0 = K0; a->ue = ue; a->ku = L.ku; a->dz = dz;
+  a->K2 = 1.0 + K0 * K0 * 0.5 * (1.0 + ue * ue);
+  a->dPhi = 2.0 * M_PI * h->p.num_slice;
+  a->e_mc2 = K_ECHARGE / K_EMASS / K_VELOCITYC / K_VELOCITYC;
+  a->sq = sqrt(ue * ue + 1.0);
+  for (int sp = 0; sp < h->p.num_species; ++sp) {
+    const double area = h->p.beam_area[sp];
+    a->coefU[sp] = dz * K_ECHARGE * K_ECHARGE * K_MU0 * K0 * sqrt(1.0 + ue * ue) / (2.0 * ks * K_EMASS * bucket * area);
+    a->coefE[sp] = K_ECHARGE * K_VELOCITYC * K_VELOCITYC * K_MU0 / ks / area / bucket;
+  }
+  const double xi = 0.25 * K0 * K0 * (1.0 - ue * ue) / (1.0 + (1.0 + ue * ue) * K0 * K0 * 0.5);
+  const double K0a = L.K0_alpha;
+  const double* B = h->p.bessel;
+  const int bc = h->p.bessel_cols, rows = h->p.bessel_rows;
+  for (int hh = 0; hh < h->p.num_harmony; ++hh) {
+    const int H = h->p.harmony[hh];
+    a->fsrc[hh][0] = a->fsrc[hh][1] = a->fpush[hh][0] = a->fpush[hh][1] = C(0.0, 0.0);
+    if (H % 2 != 1) continue;
+    const double sign = ((H - 1) / 2 % 2 == 0) ? 1.0 : -1.0;
+    const int idx = (int)(H * xi / h->p.d_bessel);
+    if (idx < 0 || idx + 1 >= rows) return false;
+    double w[2];
+    w[1] = (H * xi / h->p.d_bessel) - idx;
+    w[0] = 1.0 - w[1];
+    int order = (H - 1) / 2;
+    const double J1 = B[(size_t)idx * bc + order] * w[0] + B[(size_t)(idx + 1) * bc + order] * w[1];
+    order = (H + 1) / 2;
+    const double J2 = B[(size_t)idx * bc + order] * w[0] + B[(size_t)(idx + 1) * bc + order] * w[1];
+    a->fsrc[hh][0] = C(sign * (J1 - K0a * J2), 0.0);
+    a->fsrc[hh][1] = C(sign * (J1 + K0a * J2), 0.0);
+    a->fpush[hh][0] = C(sign * (K0a * J1 - J2), 0.0);
+    a->fpush[hh][1] = C(sign * (K0a * J1 + J2), 0.0);
+  }
+  return true;
+}
+
+static felis_status run_1d_field(felis_handle* h) {
+  OneDLaunch a;
+  if (!oned_setup(h, h->lat, &a)) return fail(h, FELIS_BAD_ARG, "invalid K0_alpha or Bessel range (1D)");
+  KernelScope ks(h, FELIS_KERNEL_ADI);
+  CK(launch_1d_field(a, h->lat.current_flag, h->st));
+  return FELIS_OK;
+}
+
+static felis_status run_1d_push(felis_handle* h, const felis_lattice& L) {
+  OneDLaunch a;
+  if (!oned_setup(h, L, &a)) return fail(h, FELIS_BAD_ARG, "invalid K0_alpha or Bessel range (1D)");
+  KernelScope ks(h, FELIS_KERNEL_PARTICLES);
+  CK(launch_1d_push(a, h->st));
+  return FELIS_OK;
+}
+
 static felis_status solve_field_impl(felis_handle* h) {
   felis_status s = ensure_ready(h);
   if (s != FELIS_OK) return s;
+  if (h->p.dimension == 1) return run_1d_field(h);
   if (h->lat.current_flag) {
     if (!h->prep_valid) {
       s = run_particles(h, OP_PREP, nullptr, &h->lat);
@@ -1022,6 +1100,7 @@ felis_status felis_transverse_push(felis_handle* h, int32_t it) {
   (void)it;
   felis_status s = ensure_ready(h);
   if (s != FELIS_OK) return s;
+  if (h->p.dimension == 1) return FELIS_OK;  // main.cpp:133-140: 3D only
   s = run_particles(h, OP_T0, &h->lat, nullptr);
   if (s != FELIS_OK) return s;
   invalidate_particles(h);
@@ -1033,7 +1112,7 @@ felis_status felis_push_theta_gamma(felis_handle* h, int32_t it) {
   (void)it;
   felis_status s = ensure_ready(h);
   if (s != FELIS_OK) return s;
-  s = run_particles(h, OP_PUSH, nullptr, &h->lat);
+  s = h->p.dimension == 1 ? run_1d_push(h, h->lat) : run_particles(h, OP_PUSH, nullptr, &h->lat);
   if (s != FELIS_OK) return s;
   invalidate_particles(h);
   return check_err(h);
@@ -1044,6 +1123,7 @@ felis_status felis_drift_theta_gamma(felis_handle* h, int32_t it) {
   (void)it;
   felis_status s = ensure_ready(h);
   if (s != FELIS_OK) return s;
+  if (h->p.dimension == 1) return FELIS_OK;  // nx = 1: no particle passes particlePush.cpp:160
   s = run_particles(h, OP_DRIFT, nullptr, &h->lat);
   if (s != FELIS_OK) return s;
   invalidate_particles(h);
@@ -1071,8 +1151,43 @@ felis_status felis_shift_field(felis_handle* h, int32_t it) {
   return FELIS_OK;
 }
 
+// One iteration of the 1D model (main.cpp:117-155 without the transverse
+// pushes): diagnostics, field, push, wrap, shift.
+static felis_status step_impl_1d(felis_handle* h, int it) {
+  const int H = h->p.num_harmony, ns = h->p.num_species;
+  if (it >= 0 && it < h->hist_n) {
+    {
+      KernelScope ks(h, FELIS_KERNEL_REDUCE);
+      launch_energy(h->G, h->U, h->ring_base, h->d_planes2, h->st);
+      launch_sum_planes(h->d_planes2, H, h->p.slice_n, 0, h->d_hist_e + (size_t)it * 2 * H, h->st);
+      h->launches[FELIS_KERNEL_REDUCE] += 1;
+    }
+    felis_status s = diag_now(h, h->d_hist_t + (size_t)it * 6 * ns, h->d_hist_b + (size_t)it * 2 * H);
+    if (s != FELIS_OK) return s;
+  }
+  felis_status s = run_1d_field(h);
+  if (s != FELIS_OK) return s;
+  update_lattice(h, it, 0);
+  update_lattice(h, it, 0.5);
+  const felis_lattice l1 = h->lat;
+  if (!l1.drift_flag) {
+    s = run_1d_push(h, l1);
+    if (s != FELIS_OK) return s;
+  }
+  s = run_particles(h, OP_WRAP, nullptr, nullptr);
+  if (s != FELIS_OK) return s;
+  h->prep_valid = false;
+  if (!l1.drift_flag && h->p.mode == FELIS_TIME_DEPENDENT) {
+    s = do_shift(h);
+    if (s != FELIS_OK) return s;
+  }
+  h->diag_valid = false;
+  return FELIS_OK;
+}
+
 // One iteration of main.cpp:117-155 with the fused particle kernel.
 static felis_status step_impl(felis_handle* h, int it) {
+  if (h->p.dimension == 1) return step_impl_1d(h, it);
   const int H = h->p.num_harmony, ns = h->p.num_species;
   const bool rec = it >= 0 && it < h->hist_n;
   // diagnostics of this iteration (state before the step)

@@ -44,14 +44,15 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
                noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
                linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
                in_air: bool = True, k_list=None, sigma_slices: float | None = None, profile_nodes: int = 65,
-               K_und: float | None = None) -> str:
+               K_und: float | None = None, dimension: int = 3) -> str:
     """Input text of one workload.  `sigma_slices` switches the flat-top
     current to a Gaussian of that rms length (in slices) centred on the bunch,
     written as a `profile_nodes`-node Polygon so that the energy-spread nodes
     still apply (loadBeam.cpp's Gaussian load type has no spread).  `K0` sets
     the photon energy by the planar resonance; `K_und` (default K0) is the
     undulator's K, e.g. K0 / sqrt(1 + polarity^2) for an elliptical undulator
-    on the same resonance (parameterSetting.cpp's default K0)."""
+    on the same resonance (parameterSetting.cpp's default K0).  `dimension` 1
+    selects the 1D model (the grid collapses to one cell per slice)."""
     static = kind == "static"
     if noise is None:
         noise = not static
@@ -99,7 +100,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  save_start=1000000
 
 [Domain]
- dimension=3
+ dimension={dimension}
  mode={'Static' if static else 'Time_Dependent'}
  minZ={minZ!r}
  maxZ={maxZ!r}

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FELIS_ABI_VERSION 1
+#define FELIS_ABI_VERSION 2
 #define FELIS_MAX_HARMONY 8
 #define FELIS_MAX_SPECIES 8
 
@@ -91,7 +91,7 @@ typedef struct felis_quad {
 typedef struct felis_params {
   int32_t abi_version; /* FELIS_ABI_VERSION */
   int32_t precision;   /* felis_precision */
-  int32_t dimension;   /* 3 (the 1D model is not implemented on the GPU) */
+  int32_t dimension;   /* 3, or 1 for the 1D model (FP64 handle) */
   int32_t mode;        /* felis_mode */
   int32_t num_harmony;
   int32_t harmony[FELIS_MAX_HARMONY];
@@ -125,6 +125,9 @@ typedef struct felis_params {
   const double* wake_e;
   const felis_undulator* undulators;
   const felis_quad* quads;
+  /* 1D model: the area 2 pi sigX sigY of each species' matched beam, which
+   * normalises its source and space-charge field (solveField.cpp:455-470) */
+  double beam_area[FELIS_MAX_SPECIES];
 } felis_params;
 
 /* Lattice state that updateK_quadG() leaves in Domain (updateK_quadG.cpp:8-94). */

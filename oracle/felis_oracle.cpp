@@ -19,6 +19,8 @@
 //   transversePush        particlePush.cpp:32-117
 //   drift_theta_gamma     particlePush.cpp:119-195
 //   push_theta_gamma_3D   particlePush.cpp:198-386
+//   push_theta_gamma_1D   particlePush.cpp:388-524
+//   solve_Sc_1D, solve_Field_U_1D  solveField.cpp:409-549
 //   solveField            solveField.cpp:49-78
 //   solve_Field_U_3D      solveField.cpp:80-185
 //   solve_Sc_3D           solveField.cpp:187-403
@@ -161,7 +163,8 @@ void pfor(int64_t n0, int64_t n1, int threads, Fn&& fn) {
 
 struct orc {
   // Domain scalars
-  int mode, numHarmony, sliceN, subSliceN, minI, nx, ny, N, numSlice, nSpecies;
+  int dimension, mode, numHarmony, sliceN, subSliceN, minI, nx, ny, N, numSlice, nSpecies;
+  double area[FELIS_MAX_SPECIES];  // 1D: 2 pi sigX sigY per species
   int L, F, nr, bn, bcols, abcN, wakeON, maxStep;
   double ks, lambda0, dz, dx, dy, dr, minX, minY, minZ, maxZ, gamma0, gamR, dBessel, abcSig;
   std::vector<int> harmony;
@@ -183,6 +186,8 @@ struct orc {
   char msg[256];
   double BJ(int row, int col) const { return bessel[(size_t)row * bcols + col]; }
 };
+
+static void push_theta_gamma_1d(orc* D);
 
 static void set_err(orc* D, int code, const char* m) {
   if (D->err == 0) {
@@ -291,6 +296,7 @@ static void update_lattice(orc* D, int iteration, double half) {
 
 // particlePush.cpp:32-117
 static void transverse_push(orc* D) {
+  if (D->dimension == 1) return;  // main.cpp:133-140 pushes transversely in 3D only
   const double dz = D->dz * 0.5;
   const double ku = D->ku, K0 = D->K0, ue = D->ue;
   const double aa = D->K0 * D->K0 * 0.25 * ue * D->ku;
@@ -360,6 +366,7 @@ static bool polarisation(orc* D, double* Phi, cd* etaX, cd* etaY) {
 
 // particlePush.cpp:119-195
 static void drift_theta_gamma(orc* D) {
+  if (D->dimension == 1) return;  // nx = 1: no particle passes the grid test of particlePush.cpp:160
   const int nx = D->nx, ny = D->ny, N = D->N;
   const double dz = D->dz, ks = D->ks, ku = D->ku, gamR = D->gamR;
   const double dx = D->dx, dy = D->dy, minX = D->minX, minY = D->minY;
@@ -409,6 +416,7 @@ static void drift_theta_gamma(orc* D) {
 
 // particlePush.cpp:198-386
 static void push_theta_gamma(orc* D) {
+  if (D->dimension == 1) { push_theta_gamma_1d(D); return; }  // particlePush.cpp:15-29
   const int nx = D->nx, ny = D->ny, nr = D->nr, N = D->N, L = D->L, F = D->F;
   const double dz = D->dz, dx = D->dx, dy = D->dy, dr = D->dr;
   const double ku = D->ku, ks = D->ks, K0 = D->K0, dBessel = D->dBessel;
@@ -824,6 +832,155 @@ static void solve_Sc(orc* D) {
   }
 }
 
+// solveField.cpp:422-549 (1D): per slice, the source of every harmonic and
+// the longitudinal space-charge modes, summed over the slice's particles in
+// order (species by species).
+static void solve_sc_1d(orc* D) {
+  const int H_n = D->numHarmony, L = D->L;
+  double Phi;
+  cd etaX, etaY;
+  if (!polarisation(D, &Phi, &etaX, &etaY)) return;
+  const double K0_alpha = D->K0_alpha;
+  const int endI = D->subSliceN + 1;
+  const double dz = D->dz, ks = D->ks, K0 = D->K0, dBessel = D->dBessel, ue = D->ue;
+  const double xi = 0.25 * K0 * K0 * (1.0 - ue * ue) / (1.0 + (1.0 + ue * ue) * K0 * K0 * 0.5);
+  for (int s = 0; s < D->nSpecies; ++s) {
+    Species& P = D->sp[s];
+    const double area = D->area[s];
+    const double coef = dz * kECharge * kECharge * kMu0 * K0 * sqrt(1.0 + ue * ue) /
+                        (2.0 * ks * kEMass * (D->lambda0 * D->numSlice) * area);
+    pfor(0, D->subSliceN, D->threads, [&](int64_t lo_, int64_t hi_) {
+    for (int sl = (int)lo_; sl < (int)hi_; ++sl) {
+      const int sliceI = sl + 1;
+      const double macro = P.weight[sl];
+      for (int64_t n = P.off[sl]; n < P.off[sl + 1]; ++n) {
+        const double th = P.theta[n], gam = P.gamma[n];
+        for (int h = 0; h < H_n; ++h) {
+          const int H = D->harmony[h];
+          cd fx = C(0, 0), fy = C(0, 0);
+          if (H % 2 == 1) {
+            const double sign = ((H - 1) / 2 % 2 == 0) ? 1.0 : -1.0;
+            const int idx = (int)(H * xi / dBessel);
+            double w[2];
+            w[1] = (H * xi / dBessel) - idx; w[0] = 1.0 - w[1];
+            int order = (H - 1) / 2;
+            const double J1 = D->BJ(idx, order) * w[0] + D->BJ(idx + 1, order) * w[1];
+            order = (H + 1) / 2;
+            const double J2 = D->BJ(idx, order) * w[0] + D->BJ(idx + 1, order) * w[1];
+            fx = C(sign * (J1 - K0_alpha * J2), 0.0);
+            fy = C(sign * (J1 + K0_alpha * J2), 0.0);
+          }
+          // macro*coef*exp((-1.0*H)*I*(th+Phi*0.5))/gam
+          const cd m = cdivr(cscale(cexpi((-1.0 * H) * (th + Phi * 0.5)), macro * coef), gam);
+          D->ScUx[h][sliceI] = csub(D->ScUx[h][sliceI], cmul(cmul(etaX, fx), m));
+          D->ScUy[h][sliceI] = csub(D->ScUy[h][sliceI], cmul(cmul(etaY, fy), m));
+        }
+      }
+    }
+    });
+  }
+  for (int l = 0; l < L; ++l)
+    for (int sliceI = 0; sliceI <= endI; ++sliceI) D->Ez[l][sliceI] = C(0, 0);
+  for (int s = 0; s < D->nSpecies; ++s) {
+    Species& P = D->sp[s];
+    const double area = D->area[s];
+    const double coef = kECharge * kVelocityC * kVelocityC * kMu0 / ks / area / (D->lambda0 * D->numSlice);
+    pfor(0, D->subSliceN, D->threads, [&](int64_t lo_, int64_t hi_) {
+    for (int sl = (int)lo_; sl < (int)hi_; ++sl) {
+      const int sliceI = sl + 1;
+      const double macro = P.weight[sl];
+      for (int64_t n = P.off[sl]; n < P.off[sl + 1]; ++n) {
+        const double th = P.theta[n];
+        for (int l = 0; l < L; ++l) {
+          // -1.0*I*coef/(1.0+l)*macro*exp(-I*(l+1.0)*th), left to right
+          cd t = C(-0.0, -1.0);
+          t = cscale(t, coef);
+          t = cdivr(t, 1.0 + l);
+          t = cscale(t, macro);
+          t = cmul(t, cexpi(-((l + 1.0) * th)));
+          D->Ez[l][sliceI] = cadd(D->Ez[l][sliceI], t);
+        }
+      }
+    }
+    });
+  }
+}
+
+// particlePush.cpp:388-524 (1D): RK4 of (theta, gamma) in the slice's field
+// value and space-charge modes, with the constant xi of the 1D model.
+static void push_theta_gamma_1d(orc* D) {
+  const int L = D->L, H_n = D->numHarmony;
+  const double ue = D->ue, ks = D->ks, ku = D->ku, K0 = D->K0, dz = D->dz, dBessel = D->dBessel;
+  const double dPhi = 2.0 * M_PI * D->numSlice;
+  const double e_mc2 = kECharge / kEMass / kVelocityC / kVelocityC;
+  double Phi;
+  cd etaX, etaY;
+  if (!polarisation(D, &Phi, &etaX, &etaY)) return;
+  const double K0_alpha = D->K0_alpha;
+  const double K2 = 1.0 + K0 * K0 * 0.5 * (1.0 + ue * ue);
+  const double coefList[5] = {0, 0, 0.5, 0.5, 1};
+  const double xi = 0.25 * K0 * K0 * (1.0 - ue * ue) / (1.0 + (1.0 + ue * ue) * K0 * K0 * 0.5);
+  for (int s = 0; s < D->nSpecies; ++s) {
+    Species& P = D->sp[s];
+    for (int sl = 0; sl < D->subSliceN; ++sl) {
+      const int sliceI = sl + 1;
+      const double wakeE = D->wakeON ? D->wakeE[sliceI - 1 + D->minI] / (kMc2 * 1.0e6) : 0.0;
+      cd Em[4], Ux[FELIS_MAX_HARMONY], Uy[FELIS_MAX_HARMONY];
+      for (int ll = 0; ll < L; ++ll) Em[ll] = D->Ez[ll][sliceI];
+      for (int h = 0; h < H_n; ++h) { Ux[h] = D->Ux[h][sliceI]; Uy[h] = D->Uy[h][sliceI]; }
+      double sumU2 = 0.0;
+      for (int h = 0; h < H_n; ++h) {
+        const int H = D->harmony[h];
+        sumU2 += (cnorm(Ux[h]) + cnorm(Uy[h])) / (2.0 * H * H);
+      }
+      std::atomic<int> overflow{0};
+      pfor(P.off[sl], P.off[sl + 1], D->threads, [&](int64_t lo_, int64_t hi_) {
+      for (int64_t n = lo_; n < hi_; ++n) {
+        const double th0 = P.theta[n], gam0 = P.gamma[n];
+        double k_th[5] = {0, 0, 0, 0, 0}, k_gam[5] = {0, 0, 0, 0, 0};
+        for (int m = 1; m < 5; ++m) {
+          const double th = th0 + dz * k_th[m - 1] * coefList[m];
+          const double gam = gam0 + dz * k_gam[m - 1] * coefList[m];
+          double sumTh = 0.0, sumG = 0.0, sumEzPart = 0.0;
+          for (int ll = 0; ll < L; ++ll) {
+            const cd e = cexpi((ll + 1.0) * th);
+            sumEzPart += 2.0 * (Em[ll].re * e.re - Em[ll].im * e.im);
+          }
+          for (int h = 0; h < H_n; ++h) {
+            const int H = D->harmony[h];
+            const double sign = ((H - 1) / 2 % 2 == 0) ? 1.0 : -1.0;
+            const int idx = (1.0 * H * xi) / dBessel;
+            double w[2];
+            w[1] = (H * xi / dBessel) - idx; w[0] = 1.0 - w[1];
+            cd fx = C(0, 0), fy = C(0, 0);
+            if (H % 2 == 1) {
+              int order = (H - 1) * 0.5;
+              const double J1 = D->BJ(idx, order) * w[0] + D->BJ(idx + 1, order) * w[1];
+              order = (H + 1) * 0.5;
+              const double J2 = D->BJ(idx, order) * w[0] + D->BJ(idx + 1, order) * w[1];
+              fx = C(sign * (K0_alpha * J1 - J2), 0.0);
+              fy = C(sign * (K0_alpha * J1 + J2), 0.0);
+            }
+            const cd e = cexpi((1.0 * H) * (th + Phi * 0.5));
+            const cd tmpComp = cmul(e, csub(cmul(cmul(etaX, fx), Ux[h]), cmul(cmul(etaY, fy), Uy[h])));
+            sumTh += (0.0 * tmpComp.re - 1.0 * tmpComp.im) / (1.0 * H);
+            sumG += tmpComp.re / (2.0 * gam);
+          }
+          k_th[m] = ku - ks / (2.0 * gam * gam) * (K2 + sumU2 + K0 * sqrt(ue * ue + 1.0) * sumTh);
+          k_gam[m] = ks * K0 * sqrt(ue * ue + 1.0) * sumG + e_mc2 * sumEzPart;
+        }
+        const double tmpTh = dz / 6.0 * (k_th[1] + 2.0 * k_th[2] + 2.0 * k_th[3] + k_th[4]);
+        if (tmpTh > dPhi || tmpTh <= -dPhi) overflow = 1;
+        P.theta[n] += tmpTh;
+        const double tmpGam = dz / 6.0 * (k_gam[1] + 2 * k_gam[2] + 2 * k_gam[3] + k_gam[4]) - dz * wakeE;
+        P.gamma[n] += tmpGam;
+      }
+      });
+      if (overflow) set_err(D, FELIS_THETA_OVERFLOW, "push_theta_gamma: |dtheta| > 2 pi numSlice");
+    }
+  }
+}
+
 // solveField.cpp:49-78
 static void solve_field(orc* D) {
   for (int h = 0; h < D->numHarmony; ++h)
@@ -831,6 +988,16 @@ static void solve_field(orc* D) {
       D->ScUx[h][sliceI] = C(0, 0);
       D->ScUy[h][sliceI] = C(0, 0);
     }
+  if (D->dimension == 1) {
+    // solveField.cpp:61-66, 409-416: U += ScU per slice
+    if (D->currentFlag) solve_sc_1d(D);
+    for (int h = 0; h < D->numHarmony; ++h)
+      for (int sliceI = 1; sliceI < D->subSliceN + 1; ++sliceI) {
+        D->Ux[h][sliceI] = cadd(D->Ux[h][sliceI], D->ScUx[h][sliceI]);
+        D->Uy[h][sliceI] = cadd(D->Uy[h][sliceI], D->ScUy[h][sliceI]);
+      }
+    return;
+  }
   if (D->currentFlag) solve_Sc(D);
   solve_field_U(D, D->Ux, D->ScUx);
   solve_field_U(D, D->Uy, D->ScUy);
@@ -975,11 +1142,14 @@ static void diagnostic_sums(orc* D, double* out) {
 extern "C" {
 
 orc* orc_create(const felis_params* p, int threads) {
-  if (!p || p->dimension != 3 || p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY) return nullptr;
+  if (!p || (p->dimension != 3 && p->dimension != 1) || p->num_harmony < 1 || p->num_harmony > FELIS_MAX_HARMONY)
+    return nullptr;
   orc* D = new orc();
   D->err = 0;
   D->msg[0] = 0;
   D->threads = threads > 0 ? threads : 1;
+  D->dimension = p->dimension;
+  for (int k = 0; k < FELIS_MAX_SPECIES; ++k) D->area[k] = p->beam_area[k];
   D->mode = p->mode;
   D->numHarmony = p->num_harmony;
   D->harmony.assign(p->harmony, p->harmony + p->num_harmony);
@@ -1024,7 +1194,7 @@ orc* orc_create(const felis_params* p, int threads) {
     o.g.assign(Q.g, Q.g + Q.numbers);
     D->quad.push_back(o);
   }
-  build_abc(D);
+  if (D->dimension == 3) build_abc(D);
   D->bessel.assign(p->bessel, p->bessel + (size_t)p->bessel_rows * p->bessel_cols);
   if (p->wake_e) D->wakeE.assign(p->wake_e, p->wake_e + p->global_slice_n);
   else D->wakeE.assign(p->global_slice_n, 0.0);

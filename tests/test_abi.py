@@ -40,8 +40,10 @@ def test_bad_arguments_return_status(fb):
     h = ctypes.c_void_p()
     assert lib.felis_create(ctypes.byref(p), ctypes.byref(h)) == fb.BAD_ARG
     p.abi_version = fb.ABI_VERSION
-    p.dimension = 1
+    p.dimension = 2  # the reference has 1D and 3D models only
     assert lib.felis_create(ctypes.byref(p), ctypes.byref(h)) == fb.UNSUPPORTED
+    p.dimension = 1  # 1D with an empty parameter set: rejected, not run
+    assert lib.felis_create(ctypes.byref(p), ctypes.byref(h)) == fb.BAD_ARG
     assert lib.felis_sort_by_slice(None, -1, None) == fb.BAD_ARG
 
 

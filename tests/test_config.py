@@ -147,3 +147,56 @@ def test_wake_circular_ac(fb, tmp_path):
     assert w.shape == (64,) and np.all(np.isfinite(w))
     # causal convolution: the head slice sees its own wake only
     assert abs(w[-1]) <= abs(w).max()
+
+
+def _sobol_direct(n, dims=3, bits=30):
+    """Point n (1-based) of the Gray-code Sobol sequence computed directly:
+    XOR of the direction numbers at the set bits of gray(n) = n ^ (n >> 1)
+    (Antonov-Saleev), direction numbers of Bratley-Fox for the polynomials
+    1, x + 1, x^2 + x + 1 (initial m 1; 1; 1, 3)."""
+    m = [[1] * (bits + 1) for _ in range(dims)]
+    for k in range(2, bits + 1):
+        m[1][k] = (2 * m[1][k - 1]) ^ m[1][k - 1]
+    m[2][2] = 3
+    for k in range(3, bits + 1):
+        m[2][k] = (2 * m[2][k - 1]) ^ (4 * m[2][k - 2]) ^ m[2][k - 2]
+    g = n ^ (n >> 1)
+    out = []
+    for d in range(dims):
+        x = 0
+        for k in range(1, bits + 1):
+            if (g >> (k - 1)) & 1:
+                x ^= m[d][k] << (bits - k)
+        out.append(x / 2.0 ** bits)
+    return out
+
+
+def test_1d_loader(fb, tmp_path):
+    """loadBeam.cpp:271-446: particles without transverse coordinates, the
+    phase of each beamlet's first particle and its energy from consecutive
+    Sobol points (noise off)."""
+    from felis_b200 import workloads
+
+    path = workloads.write_input(str(tmp_path / "d1.inp"), kind="sase", slices=6, beamlets=16, per_beamlet=4,
+                                 dimension=1, noise=False, spread_pct=0.01)
+    cfg = fb.Config(path)
+    p = cfg.params
+    b = cfg.load_beam(0, seed=3)
+    n = int(b["offsets"][-1])
+    assert n == 6 * 16 * 4
+    for k in ("x", "y", "px", "py"):
+        assert not np.any(b[k])
+    dPhi = 2 * math.pi * p.num_slice
+    div = 2 * math.pi / 4
+    gamma0 = p.gamma0
+    dGam = 1e-4 * gamma0  # spread 0.01 % with the flat energy-spread profile
+    for beamlet in range(24):
+        v = _sobol_direct(beamlet + 1)
+        th0 = v[0] * dPhi
+        for q in range(4):
+            assert b["theta"][beamlet * 4 + q] == th0 + q * div
+        expect = gamma0 + dGam * math.sqrt(-2.0 * math.log(v[1])) * math.cos(v[2] * 2.0 * math.pi)
+        assert abs(b["gamma"][beamlet * 4] - expect) <= 1e-12 * gamma0
+    # 1D seed: one value per slice; the 1D Domain has nx = ny = 1
+    ux, uy = cfg.load_seed(0)
+    assert ux.shape == (p.slice_n + 2, 1, 1) and np.all(ux[1:-1] != 0) and not np.any(ux[[0, -1]])
