@@ -13,6 +13,8 @@
 #include <string.h>
 
 #include <algorithm>
+#include <cmath>
+#include <initializer_list>
 #include <complex>
 #include <map>
 #include <string>
@@ -58,6 +60,7 @@ struct Inst {
   int nsrc = 0;
   int src_plane[FELIS_MAX_HARMONY] = {0};
   int cx[5] = {0}, cy[5] = {0};  // ADI chunks of the interior columns / rows
+  int adi_k[FELIS_MAX_HARMONY][8] = {};  // constant ranges and product lengths (adi_ranges)
   double* part_e = nullptr;
   double* part_b = nullptr;
   int* err = nullptr;
@@ -265,6 +268,56 @@ void adi_tables(const felis_params& p, int hidx, int M, const int cx[5], const i
   }
 }
 
+// Where the ADI kernel may use constants instead of table reads, and where
+// it may skip the chunk products: out = {kx0, kx1, ky0, ky1, gx, qx, gy, qy}
+// for the 16 tables t of one harmonic (layout of adi_tables).  [kx0, kx1) is
+// the widest range of interior columns around the middle where the
+// column-indexed tables (0-2: x sweep, 13-15: right-hand side of the y sweep)
+// hold the same values bit for bit (they vary inside the absorbing layers,
+// and the Thomas coefficients settle within a few cells of them); [ky0, ky1)
+// likewise for the row-indexed tables (5-7, 10-12).  gx: over how many points
+// from a chunk's start the forward product G of the x sweep has a component
+// of magnitude >= 2^-40 (beyond, the carry it scales is far below FP32
+// resolution); qx: the same for Q from a chunk's end; gy, qy for the y sweep.
+void adi_ranges(const std::vector<float2>& t, int M, int mx, int my, const int cx[5], const int cy[5], int out[8]) {
+  auto eq = [&](int tab, int a, int b) {
+    const float2 u = t[(size_t)tab * M + a], v = t[(size_t)tab * M + b];
+    return memcmp(&u, &v, sizeof(float2)) == 0;
+  };
+  auto range = [&](int m, std::initializer_list<int> tabs, int* o) {
+    const int ref = m / 2;
+    auto same = [&](int k) {
+      for (int tab : tabs)
+        if (!eq(tab, k, ref)) return false;
+      return true;
+    };
+    int lo = ref, hi = ref + 1;
+    while (lo > 0 && same(lo - 1)) --lo;
+    while (hi < m && same(hi)) ++hi;
+    o[0] = lo;
+    o[1] = hi;
+  };
+  range(mx, {0, 1, 2, 13, 14, 15}, out);
+  range(my, {5, 6, 7, 10, 11, 12}, out + 2);
+  const float thr = 0x1p-40f;
+  auto big = [&](int tab, int k) {
+    const float2 v = t[(size_t)tab * M + k];
+    return std::fabs(v.x) >= thr || std::fabs(v.y) >= thr;
+  };
+  auto lengths = [&](const int* ch, int tg, int tq, int* o) {
+    int g = 0, q = 0;
+    for (int c = 0; c < 4; ++c)
+      for (int k = ch[c]; k < ch[c + 1]; ++k) {
+        if (big(tg, k)) g = std::max(g, k - ch[c] + 1);
+        if (big(tq, k)) q = std::max(q, ch[c + 1] - k);
+      }
+    o[0] = g;
+    o[1] = q;
+  };
+  lengths(cx, 3, 4, out + 4);
+  lengths(cy, 8, 9, out + 6);
+}
+
 }  // namespace
 
 // ADI planes of one grid size: one launch each, so that small grids are not
@@ -348,6 +401,7 @@ felis_status upload_inst_table(felis_batch* b) {
     D.F = p.scf_mode; D.nr = p.nr; D.bn = p.bessel_rows; D.bcols = p.bessel_cols;
     D.pitch = (p.nx - 2) | 1;
     for (int q = 0; q < 5; ++q) { D.cx[q] = I.cx[q]; D.cy[q] = I.cy[q]; }
+    memcpy(D.adi_k, I.adi_k, sizeof(D.adi_k));
     D.numSlice = p.num_slice; D.minI = p.min_i; D.wakeOn = p.wake_on;
     D.nsrc = I.nsrc;
     for (int i = 0; i < FELIS_MAX_HARMONY; ++i) {
@@ -538,8 +592,8 @@ felis_status ensure_launch(felis_batch* b) {
   b->adi_smem_max = 0;
   for (AdiClass& c : b->adi_classes) {
     if (std::max(c.nx, c.ny) > 256) return bfail(b, FELIS_UNSUPPORTED, "grid wider than 256 points");
-    // four threads per interior row (x sweep) and per interior column (y sweep)
-    c.threads = ((4 * (std::max(c.nx, c.ny) - 2) + 31) / 32) * 32;
+    // four chunks of every interior row (x sweep) and column (y sweep)
+    c.threads = batch_adi_threads(c.nx, c.ny);
     // 1 KB of every CTA's share stays for static shared memory
     const size_t cap = (size_t)b->dev_smem - 1024;
     const size_t base = batch_adi_smem(c.nx, c.ny, 0);
@@ -710,6 +764,7 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
     for (int h = 0; h < H; ++h) {
       std::vector<float2> t;
       adi_tables(*p, h, M, I.cx, I.cy, t);
+      adi_ranges(t, M, p->nx - 2, p->ny - 2, I.cx, I.cy, I.adi_k[h]);
       tabs.insert(tabs.end(), t.begin(), t.end());
     }
     if (e == cudaSuccess) e = cudaMalloc(&I.adi, tabs.size() * sizeof(float2));

@@ -20,6 +20,12 @@ struct BInst {
   // and the four chunks each interior row / column is split into (starts,
   // then the interior count): cx over the nx - 2 columns, cy over the rows
   int pitch, cx[5], cy[5];
+  // per harmonic, from its tables (batch.cu adi_ranges): the interior index
+  // ranges [kx0, kx1) over columns and [ky0, ky1) over rows where every
+  // coefficient table of that direction holds one value, and the lengths
+  // over which the chunk products matter (a component >= 2^-40): G from a
+  // chunk's start, Q from its end.  {kx0, kx1, ky0, ky1, gx, qx, gy, qy}
+  int adi_k[FELIS_MAX_HARMONY][8];
   int nsrc;                             // source planes per slice
   int harmony[FELIS_MAX_HARMONY];
   int src_plane[FELIS_MAX_HARMONY];     // first source plane of each harmonic
@@ -91,8 +97,12 @@ void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);
 void launch_batch_reduce(const BInst* inst, int ninst, const BStep* step, double* hist_e, double* hist_t,
                          double* hist_b, int hist_stride_e, int hist_stride_t, int hist_stride_b, cudaStream_t st);
-// Shared memory of the ADI launch with `src_cells` source cells staged.
-size_t batch_adi_smem(int nx_max, int ny_max, int src_cells);
+// Threads of the ADI launch of one grid size: four chunk groups of the
+// interior line count rounded up to whole warps.
+int batch_adi_threads(int nx, int ny);
+// Shared memory of the ADI launch of one grid size with `src_cells` source
+// cells staged.
+size_t batch_adi_smem(int nx, int ny, int src_cells);
 // Shared memory of the push launch with room for the accumulators of
 // `box_cells` source cells of every source plane.
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells);

@@ -124,47 +124,116 @@ __device__ __forceinline__ float quantum(float bound) {
 //
 // Each sweep is a forward and a backward first-order linear recurrence along
 // every interior row (x) or column (y), with data-independent coefficients.
-// Four threads (a lane quad) share a line, one chunk each: a thread runs the
-// recurrence over its chunk from a zero start, the quad composes the chunks'
-// affine carry maps with two shuffles (a scan over four elements), and the
-// thread corrects its chunk by the carry times the chunk product of the
-// coefficients (host tables G, Q).  Exact in real arithmetic; in FP32 the
-// rounding differs from the serial order by a few ulps.
+// Each line is split into four chunks.  Thread (q, l) runs chunk q of line l:
+// q = tid / NL and l = tid % NL with NL a multiple of 32, so all lanes of a
+// warp work on the same chunk of 32 neighbouring lines, run the same trip
+// counts and take the same branches.  A thread runs the recurrence over its
+// chunk from a zero start and publishes the chunk's end value; after a
+// barrier, chunk q composes the carry of the chunks before it (forward) or
+// after it (backward) with the chunk products at their ends, at most three
+// steps.  It then corrects its own points by the carry times the chunk
+// product of the coefficients (host tables G, Q).  This is exact in real
+// arithmetic; in FP32 the rounding differs from the serial order by a few
+// ulps.  The products fall off geometrically (by |alpha| / H per point,
+// about 0.01 on the usual grids), so the correction runs only over the points
+// where a component is still 2^-40 or more.  Outside the absorbing layers
+// every coefficient table holds one value, which those points take from
+// registers (BInst::adi_k).
 //
 // The right-hand side of each sweep reads the neighbouring lines, which other
-// threads overwrite: the x sweep's is formed in place in the staged plane
-// (thread per column chunk, rows in registers, the rows either side of the
-// chunk read before a barrier), the y sweep's while the x sweep's result is
-// finished (thread per row chunk).  Four barriers per plane; the final values
-// go straight to global memory (edge cells keep their values: the ADI never
-// writes them).
+// threads overwrite.  The x sweep's is formed in place in the staged plane
+// (thread per column and row chunk; the rows either side of the chunk are
+// read before a barrier).  The y sweep's is formed while the x sweep's result
+// is finished (thread per row and column chunk).  The source term is added
+// afterwards, on the source box only.  Seven barriers per plane; the final
+// values go straight to global memory (edge cells keep their values: the
+// ADI never writes them).
 // ============================================================================
-__device__ __forceinline__ float2 shfl_up2(float2 v, int d) {
-  return make_float2(__shfl_up_sync(0xffffffffu, v.x, d, 4), __shfl_up_sync(0xffffffffu, v.y, d, 4));
+
+// An interior index range [lo, hi) split at the range [k0, k1) where the
+// coefficient tables hold one value: [lo, a) and [b, hi) read the tables,
+// [a, b) uses that value from registers.
+__device__ __forceinline__ void split3(int lo, int hi, int k0, int k1, int& a, int& b) {
+  a = min(max(k0, lo), hi);
+  b = min(max(k1, a), hi);
 }
-__device__ __forceinline__ float2 shfl_down2(float2 v, int d) {
-  return make_float2(__shfl_down_sync(0xffffffffu, v.x, d, 4), __shfl_down_sync(0xffffffffu, v.y, d, 4));
-}
-// Carry into chunk q of the forward recurrence x_c = L_c + G_c x_{start-1}:
-// the composition of the maps of chunks 0..q-1 applied to zero.
-__device__ __forceinline__ float2 carry_fwd(float2 g, float2 l, int q) {
-#pragma unroll
-  for (int d = 1; d < 4; d <<= 1) {
-    const float2 gp = shfl_up2(g, d), lp = shfl_up2(l, d);
-    if (q >= d) { l = cad(l, cm(g, lp)); g = cm(g, gp); }
+
+// The loops below run along one line of a plane in shared memory, stride
+// `st` (1 along a row, the pitch along a column), in place.  Each loads the
+// next point before it stores the current one: the compiler cannot move a
+// shared-memory load above a store to the same array.  The forward loop's
+// load one point past its range stays inside the shared-memory allocation
+// (rows have pitch >= nx - 2, the tables follow the plane); its value is not
+// used.
+
+// Right-hand side v_k = ka_k u_{k+1} + kb_k u_k - kc_k u_{k-1}, k in [a, b)
+// of a chunk that ends at `end`.  (um, u0, up) hold u_{k-1}, u_k, u_{k+1} and
+// are advanced; u_{end} is `ue` (the point past the chunk, read before it
+// changed).
+template <bool K>
+__device__ __forceinline__ void rhs_run(float2* __restrict__ v, int st, int a, int b, int end,
+                                        const float2* ra, const float2* rb, const float2* rc, float2 ca, float2 cb,
+                                        float2 cc, float2& um, float2& u0, float2& up, float2 ue) {
+  const int bm = min(b, end - 2);  // below bm, u_{k+2} lies inside the chunk
+  int k = a;
+  for (; k < bm; ++k) {
+    const float2 un = v[(k + 2) * st];
+    const float2 ka = K ? ca : ra[k], kb = K ? cb : rb[k], kc = K ? cc : rc[k];
+    v[k * st] = csb(cad(cm(ka, up), cm(kb, u0)), cm(kc, um));
+    um = u0;
+    u0 = up;
+    up = un;
   }
-  const float2 ex = shfl_up2(l, 1);
-  return q == 0 ? make_float2(0.f, 0.f) : ex;
-}
-// Carry into chunk q of the backward recurrence x_c = B_c + Q_c x_{end+1}.
-__device__ __forceinline__ float2 carry_bwd(float2 g, float2 l, int q) {
-#pragma unroll
-  for (int d = 1; d < 4; d <<= 1) {
-    const float2 gp = shfl_down2(g, d), lp = shfl_down2(l, d);
-    if (q + d < 4) { l = cad(l, cm(g, lp)); g = cm(g, gp); }
+  for (; k < b; ++k) {
+    const float2 un = ue;  // used only where k + 2 == end
+    const float2 ka = K ? ca : ra[k], kb = K ? cb : rb[k], kc = K ? cc : rc[k];
+    v[k * st] = csb(cad(cm(ka, up), cm(kb, u0)), cm(kc, um));
+    um = u0;
+    u0 = up;
+    up = un;
   }
-  const float2 ex = shfl_down2(l, 1);
-  return q == 3 ? make_float2(0.f, 0.f) : ex;
+}
+
+// Forward recurrence L_k = v_k ka_k - km_k L_{k-1}, k in [a, b).
+template <bool K>
+__device__ __forceinline__ float2 fwd_run(float2* __restrict__ v, int st, int a, int b, const float2* ta,
+                                          const float2* tm, float2 ca, float2 cmv, float2 L) {
+  if (a < b) {
+    float2 x = v[a * st];
+    for (int k = a; k < b; ++k) {
+      const float2 xn = v[(k + 1) * st];
+      const float2 ka = K ? ca : ta[k], km = K ? cmv : tm[k];
+      L = csb(cm(x, ka), cm(km, L));
+      v[k * st] = L;
+      x = xn;
+    }
+  }
+  return L;
+}
+
+// Backward recurrence B_k = (v_k - B_{k+1}) kr_k, k from b - 1 down to a.
+template <bool K>
+__device__ __forceinline__ float2 bwd_run(float2* __restrict__ v, int st, int a, int b, const float2* tr, float2 cr,
+                                          float2 B) {
+  if (a < b) {
+    float2 x = v[(b - 1) * st];
+    for (int k = b - 1; k > a; --k) {
+      const float2 xn = v[(k - 1) * st];
+      const float2 kr = K ? cr : tr[k];
+      B = cm(csb(x, B), kr);
+      v[k * st] = B;
+      x = xn;
+    }
+    const float2 kr = K ? cr : tr[a];
+    B = cm(csb(x, B), kr);
+    v[a * st] = B;
+  }
+  return B;
+}
+
+// Carry correction v_k += g_k d, k in [a, b).
+__device__ __forceinline__ void axpy_run(float2* __restrict__ v, int st, int a, int b, const float2* g, float2 d) {
+  for (int k = a; k < b; ++k) v[k * st] = cad(v[k * st], cm(g[k], d));
 }
 
 __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
@@ -177,11 +246,16 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   const int S = I.S, nx = I.nx, ny = I.ny, P = I.pitch, Mx = nx > ny ? nx : ny;
   const int mx = nx - 2, my = ny - 2;
   const int tid = threadIdx.x, nt = blockDim.x;
+  const int NL = nt >> 2;  // lines per chunk: a multiple of 32, >= max(mx, my)
+  const int q = tid / NL, l = tid - q * NL;
   float2* U = I.U + ((size_t)hp * S + (s + T.ring_base) % S) * I.N;
   const float2* ad = I.adi_c + (size_t)h * 16 * Mx;
   float2* pl = reinterpret_cast<float2*>(sm);  // interior cells, [my][P]
   float2* tb = pl + (size_t)my * P;            // 16 tables of Mx
-  float2* ssrc = tb + 16 * Mx;
+  float2* cf = tb + 16 * Mx;                   // forward end values of chunks 0-2, [3][NL]
+  float2* cb = cf + 3 * NL;                    // backward start values of chunks 1-3
+  float2* ce = cb + 3 * NL;                    // backward end values of chunks 0-2 (x sweep)
+  float2* ssrc = ce + 3 * NL;
   for (int k = tid; k < 16 * Mx; k += nt) cp_async8(tb + k, ad + k);
   {
     const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
@@ -201,7 +275,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
     // the deposit packs the slice's source planes back to back, `cells` each
     const int p = I.src_plane[h] + ((I.harmony[h] & 1) ? 0 : pol);
     const float2* g = I.src + (size_t)s * I.nsrc * I.N + (size_t)p * cells;
-    const size_t used = ((size_t)my * P + 16 * (size_t)Mx) * sizeof(float2);
+    const size_t used = ((size_t)my * P + 16 * (size_t)Mx + 9 * (size_t)NL) * sizeof(float2);
     if (cells > 0 && used + (size_t)cells * sizeof(float2) <= (size_t)a.smem_bytes) {
       for (int k = tid; k < cells; k += nt) cp_async8(ssrc + k, g + k);
       Sc = ssrc;
@@ -215,13 +289,17 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   cp_async_wait_all();
   __syncthreads();
   const float2 zero = make_float2(0.f, 0.f);
-  // ---- x sweep right-hand side: thread (column, row chunk), in place in the
-  // staged plane; the rows either side of the chunk are read first
+  const int* K8 = I.adi_k[h];
+  const int kx0 = K8[0], kx1 = K8[1], ky0 = K8[2], ky1 = K8[3], gx = K8[4], qx = K8[5], gy = K8[6], qy = K8[7];
+  const int kcx = kx0 < kx1 ? kx0 : 0, kcy = ky0 < ky1 ? ky0 : 0;  // where the constants are read
+  const int c0 = I.cx[q], c1 = I.cx[q + 1];  // this thread's chunk of a row (x sweep)
+  const int r0 = I.cy[q], r1 = I.cy[q + 1];  // and of a column (x right-hand side, y sweep)
   double e = 0.0;
+  // ---- x sweep right-hand side: thread (column l, row chunk q), in place in
+  // the staged plane; the rows either side of the chunk are read first
   {
-    const int c = tid % mx, qc = tid / mx;
-    const bool valid = qc < 4;
-    const int r0 = valid ? I.cy[qc] : 0, r1 = valid ? I.cy[qc + 1] : 0, i = c + 1;
+    const bool valid = l < mx;
+    const int c = valid ? l : 0, i = c + 1;
     float2 um = zero, ul = zero;
     if (valid) {
       um = r0 == 0 ? U[i] : pl[(r0 - 1) * P + c];
@@ -237,143 +315,136 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       e += (double)(v.x * v.x + v.y * v.y);
     }
     __syncthreads();
-    // every loop below loads the next step's operands before it stores: the
-    // compiler cannot move a shared-memory load above a store to the same array
     if (valid) {
       const float2* ra = tb + 10 * Mx;
       const float2* rb = tb + 11 * Mx;
       const float2* rc = tb + 12 * Mx;
-      float2 u0 = pl[r0 * P + c];
-      float2 up = r0 + 1 < r1 ? pl[(r0 + 1) * P + c] : ul;
-      // the source term of this column: one range test per column, one per row
-      const bool scol = src && i >= bi0 && i <= bi1;
-      const float2* sc = scol ? Sc + (i - bi0) : Sc;
-      auto srow = [&](int j) -> float2 {
-        return (scol && j >= bj0 && j <= bj1) ? cm(sfac, sc[(j - bj0) * bw]) : zero;
-      };
-      float2 ka = ra[r0], kb = rb[r0], kc = rc[r0], sv = srow(r0 + 1);
-      for (int r = r0; r < r1; ++r) {
-        const int rn = r + 1 < r1 ? r + 1 : r;
-        const float2 upn = r + 2 < r1 ? pl[(r + 2) * P + c] : ul;
-        const float2 kan = ra[rn], kbn = rb[rn], kcn = rc[rn], svn = srow(rn + 1);
-        pl[r * P + c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
-        um = u0;
-        u0 = up;
-        up = upn;
-        ka = kan; kb = kbn; kc = kcn; sv = svn;
+      float2* v = pl + c;
+      float2 u0 = v[r0 * P];
+      float2 up = r0 + 1 < r1 ? v[(r0 + 1) * P] : ul;
+      int ka_, kb_;
+      split3(r0, r1, ky0, ky1, ka_, kb_);
+      const float2 ca = ra[kcy], cb_ = rb[kcy], cc = rc[kcy];
+      rhs_run<false>(v, P, r0, ka_, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
+      rhs_run<true>(v, P, ka_, kb_, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
+      rhs_run<false>(v, P, kb_, r1, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
+      // the source term, on the rows of the slice's source box only
+      if (src && i >= bi0 && i <= bi1) {
+        const float2* sc = Sc + (i - bi0);
+        for (int r = max(r0, bj0 - 1); r < min(r1, bj1); ++r) v[r * P] = cad(v[r * P], cm(sfac, sc[(r + 1 - bj0) * bw]));
       }
     }
   }
   __syncthreads();
-  const int q = tid & 3, line = tid >> 2;
-  // ---- x sweep: thread (row, column chunk)
+  // ---- x sweep: thread (row l, column chunk q)
   {
     const float2* pa = tb;
     const float2* pm = tb + Mx;
     const float2* pr = tb + 2 * Mx;
     const float2* pG = tb + 3 * Mx;
     const float2* pQ = tb + 4 * Mx;
-    const bool valid = line < my;
-    const int c0 = I.cx[q], c1 = I.cx[q + 1];
-    float2* row = pl + (valid ? line : 0) * P;
-    float2 L = zero;
+    const bool valid = l < my;
+    float2* row = pl + (valid ? l : 0) * P;
+    int ka_, kb_;
+    split3(c0, c1, kx0, kx1, ka_, kb_);
     if (valid) {
-      float2 v = row[c0], ka = pa[c0], km = pm[c0];
-      for (int c = c0; c < c1; ++c) {
-        const int cn = c + 1;  // one past the chunk stays inside the plane or the tables
-        const float2 vn = row[cn], kan = pa[cn], kmn = pm[cn];
-        L = csb(cm(v, ka), cm(km, L));
-        row[c] = L;
-        v = vn; ka = kan; km = kmn;
-      }
+      const float2 ca = pa[kcx], cmv = pm[kcx];
+      float2 L = fwd_run<false>(row, 1, c0, ka_, pa, pm, ca, cmv, zero);
+      L = fwd_run<true>(row, 1, ka_, kb_, pa, pm, ca, cmv, L);
+      L = fwd_run<false>(row, 1, kb_, c1, pa, pm, ca, cmv, L);
+      if (q < 3) cf[q * NL + l] = L;
     }
-    const float2 din = carry_fwd(pG[c1 - 1], L, q);
-    float2 B = zero, Blast = zero;
+    __syncthreads();
     if (valid) {
-      float2 v = row[c1 - 1], kg = pG[c1 - 1], kr = pr[c1 - 1];
-      for (int c = c1 - 1; c >= c0; --c) {
-        const int cn = c > c0 ? c - 1 : c;
-        const float2 vn = row[cn], kgn = pG[cn], krn = pr[cn];
-        B = cm(csb(cad(v, cm(kg, din)), B), kr);
-        row[c] = B;
-        if (c == c1 - 1) Blast = B;
-        v = vn; kg = kgn; kr = krn;
-      }
+      // carry into the chunk: the forward result left of it, composed over the chunks before
+      float2 din = zero;
+      for (int p = 0; p < q; ++p) din = cad(cf[p * NL + l], cm(pG[I.cx[p + 1] - 1], din));
+      axpy_run(row, 1, c0, min(c1, c0 + gx), pG, din);
+      const float2 cr = pr[kcx];
+      float2 B = bwd_run<false>(row, 1, kb_, c1, pr, cr, zero);
+      B = bwd_run<true>(row, 1, ka_, kb_, pr, cr, B);
+      B = bwd_run<false>(row, 1, c0, ka_, pr, cr, B);
+      if (q > 0) cb[(q - 1) * NL + l] = B;
+      if (q < 3) ce[q * NL + l] = row[c1 - 1];
     }
-    const float2 uin = carry_bwd(pQ[c0], B, q);
-    // x sweep result at the chunk's last point, and from the quad's previous
-    // thread at the point left of the chunk (zero left of the first column)
-    const float2 uend = cad(Blast, cm(pQ[c1 - 1], uin));
-    const float2 uprev = shfl_up2(uend, 1);
-    // ---- finish the x sweep and form the y sweep's right-hand side
+    __syncthreads();
     if (valid) {
+      // carry into the chunk from the right: the x sweep's result at c1
+      float2 uin = zero;
+      for (int p = 3; p > q; --p) uin = cad(cb[(p - 1) * NL + l], cm(pQ[I.cx[p]], uin));
+      axpy_run(row, 1, max(c0, c1 - qx), c1, pQ, uin);
+      // the x sweep's result left of the chunk (zero left of the first column):
+      // the previous chunk's last point corrected by its carry, the result at c0
+      const float2 uprev = q > 0 ? cad(ce[(q - 1) * NL + l], cm(pQ[c0 - 1], row[c0])) : zero;
+      // ---- the y sweep's right-hand side from the x sweep's result
       const float2* ra = tb + 13 * Mx;
       const float2* rb = tb + 14 * Mx;
       const float2* rc = tb + 15 * Mx;
-      const int j = line + 1;
-      float2 um = q == 0 ? zero : uprev;
-      float2 u0 = cad(row[c0], cm(pQ[c0], uin));
-      float2 up = c0 + 1 < c1 ? cad(row[c0 + 1], cm(pQ[c0 + 1], uin)) : uin;
-      const bool srw = src && j >= bj0 && j <= bj1;
-      const float2* sr = srw ? Sc + (j - bj0) * bw : Sc;
-      auto scolv = [&](int i) -> float2 { return (srw && i >= bi0 && i <= bi1) ? cm(sfac, sr[i - bi0]) : zero; };
-      float2 ka = ra[c0], kb = rb[c0], kc = rc[c0], sv = scolv(c0 + 1);
-      for (int c = c0; c < c1; ++c) {
-        const int cn = c + 1, c2 = c + 2;  // past the chunk: read, not used
-        const float2 b2 = row[c2], q2 = pQ[c2];
-        const float2 kan = ra[cn], kbn = rb[cn], kcn = rc[cn], svn = scolv(cn + 1);
-        row[c] = cad(cad(cm(ka, up), cm(kb, u0)), csb(sv, cm(kc, um)));
-        um = u0;
-        u0 = up;
-        up = c + 2 < c1 ? cad(b2, cm(q2, uin)) : uin;
-        ka = kan; kb = kbn; kc = kcn; sv = svn;
+      const int j = l + 1;
+      float2 um = uprev;
+      float2 u0 = row[c0];
+      float2 up = c0 + 1 < c1 ? row[c0 + 1] : uin;
+      const float2 ca = ra[kcx], cb_ = rb[kcx], cc = rc[kcx];
+      rhs_run<false>(row, 1, c0, ka_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
+      rhs_run<true>(row, 1, ka_, kb_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
+      rhs_run<false>(row, 1, kb_, c1, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
+      if (src && j >= bj0 && j <= bj1) {
+        const float2* sr = Sc + (j - bj0) * bw;
+        for (int c = max(c0, bi0 - 1); c < min(c1, bi1); ++c) row[c] = cad(row[c], cm(sfac, sr[c + 1 - bi0]));
       }
     }
   }
   __syncthreads();
-  // ---- y sweep: thread (column, row chunk); results to global memory
+  // ---- y sweep: thread (column l, row chunk q); results to global memory
   {
     const float2* pa = tb + 5 * Mx;
     const float2* pm = tb + 6 * Mx;
     const float2* pr = tb + 7 * Mx;
     const float2* pG = tb + 8 * Mx;
     const float2* pQ = tb + 9 * Mx;
-    const bool valid = line < mx;
-    const int c = valid ? line : 0;
-    const int r0 = I.cy[q], r1 = I.cy[q + 1];
-    float2 L = zero;
+    const bool valid = l < mx;
+    const int c = valid ? l : 0;
+    float2* v = pl + c;
+    int ka_, kb_;
+    split3(r0, r1, ky0, ky1, ka_, kb_);
     if (valid) {
-      float2 v = pl[r0 * P + c], ka = pa[r0], km = pm[r0];
-      for (int r = r0; r < r1; ++r) {
-        const int rn = r + 1;
-        const float2 vn = pl[rn * P + c], kan = pa[rn], kmn = pm[rn];
-        L = csb(cm(v, ka), cm(km, L));
-        pl[r * P + c] = L;
-        v = vn; ka = kan; km = kmn;
-      }
+      const float2 ca = pa[kcy], cmv = pm[kcy];
+      float2 L = fwd_run<false>(v, P, r0, ka_, pa, pm, ca, cmv, zero);
+      L = fwd_run<true>(v, P, ka_, kb_, pa, pm, ca, cmv, L);
+      L = fwd_run<false>(v, P, kb_, r1, pa, pm, ca, cmv, L);
+      if (q < 3) cf[q * NL + l] = L;
     }
-    const float2 din = carry_fwd(pG[r1 - 1], L, q);
-    float2 B = zero;
+    __syncthreads();
     if (valid) {
-      float2 v = pl[(r1 - 1) * P + c], kg = pG[r1 - 1], kr = pr[r1 - 1];
-      for (int r = r1 - 1; r >= r0; --r) {
-        const int rn = r > r0 ? r - 1 : r;
-        const float2 vn = pl[rn * P + c], kgn = pG[rn], krn = pr[rn];
-        B = cm(csb(cad(v, cm(kg, din)), B), kr);
-        pl[r * P + c] = B;
-        v = vn; kg = kgn; kr = krn;
-      }
+      float2 din = zero;
+      for (int p = 0; p < q; ++p) din = cad(cf[p * NL + l], cm(pG[I.cy[p + 1] - 1], din));
+      axpy_run(v, P, r0, min(r1, r0 + gy), pG, din);
+      const float2 cr = pr[kcy];
+      float2 B = bwd_run<false>(v, P, kb_, r1, pr, cr, zero);
+      B = bwd_run<true>(v, P, ka_, kb_, pr, cr, B);
+      B = bwd_run<false>(v, P, r0, ka_, pr, cr, B);
+      if (q > 0) cb[(q - 1) * NL + l] = B;
     }
-    const float2 uin = carry_bwd(pQ[r0], B, q);
+    __syncthreads();
     if (valid) {
-      float2 v = pl[r0 * P + c], kq = pQ[r0];
-      for (int r = r0; r < r1; ++r) {
-        const int rn = r + 1;
-        const float2 vn = pl[rn * P + c], kqn = pQ[rn];
-        const float2 o = cad(v, cm(kq, uin));
-        U[(size_t)(r + 1) * nx + c + 1] = o;
+      float2 uin = zero;
+      for (int p = 3; p > q; --p) uin = cad(cb[(p - 1) * NL + l], cm(pQ[I.cy[p]], uin));
+      // y sweep result u_r = v_r + Q_r uin; Q matters on the last qy rows only
+      float2* Ug = U + nx + c + 1;
+      const int rq = max(r0, r1 - qy);
+      float2 x = v[r0 * P];
+      for (int r = r0; r < rq; ++r) {
+        const float2 xn = v[(r + 1) * P];
+        Ug[(size_t)r * nx] = x;
+        e += (double)(x.x * x.x + x.y * x.y);
+        x = xn;
+      }
+      for (int r = rq; r < r1; ++r) {
+        const float2 xn = v[(r + 1) * P];
+        const float2 o = cad(x, cm(pQ[r], uin));
+        Ug[(size_t)r * nx] = o;
         e += (double)(o.x * o.x + o.y * o.y);
-        v = vn; kq = kqn;
+        x = xn;
       }
     }
   }
@@ -1008,7 +1079,13 @@ PushKernel push_kernel(int H) {
 
 size_t batch_adi_smem(int nx_max, int ny_max, int src_cells) {
   const int M = nx_max > ny_max ? nx_max : ny_max;
-  return ((size_t)(ny_max - 2) * ((nx_max - 2) | 1) + 16 * (size_t)M + (size_t)src_cells) * sizeof(float2);
+  const size_t NL = (size_t)batch_adi_threads(nx_max, ny_max) / 4;
+  return ((size_t)(ny_max - 2) * ((nx_max - 2) | 1) + 16 * (size_t)M + 9 * NL + (size_t)src_cells) * sizeof(float2);
+}
+
+int batch_adi_threads(int nx, int ny) {
+  const int m = (nx > ny ? nx : ny) - 2;
+  return 4 * (((m + 31) / 32) * 32);
 }
 
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
