@@ -153,6 +153,8 @@ _sig("felis_config_load_beam", C.c_int, _vp, C.c_int32, C.c_uint64, _i64p, _dp, 
 _sig("felis_config_load_beam_device", C.c_int, _vp, C.c_int32, C.c_uint64, _i64p, _dp, _dp, _dp, _dp, _dp, _dp, _dp)
 _sig("felis_config_load_seed", C.c_int, _vp, C.c_int32, _dp, _dp)
 _sig("felis_config_wake", C.c_int, _vp, _dp, _dp)
+_sig("felis_config_wake_device", C.c_int, _vp, _dp, _dp)
+_sig("felis_config_wake_function", C.c_int, _vp, _dp)
 _sig("felis_detmath_sincos", None, C.c_double, _dp, _dp)
 _sig("felis_detmath_atan", C.c_double, C.c_double)
 _sig("felis_detmath_atan2", C.c_double, C.c_double, C.c_double)
@@ -282,13 +284,24 @@ class Config:
         shp = (p.slice_n + 2, p.ny, p.nx)
         return (ux[0::2] + 1j * ux[1::2]).reshape(shp), (uy[0::2] + 1j * uy[1::2]).reshape(shp)
 
-    def wake(self, den: np.ndarray) -> np.ndarray:
-        """Wake energy loss per global slice from the slice charge (wakeField.cpp:9-50)."""
+    def wake(self, den: np.ndarray, device: bool = False) -> np.ndarray:
+        """Wake energy loss per global slice from the slice charge
+        (wakeField.cpp:9-50); `device` computes the wake function (when none
+        is cached) and the convolution on the GPU."""
         den = _f64(den)
         out = np.zeros(self.params.global_slice_n)
-        st = _lib.felis_config_wake(self._h, _p(den), _p(out))
+        fn = _lib.felis_config_wake_device if device else _lib.felis_config_wake
+        st = fn(self._h, _p(den), _p(out))
         if st != OK:
             raise FelisError(st, "wake")
+        return out
+
+    def wake_function(self) -> np.ndarray:
+        """The cached wake function per global slice distance (wakeField.cpp:128-140)."""
+        out = np.zeros(self.params.global_slice_n)
+        st = _lib.felis_config_wake_function(self._h, _p(out))
+        if st != OK:
+            raise FelisError(st, "wake_function")
         return out
 
 

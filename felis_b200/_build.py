@@ -32,6 +32,7 @@ UNITS = [
     ("lib/k_field.cu", ["--fmad=false"]),
     ("lib/k_load.cu", ["--fmad=false"]),
     ("lib/k_1d.cu", ["--fmad=false"]),
+    ("lib/k_wake.cu", ["--fmad=false"]),
     ("lib/k_sort.cu", []),
     ("lib/batch.cu", []),
     ("lib/k_batch.cu", ["--use_fast_math"]),

@@ -31,6 +31,7 @@
 
 #include "../../../include/felis_b200.h"
 #include "../lib/load.cuh"
+#include "../lib/wake.cuh"
 
 namespace {
 
@@ -1129,6 +1130,67 @@ felis_status felis_config_wake(felis_config* c, const double* den_in, double* wa
   for (int i = sliceN - 1; i >= 0; --i)
     for (int ii = i; ii >= 0; --ii) wake_e[ii] += den[i] * c->wakeF[i - ii] * dZ * coef;
   for (int i = 0; i < sliceN; ++i) c->wake_e[i] = wake_e[i];
+  return FELIS_OK;
+}
+
+// The same on the device: wakeFunction (wakeField.cpp:53-159) when no wake
+// function is cached yet, and the convolution of updateWakeField
+// (wakeField.cpp:9-50) in the reference's order.  The density is normalised
+// on the host as in felis_config_wake.
+felis_status felis_config_wake_device(felis_config* c, const double* den_in, double* wake_e) {
+  if (!c || !den_in || !wake_e) return FELIS_BAD_ARG;
+  const felis_params& p = c->p;
+  const int sliceN = p.global_slice_n;
+  const double dZ = p.num_slice * p.lambda0;
+  std::vector<double> den(den_in, den_in + sliceN);
+  double totalCnt = 0.0;
+  for (double v : den) totalCnt += v;
+  if (totalCnt > 0.0) {
+    const double norm = 1.0 / (totalCnt * dZ);
+    for (double& v : den) v *= norm;
+  }
+  const double coef = totalCnt * 1.602e-19;
+  const size_t S = (size_t)std::max(sliceN, 1);
+  double *d_imp = nullptr, *d_wf = nullptr, *d_den = nullptr, *d_we = nullptr;
+  cudaError_t e = cudaMalloc(&d_imp, (felis::kWakeNumK + 1) * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_wf, S * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_den, S * sizeof(double));
+  if (e == cudaSuccess) e = cudaMalloc(&d_we, S * sizeof(double));
+  const bool compute = c->wakeF.empty();
+  if (e == cudaSuccess && compute) {
+    felis::WakeArgs a{};
+    a.shape = c->wakeShape; a.acdc = c->acdc; a.S = sliceN; a.dZ = dZ;
+    a.s0 = pow(2.0 * c->radius * c->radius / kZ0 / c->cond, 1.0 / 3.0);
+    a.ctau = c->ctau;
+    a.coef = kZ0 * 3e8 / M_PI / c->radius / c->radius / M_PI;
+    a.impZ = d_imp; a.wakeF = d_wf;
+    e = felis::launch_wake_function(a, 0);
+  } else if (e == cudaSuccess && sliceN > 0) {
+    e = cudaMemcpy(d_wf, c->wakeF.data(), sliceN * sizeof(double), cudaMemcpyHostToDevice);
+  }
+  if (e == cudaSuccess && sliceN > 0) e = cudaMemcpy(d_den, den.data(), sliceN * sizeof(double), cudaMemcpyHostToDevice);
+  if (e == cudaSuccess) e = felis::launch_wake_field(d_den, d_wf, sliceN, dZ, coef, d_we, 0);
+  if (e == cudaSuccess && sliceN > 0) e = cudaMemcpy(wake_e, d_we, sliceN * sizeof(double), cudaMemcpyDeviceToHost);
+  if (e == cudaSuccess && compute) {
+    c->wakeF.assign(sliceN, 0.0);
+    if (sliceN > 0) e = cudaMemcpy(c->wakeF.data(), d_wf, sliceN * sizeof(double), cudaMemcpyDeviceToHost);
+  }
+  for (double* q : {d_imp, d_wf, d_den, d_we})
+    if (q) cudaFree(q);
+  if (e != cudaSuccess) {
+    if (compute) c->wakeF.clear();
+    g_err = std::string("felis_config_wake_device: ") + cudaGetErrorString(e);
+    return FELIS_CUDA_ERROR;
+  }
+  for (int i = 0; i < sliceN; ++i) c->wake_e[i] = wake_e[i];
+  return FELIS_OK;
+}
+
+// The cached wake function (wakeField.cpp:128-140), global slice distances.
+felis_status felis_config_wake_function(felis_config* c, double* wake_f) {
+  if (!c || !wake_f) return FELIS_BAD_ARG;
+  if (c->wakeF.empty()) wake_function(c);
+  std::copy(c->wakeF.begin(), c->wakeF.end(), wake_f);
   return FELIS_OK;
 }
 

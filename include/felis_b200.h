@@ -412,6 +412,16 @@ felis_status felis_config_load_seed(felis_config* c, int32_t harmonic_index,
 /* Wake energy loss per slice (wakeField.cpp:9-50,53-159,161-223) from the
  * per-slice charge (den[s] = weight * count, summed over species). */
 felis_status felis_config_wake(felis_config* c, const double* den, double* wake_e);
+/* The same computed on the GPU (wakeField.cpp:9-50, 53-159; host buffers,
+ * the device arrays are allocated per call): the wake function when none is
+ * cached yet (agrees with the host's to about 1e-13), then the convolution
+ * with the density in the reference's order (bit-identical to
+ * felis_config_wake for the same wake function).  The wake function is
+ * cached in the config for later calls of either entry point. */
+felis_status felis_config_wake_device(felis_config* c, const double* den, double* wake_e);
+/* The cached wake function W(i dZ) per global slice distance
+ * (wakeField.cpp:128-140), computed on the host when none is cached. */
+felis_status felis_config_wake_function(felis_config* c, double* wake_f);
 
 /* ---- deterministic elementary functions (host versions, for tests) ------ */
 void felis_detmath_sincos(double x, double* s, double* c);
