@@ -191,31 +191,13 @@ void transverse_maps(const Inst& I, const felis_lattice& l0, const felis_lattice
 // solveField.cpp:138-180 rewritten with reciprocals): per direction p = 1/aP
 // (last row 1), m = a/(aP CC[i-1]) (first row 0, last row 1/CC[i-1]),
 // r = 1/CC, and the right-hand-side coefficients.
-// Four chunks of an interior line of m points, for the partitioned
-// recurrences of the ADI: starts with residues 0, 4, 8, 12 (mod 16) in some
-// order, so that the lanes of a quad walking the four chunks of one line, four
-// lines per half-warp, hit 16 distinct 8-byte shared-memory words when the
-// row pitch is odd; among those, the split with the shortest longest chunk.
+// Four equal chunks of an interior line of m points, for the partitioned
+// recurrences of the ADI.  The kernel's lanes walk one chunk of 32
+// neighbouring lines (odd row pitch), so any chunk start is free of
+// shared-memory bank conflicts; equal chunks keep the four chunk groups
+// equally long between the barriers.
 void adi_chunks(int m, int out[5]) {
-  static const int perm[6][3] = {{4, 8, 12}, {4, 12, 8}, {8, 4, 12}, {8, 12, 4}, {12, 4, 8}, {12, 8, 4}};
-  int best = 1 << 30;
-  out[0] = 0; out[4] = m;
-  for (int q = 1; q < 4; ++q) out[q] = q * m / 4;
-  for (const auto& rs : perm) {
-    int cand[3][2];
-    for (int q = 0; q < 3; ++q) {
-      const int ideal = (q + 1) * m / 4, r = rs[q];
-      const int lo = ideal - (((ideal - r) % 16) + 16) % 16;
-      cand[q][0] = lo;
-      cand[q][1] = lo + 16;
-    }
-    for (int a = 0; a < 8; ++a) {
-      const int s1 = cand[0][a & 1], s2 = cand[1][(a >> 1) & 1], s3 = cand[2][(a >> 2) & 1];
-      if (!(0 < s1 && s1 < s2 && s2 < s3 && s3 < m)) continue;
-      const int len = std::max(std::max(s1, s2 - s1), std::max(s3 - s2, m - s3));
-      if (len < best) { best = len; out[1] = s1; out[2] = s2; out[3] = s3; }
-    }
-  }
+  for (int q = 0; q <= 4; ++q) out[q] = q * m / 4;
 }
 
 // Complex tables of the ADI of harmonic hidx (solveField.cpp:80-185), indexed
