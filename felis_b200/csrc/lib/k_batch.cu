@@ -526,17 +526,31 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
                                              int ny, int bi0, int bi1, int bj0, int bj1, int bw, int cells,
                                              float iq2, float iqr, acc_t* gacc, unsigned sacc, unsigned sR,
                                              float dr, float idr2, int nr, int L, int F) {
+  // the next particle's state is loaded one iteration ahead: the accumulator
+  // adds below are compiler memory barriers, so no load moves above them
+  float nxv = 0.f, nyv = 0.f, ndg = 0.f, npx = 0.f, npy = 0.f;
+  double nth = 0.0;
+  if ((int)threadIdx.x < P) {
+    const int64_t n = p0 + threadIdx.x;
+    nxv = xs[n]; nyv = ys[n]; ndg = dgs[n]; nth = ths[n];
+    if (has_even) { npx = pxs[n]; npy = pys[n]; }
+  }
   for (int q = threadIdx.x; q < P; q += blockDim.x) {
-    const int64_t n = p0 + q;
-    const float x = xs[n], y = ys[n], g = gRf + dgs[n];
-    const float thr = theta_red(ths[n]);
+    const float x = nxv, y = nyv, g = gRf + ndg, px = npx, py = npy;
+    const double th = nth;
+    if (q + (int)blockDim.x < P) {
+      const int64_t m = p0 + q + blockDim.x;
+      nxv = xs[m]; nyv = ys[m]; ndg = dgs[m]; nth = ths[m];
+      if (has_even) { npx = pxs[m]; npy = pys[m]; }
+    }
+    const float thr = theta_red(th);
     const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
     const int ii = (int)gx, jj = (int)gy;
     if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
       const float wx1 = gx - ii, wy1 = gy - jj;
       float xi2 = 0.f;
       float2 eP = make_float2(1.f, 0.f);
-      if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, pxs[n], pys[n], &xi2, &eP);
+      if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
       int cidx[4];
       float wv[4];
 #pragma unroll
