@@ -335,6 +335,10 @@ struct felis_batch {
   int src_valid_it = -1;  // iteration whose solveField source is in the buffers
   double last_run_ms = 0.0;
   int* h_err = nullptr;
+  // device staging of host transfers (FP64 particles and field planes are
+  // copied as they are and rounded or widened on the device)
+  double* stage = nullptr;
+  size_t stage_bytes = 0;
 };
 
 namespace {
@@ -783,7 +787,7 @@ void felis_batch_destroy(felis_batch* b) {
                     I.src, I.sbox, I.part_e, I.part_b, I.err};
     for (void* q : ptrs) if (q) cudaFree(q);
   }
-  void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_he, b->d_ht, b->d_hb};
+  void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_he, b->d_ht, b->d_hb, b->stage};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (b->h_err) cudaFreeHost(b->h_err);
   for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
@@ -792,6 +796,20 @@ void felis_batch_destroy(felis_batch* b) {
 }
 
 const char* felis_batch_last_error(const felis_batch* b) { return b ? b->err.c_str() : "null ensemble"; }
+
+namespace {
+// The staging buffer holds at least `bytes`.
+cudaError_t ensure_stage(felis_batch* b, size_t bytes) {
+  if (b->stage_bytes >= bytes) return cudaSuccess;
+  cudaError_t e = cudaStreamSynchronize(b->st);
+  if (e == cudaSuccess && b->stage) e = cudaFree(b->stage);
+  b->stage = nullptr;
+  b->stage_bytes = 0;
+  if (e == cudaSuccess) e = cudaMalloc(&b->stage, bytes);
+  if (e == cudaSuccess) b->stage_bytes = bytes;
+  return e;
+}
+}  // namespace
 
 felis_status felis_batch_upload_particles(felis_batch* b, int32_t inst, const double* x, const double* y,
                                           const double* px, const double* py, const double* theta,
@@ -820,23 +838,23 @@ felis_status felis_batch_upload_particles(felis_batch* b, int32_t inst, const do
   b->src_valid_it = -1;       // the next run deposits first
   const double* src[5] = {x, y, px, py, gamma};
   float* dst[5] = {I.x, I.y, I.px, I.py, I.dg};
-  // host arrays are rounded on the host, device arrays (the device beam
-  // loader's) on the device; gamma is stored as gamma - gamR
+  // every array is rounded on the device; gamma is stored as gamma - gamR.
+  // Device arrays (the device beam loader's) are read in place; host arrays
+  // are copied as they are through the theta buffer (n doubles), which
+  // receives theta itself last
   cudaPointerAttributes at{};
   const bool on_device = n > 0 && cudaPointerGetAttributes(&at, x) == cudaSuccess && at.type == cudaMemoryTypeDevice;
-  if (on_device) {
-    for (int k = 0; k < 5; ++k) BCK(launch_f64_to_f32(src[k], dst[k], n, k == 4 ? I.p.gam_r : 0.0, b->st));
-    BCK(cudaMemcpyAsync(I.th, theta, n * sizeof(double), cudaMemcpyDeviceToDevice, b->st));
-    BCK(cudaStreamSynchronize(b->st));
-  } else {
-    std::vector<float> tmp(n);
-    for (int k = 0; k < 5; ++k) {
-      const double off = k == 4 ? I.p.gam_r : 0.0;
-      for (int64_t i = 0; i < n; ++i) tmp[i] = (float)(src[k][i] - off);
-      if (n) BCK(cudaMemcpy(dst[k], tmp.data(), n * sizeof(float), cudaMemcpyHostToDevice));
+  for (int k = 0; k < 5 && n > 0; ++k) {
+    const double off = k == 4 ? I.p.gam_r : 0.0;
+    if (on_device) {
+      BCK(launch_f64_to_f32(src[k], dst[k], n, off, b->st));
+    } else {
+      BCK(cudaMemcpyAsync(I.th, src[k], n * sizeof(double), cudaMemcpyDefault, b->st));
+      BCK(launch_f64_to_f32(I.th, dst[k], n, off, b->st));
     }
-    if (n) BCK(cudaMemcpy(I.th, theta, n * sizeof(double), cudaMemcpyHostToDevice));
   }
+  if (n) BCK(cudaMemcpyAsync(I.th, theta, n * sizeof(double), cudaMemcpyDefault, b->st));
+  BCK(cudaStreamSynchronize(b->st));
   BCK(cudaMemcpy(I.soff, slice_offsets, (S + 1) * sizeof(int64_t), cudaMemcpyHostToDevice));
   std::vector<float> w(weights, weights + S);
   BCK(cudaMemcpy(I.weight, w.data(), S * sizeof(float), cudaMemcpyHostToDevice));
@@ -848,18 +866,18 @@ felis_status felis_batch_download_particles(felis_batch* b, int32_t inst, double
                                             double* py, double* theta, double* gamma) {
   if (!b || inst < 0 || inst >= (int)b->in.size() || !b->in[inst].uploaded) return bfail(b, FELIS_BAD_ARG, "bad argument");
   Inst& I = b->in[inst];
-  BCK(cudaStreamSynchronize(b->st));
   const int64_t n = I.count;
-  std::vector<float> tmp(n);
+  // widened on the device into the staging buffer, then copied as they are
   double* dst[5] = {x, y, px, py, gamma};
   const float* src[5] = {I.x, I.y, I.px, I.py, I.dg};
+  if (n) BCK(ensure_stage(b, n * sizeof(double)));
   for (int k = 0; k < 5; ++k) {
     if (!dst[k] || !n) continue;
-    BCK(cudaMemcpy(tmp.data(), src[k], n * sizeof(float), cudaMemcpyDeviceToHost));
-    const double off = k == 4 ? I.p.gam_r : 0.0;
-    for (int64_t i = 0; i < n; ++i) dst[k][i] = off + (double)tmp[i];
+    BCK(launch_f32_to_f64(src[k], b->stage, n, k == 4 ? I.p.gam_r : 0.0, b->st));
+    BCK(cudaMemcpyAsync(dst[k], b->stage, n * sizeof(double), cudaMemcpyDefault, b->st));
   }
-  if (theta && n) BCK(cudaMemcpy(theta, I.th, n * sizeof(double), cudaMemcpyDeviceToHost));
+  if (theta && n) BCK(cudaMemcpyAsync(theta, I.th, n * sizeof(double), cudaMemcpyDefault, b->st));
+  BCK(cudaStreamSynchronize(b->st));
   return FELIS_OK;
 }
 
@@ -868,14 +886,19 @@ felis_status felis_batch_upload_field(felis_batch* b, int32_t inst, int32_t hidx
   Inst& I = b->in[inst];
   if (hidx < 0 || hidx >= I.p.num_harmony || pol < 0 || pol > 1) return bfail(b, FELIS_BAD_ARG, "bad harmonic/pol");
   const int S = I.p.slice_n;
-  const size_t N = (size_t)I.p.nx * I.p.ny;
-  std::vector<float2> plane(N);
-  for (int s = 0; s < S; ++s) {
-    const double* src = data + 2 * (size_t)(s + 1) * N;
-    for (size_t k = 0; k < N; ++k) plane[k] = make_float2((float)src[2 * k], (float)src[2 * k + 1]);
-    const int phys = (s + I.ring_base) % S;
-    BCK(cudaMemcpy(I.U + ((size_t)(hidx * 2 + pol) * S + phys) * N, plane.data(), N * sizeof(float2), cudaMemcpyHostToDevice));
+  const int N = I.p.nx * I.p.ny;
+  // the slices' planes (the reference layout's planes 1..S) copied as they
+  // are into the staging buffer, in blocks of slices, and rounded into the ring
+  const size_t plane_bytes = (size_t)N * 2 * sizeof(double);
+  BCK(ensure_stage(b, std::max(plane_bytes, std::min((size_t)S * plane_bytes, (size_t)64 << 20))));
+  const int per = (int)std::max<size_t>(1, b->stage_bytes / plane_bytes);
+  float2* U = I.U + (size_t)(hidx * 2 + pol) * S * N;
+  for (int s0 = 0; s0 < S; s0 += per) {
+    const int ns = std::min(per, S - s0);
+    BCK(cudaMemcpyAsync(b->stage, data + 2 * (size_t)(s0 + 1) * N, (size_t)ns * plane_bytes, cudaMemcpyDefault, b->st));
+    BCK(launch_field_to_f32(b->stage, U, s0, ns, S, N, I.ring_base, b->st));
   }
+  BCK(cudaStreamSynchronize(b->st));
   return FELIS_OK;
 }
 

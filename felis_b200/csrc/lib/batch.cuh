@@ -90,8 +90,15 @@ struct BatchLaunch {
 enum { BATCH_PUSH = 0, BATCH_DEPOSIT_ONLY = 1 };
 
 void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st);
-// dst[i] = (float)(src[i] - off) on the device (uploads of device arrays).
+// dst[i] = (float)(src[i] - off) on the device (particle uploads).
 cudaError_t launch_f64_to_f32(const double* src, float* dst, int64_t n, double off, cudaStream_t st);
+// dst[i] = off + (double)src[i] on the device (particle downloads).
+cudaError_t launch_f32_to_f64(const float* src, double* dst, int64_t n, double off, cudaStream_t st);
+// Slices [s0, s0 + ns) of one field plane set, complex FP64 in the reference
+// layout (slice s at src + 2 (s - s0) N doubles), rounded into the ring U
+// (slice s at ring plane (s + ring_base) % S).
+cudaError_t launch_field_to_f32(const double* src, float2* U, int s0, int ns, int S, int N, int ring_base,
+                                cudaStream_t st);
 // H: the largest harmonic count of the ensemble (selects the kernel instance).
 void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st);
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);

@@ -1134,12 +1134,44 @@ __global__ void k_f64_to_f32(const double* __restrict__ src, float* __restrict__
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
     dst[i] = (float)(src[i] - off);
 }
+__global__ void k_f32_to_f64(const float* __restrict__ src, double* __restrict__ dst, int64_t n, double off) {
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
+    dst[i] = off + (double)src[i];
+}
+// slices [s0, s0 + ns) of one (harmonic, pol) field from the reference
+// layout (complex FP64, plane s at src + (s - s0) N) into the ring
+__global__ void k_field_to_f32(const double2* __restrict__ src, float2* __restrict__ U, int s0, int ns, int S, int N,
+                               int ring_base) {
+  const int64_t tot = (int64_t)ns * N;
+  for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < tot; i += (int64_t)gridDim.x * blockDim.x) {
+    const int s = s0 + (int)(i / N), k = (int)(i % N);
+    const double2 v = src[i];
+    U[(size_t)((s + ring_base) % S) * N + k] = make_float2((float)v.x, (float)v.y);
+  }
+}
 }  // namespace
 
 cudaError_t launch_f64_to_f32(const double* src, float* dst, int64_t n, double off, cudaStream_t st) {
   if (n <= 0) return cudaSuccess;
   const int64_t blocks = (n + 255) / 256;
   k_f64_to_f32<<<(int)(blocks < 4736 ? blocks : 4736), 256, 0, st>>>(src, dst, n, off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_f32_to_f64(const float* src, double* dst, int64_t n, double off, cudaStream_t st) {
+  if (n <= 0) return cudaSuccess;
+  const int64_t blocks = (n + 255) / 256;
+  k_f32_to_f64<<<(int)(blocks < 4736 ? blocks : 4736), 256, 0, st>>>(src, dst, n, off);
+  return cudaGetLastError();
+}
+
+cudaError_t launch_field_to_f32(const double* src, float2* U, int s0, int ns, int S, int N, int ring_base,
+                                cudaStream_t st) {
+  const int64_t tot = (int64_t)ns * N;
+  if (tot <= 0) return cudaSuccess;
+  const int64_t blocks = (tot + 255) / 256;
+  k_field_to_f32<<<(int)(blocks < 4736 ? blocks : 4736), 256, 0, st>>>(reinterpret_cast<const double2*>(src), U, s0,
+                                                                        ns, S, N, ring_base);
   return cudaGetLastError();
 }
 
