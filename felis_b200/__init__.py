@@ -348,10 +348,19 @@ class Handle:
         self._ck(_lib.felis_upload_particles(self._h, species, *(p for _, p in arrs), off.ctypes.data_as(_i64p), _p(w)))
         self._counts[species] = int(off[-1])
 
-    def download_particles(self, species: int = 0) -> dict:
+    def download_particles(self, species: int = 0, out: dict | None = None) -> dict:
+        """Particle state of one species.  `out` may hold the six arrays to
+        fill (contiguous float64 of the particle count, e.g. pinned host
+        buffers for full-speed copies); new arrays otherwise."""
         n = self._counts[species]
-        out = {k: np.zeros(n) for k in ("x", "y", "px", "py", "theta", "gamma")}
-        self._ck(_lib.felis_download_particles(self._h, species, *(_p(out[k]) for k in ("x", "y", "px", "py", "theta", "gamma"))))
+        keys = ("x", "y", "px", "py", "theta", "gamma")
+        if out is None:
+            out = {k: np.zeros(n) for k in keys}
+        for k in keys:
+            a = out[k]
+            if a.dtype != np.float64 or a.size != n or not a.flags.c_contiguous:
+                raise ValueError(f"out[{k!r}]: contiguous float64 of {n} elements expected")
+        self._ck(_lib.felis_download_particles(self._h, species, *(_p(out[k]) for k in keys)))
         return out
 
     def upload_field(self, hidx: int, pol: int, data: np.ndarray):
@@ -536,10 +545,18 @@ class Batch:
                                                    off.ctypes.data_as(_i64p), _p(w)))
         self._counts[inst] = int(off[-1])
 
-    def download_particles(self, inst: int) -> dict:
+    def download_particles(self, inst: int, out: dict | None = None) -> dict:
+        """Particle state of one instance (FP64).  `out` may hold the six
+        arrays to fill (contiguous float64 of the particle count, e.g. pinned
+        host buffers for full-speed copies); new arrays otherwise."""
         n = self._counts[inst]
         keys = ("x", "y", "px", "py", "theta", "gamma")
-        out = {k: np.zeros(n) for k in keys}
+        if out is None:
+            out = {k: np.zeros(n) for k in keys}
+        for k in keys:
+            a = out[k]
+            if a.dtype != np.float64 or a.size != n or not a.flags.c_contiguous:
+                raise ValueError(f"out[{k!r}]: contiguous float64 of {n} elements expected")
         self._ck(_lib.felis_batch_download_particles(self._b, inst, *(_p(out[k]) for k in keys)))
         return out
 
