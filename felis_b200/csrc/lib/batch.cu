@@ -994,8 +994,8 @@ felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1) {
 }
 
 // Online launch-shape tuner.  The particle state and the fields after a step
-// do not depend on the launch shape (fixed-point deposit, one thread per ADI
-// row or column, one thread per particle), so the tuner advances the
+// do not depend on the launch shape (fixed-point deposit, ADI chunks fixed by
+// the grid, one thread per particle), so the tuner advances the
 // ensemble through real iterations, each candidate shape for `steps` of
 // them, and keeps the fastest.  Results are cached per ensemble geometry.
 felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it) {

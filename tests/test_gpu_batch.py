@@ -230,6 +230,25 @@ def test_tune_advances_and_caches(fb, seeded):
     assert again.tune(0, 2) == 0  # cached: nothing run
 
 
+def test_download_into_caller_buffers(fb, seeded):
+    """download_particles(out=...) fills the given arrays with the same values
+    as a download into new arrays; a wrong buffer is refused."""
+    cfg, beam, fields = seeded
+    b = fb.Batch([cfg.params])
+    _upload(fb, b, 0, cfg, beam, fields)
+    b.run(0, 6)
+    ref = b.download_particles(0)
+    n = ref["x"].size
+    out = {k: np.full(n, np.nan) for k in ref}
+    got = b.download_particles(0, out=out)
+    assert got is out
+    for k in ref:
+        assert np.array_equal(out[k], ref[k]), k
+    with pytest.raises(ValueError):
+        b.download_particles(0, out=dict(out, x=np.zeros(n, dtype=np.float32)))
+    b.close()
+
+
 def test_errors_are_reported(fb, seeded):
     cfg, beam, fields = seeded
     b = fb.Batch([cfg.params])

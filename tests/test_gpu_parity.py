@@ -138,6 +138,11 @@ def test_graph_run_equals_steps(fb, oracle_mod, tmp_path):
     d1, d2 = g1.diagnostics(0, n), g2.diagnostics(0, n)
     for x, y in zip(d1, d2):
         assert_bits(x, y, "graph vs steps: diagnostics")
+    # the same state downloaded into caller buffers
+    out = {k: np.full(a[k].size, np.nan) for k in a}
+    assert g2.download_particles(0, out=out) is out
+    for k in a:
+        assert_bits(out[k], b[k], f"download into caller buffers: {k}")
 
 
 def test_drop_in_loop_equals_fused(fb, oracle_mod, tmp_path):
