@@ -236,6 +236,22 @@ __device__ __forceinline__ void axpy_run(float2* __restrict__ v, int st, int a, 
   for (int k = a; k < b; ++k) v[k * st] = cad(v[k * st], cm(g[k], d));
 }
 
+// Source term v_k += f src[(k + 1 - k0) * ss], k in [a, b), along a line of
+// stride st.  The source is read eight points at a time before the stores:
+// it may live in global memory (a box too large to stage), and a generic
+// pointer cannot be moved past the shared-memory stores.
+__device__ __forceinline__ void add_source(float2* __restrict__ v, int st, int a, int b, const float2* src, int k0,
+                                           int ss, float2 f) {
+  for (int k = a; k < b; k += 8) {
+    float2 t[8];
+#pragma unroll
+    for (int u = 0; u < 8; ++u) t[u] = k + u < b ? src[(k + u + 1 - k0) * ss] : make_float2(0.f, 0.f);
+#pragma unroll
+    for (int u = 0; u < 8; ++u)
+      if (k + u < b) v[(k + u) * st] = cad(v[(k + u) * st], cm(f, t[u]));
+  }
+}
+
 __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ double redd[32];
@@ -329,10 +345,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       rhs_run<true>(v, P, ka_, kb_, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
       rhs_run<false>(v, P, kb_, r1, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
       // the source term, on the rows of the slice's source box only
-      if (src && i >= bi0 && i <= bi1) {
-        const float2* sc = Sc + (i - bi0);
-        for (int r = max(r0, bj0 - 1); r < min(r1, bj1); ++r) v[r * P] = cad(v[r * P], cm(sfac, sc[(r + 1 - bj0) * bw]));
-      }
+      if (src && i >= bi0 && i <= bi1) add_source(v, P, max(r0, bj0 - 1), min(r1, bj1), Sc + (i - bi0), bj0, bw, sfac);
     }
   }
   __syncthreads();
@@ -388,10 +401,7 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       rhs_run<false>(row, 1, c0, ka_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
       rhs_run<true>(row, 1, ka_, kb_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
       rhs_run<false>(row, 1, kb_, c1, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
-      if (src && j >= bj0 && j <= bj1) {
-        const float2* sr = Sc + (j - bj0) * bw;
-        for (int c = max(c0, bi0 - 1); c < min(c1, bi1); ++c) row[c] = cad(row[c], cm(sfac, sr[c + 1 - bi0]));
-      }
+      if (src && j >= bj0 && j <= bj1) add_source(row, 1, max(c0, bi0 - 1), min(c1, bi1), Sc + (j - bj0) * bw, bi0, 1, sfac);
     }
   }
   __syncthreads();
@@ -496,14 +506,37 @@ __device__ __forceinline__ void ffac_t(const BesselTab& B, int H, float xi, floa
   }
 }
 
+// Shrinks [i0, i1] x [j0, j1] to its central window of at most `cap` cells
+// (about the same aspect); empty (i1 < i0) when no 2 x 2 window fits.  The
+// same for every thread of a CTA.
+__device__ __forceinline__ void shrink_window(int& i0, int& i1, int& j0, int& j1, int cap) {
+  const int w = i1 - i0 + 1, h = j1 - j0 + 1;
+  if (w <= 0 || h <= 0 || w * h <= cap) return;
+  if (cap < 4) { i1 = i0 - 1; return; }
+  const float sc = sqrtf((float)cap / ((float)w * (float)h));
+  int w2 = max(2, min(w, (int)((float)w * sc))), h2 = max(2, min(h, (int)((float)h * sc)));
+  while (w2 * h2 > cap) {
+    if (w2 >= h2 && w2 > 2) --w2;
+    else if (h2 > 2) --h2;
+    else break;
+  }
+  if (w2 * h2 > cap) { i1 = i0 - 1; return; }
+  i0 += (w - w2) / 2; i1 = i0 + w2 - 1;
+  j0 += (h - h2) / 2; j1 = j0 + h2 - 1;
+}
+
 // Fixed-point adds without a return value: shared-memory accumulators by
 // their 32-bit shared address, global ones by pointer.
 __device__ __forceinline__ void red_s(unsigned saddr, acc_t v) {
   if (v != 0) asm volatile("red.shared.add.s32 [%0], %1;\n" ::"r"(saddr), "r"(v) : "memory");
 }
+// SH: every accumulator in shared memory, at idx.  Otherwise the box's
+// accumulators are in global memory (idx) and those of its central window in
+// shared memory (widx, -1 outside the window).
 template <bool SH>
-__device__ __forceinline__ void acc_to(acc_t* gbase, unsigned sbase, int idx, acc_t v) {
+__device__ __forceinline__ void acc_to(acc_t* gbase, unsigned sbase, int idx, int widx, acc_t v) {
   if (SH) red_s(sbase + 4u * (unsigned)idx, v);
+  else if (widx >= 0) red_s(sbase + 4u * (unsigned)widx, v);
   else if (v != 0) atomicAdd(gbase + idx, v);
 }
 
@@ -514,7 +547,8 @@ struct DepConst {
 };
 
 // Pass 2: the source deposit (solveField.cpp:252-357) of the pushed
-// particles into the fixed-point accumulators (2D: shared or global, radial:
+// particles into the fixed-point accumulators (2D: shared, or global with the
+// window [wi0, wi1] x [wj0, wj1] of wcells cells in shared memory; radial:
 // shared).
 template <int HM, bool SH>
 __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const float* __restrict__ ys,
@@ -524,8 +558,10 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
                                              bool has_even, const DepConst& D, const BesselTab& B, float weight,
                                              float gRf, float minX, float minY, float idx_, float idy_, int nx,
                                              int ny, int bi0, int bi1, int bj0, int bj1, int bw, int cells,
-                                             float iq2, float iqr, acc_t* gacc, unsigned sacc, unsigned sR,
-                                             float dr, float idr2, int nr, int L, int F) {
+                                             int wi0, int wi1, int wj0, int wj1, int wcells, float iq2, float iqr,
+                                             acc_t* gacc, unsigned sacc, unsigned sR, float dr, float idr2, int nr,
+                                             int L, int F) {
+  const int ww = wi1 - wi0 + 1;
   // the next particle's state is loaded one iteration ahead: the accumulator
   // adds below are compiler memory barriers, so no load moves above them
   float nxv = 0.f, nyv = 0.f, ndg = 0.f, npx = 0.f, npy = 0.f;
@@ -551,13 +587,15 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
       float xi2 = 0.f;
       float2 eP = make_float2(1.f, 0.f);
       if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
-      int cidx[4];
+      int cidx[4], widx[4];
       float wv[4];
 #pragma unroll
       for (int cb = 0; cb < 4; ++cb) {
         const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
         const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
         cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
+        const bool inw = !SH && ti >= wi0 && ti <= wi1 && tj >= wj0 && tj <= wj1;
+        widx[cb] = inw ? (tj - wj0) * ww + (ti - wi0) : -1;
         wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
       }
       const float ig = 1.f / g;
@@ -567,13 +605,14 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
         const int Hh = hh[h];
         const float2 e = expif(-(float)Hh * (thr + D.Phi_half));
         const float2 mc = cs(e, (float)Hh * weight * D.coef_U * ig);
-        const int base = sp[h] * cells * 2;
+        const int base = sp[h] * cells * 2, wbase = sp[h] * wcells * 2;
         if (Hh & 1) {
 #pragma unroll
           for (int cb = 0; cb < 4; ++cb) {
             if (cidx[cb] < 0) continue;
-            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], fix(mc.x * wv[cb], iq2));
-            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, fix(mc.y * wv[cb], iq2));
+            const int wk = widx[cb] < 0 ? -1 : wbase + 2 * widx[cb];
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], wk, fix(mc.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, wk < 0 ? -1 : wk + 1, fix(mc.y * wv[cb], iq2));
           }
         } else {
           float2 fx, fy;
@@ -582,10 +621,12 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
 #pragma unroll
           for (int cb = 0; cb < 4; ++cb) {
             if (cidx[cb] < 0) continue;
-            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], fix(-ax.x * wv[cb], iq2));
-            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, fix(-ax.y * wv[cb], iq2));
-            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]), fix(-ay.x * wv[cb], iq2));
-            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]) + 1, fix(-ay.y * wv[cb], iq2));
+            const int wk = widx[cb] < 0 ? -1 : wbase + 2 * widx[cb];
+            const int wky = widx[cb] < 0 ? -1 : wbase + 2 * (wcells + widx[cb]);
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], wk, fix(-ax.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, wk < 0 ? -1 : wk + 1, fix(-ax.y * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]), wky, fix(-ay.x * wv[cb], iq2));
+            acc_to<SH>(gacc, sacc, base + 2 * (cells + cidx[cb]) + 1, wky < 0 ? -1 : wky + 1, fix(-ay.y * wv[cb], iq2));
           }
         }
       }
@@ -725,9 +766,11 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     {
       const int4 b = I.sbox[s];
       if (b.y >= b.x && b.w >= b.z) {
-        const int i0 = max(0, b.x - 3), i1 = min(nx - 1, b.y + 3), j0 = max(0, b.z - 3), j1 = min(ny - 1, b.w + 3);
+        int i0 = max(0, b.x - 3), i1 = min(nx - 1, b.y + 3), j0 = max(0, b.z - 3), j1 = min(ny - 1, b.w + 3);
+        // a box too large for the area: its central window (the beam's core)
+        shrink_window(i0, i1, j0, j1, (int)(area_bytes / ((size_t)2 * H * sizeof(float2))));
         const int w = i1 - i0 + 1, cells = w * (j1 - j0 + 1);
-        if ((size_t)2 * H * cells * sizeof(float2) <= area_bytes) {
+        if (i1 >= i0 && j1 >= j0) {
           fi0 = i0; fi1 = i1; fj0 = j0; fj1 = j1; fbw = w; fcells = cells;
           float2* dst = reinterpret_cast<float2*>(area);
           for (int hp = 0; hp < 2 * H; ++hp)
@@ -947,20 +990,44 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
   float2* gsrc = I.src + (size_t)s * nsrc * N;
   const bool in_smem = nacc * sizeof(acc_t) <= area_bytes;
   acc_t* acc = in_smem ? reinterpret_cast<acc_t*>(area) : reinterpret_cast<acc_t*>(gsrc);
+  // a box too large for the area accumulates in the source buffer, its
+  // central window (the beam's core, where most particles add) in the area;
+  // integer sums, so the split does not change the result
+  int wi0 = bi0, wi1 = bi1, wj0 = bj0, wj1 = bj1;
+  if (!in_smem) shrink_window(wi0, wi1, wj0, wj1, (int)(area_bytes / ((size_t)nsrc * 2 * sizeof(acc_t))));
+  const int wcells = (!in_smem && cells > 0 && wi1 >= wi0 && wj1 >= wj0) ? (wi1 - wi0 + 1) * (wj1 - wj0 + 1) : 0;
+  if (!wcells) { wi0 = 1; wi1 = 0; wj0 = 1; wj1 = 0; }
   for (size_t k = tid; k < nacc; k += nt) acc[k] = 0;
+  for (int k = tid; k < nsrc * wcells * 2; k += nt) reinterpret_cast<acc_t*>(area)[k] = 0;
   for (int k = tid; k < LF * nr * 2; k += nt) sR[k] = 0;
   __syncthreads();
   const unsigned sacc = (unsigned)__cvta_generic_to_shared(area);
   const unsigned sRa = (unsigned)__cvta_generic_to_shared(sR);
   if (in_smem)
     deposit_pass<HM, true>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
-                           idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, iq2, iqr, nullptr, sacc, sRa, dr,
-                           idr2, nr, L, F);
+                           idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, 1, 0, 1, 0, 0, iq2, iqr, nullptr, sacc,
+                           sRa, dr, idr2, nr, L, F);
   else
     deposit_pass<HM, false>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
-                            idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, iq2, iqr, acc, 0u, sRa, dr, idr2, nr,
-                            L, F);
+                            idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, wi0, wi1, wj0, wj1, wcells, iq2, iqr,
+                            acc, sacc, sRa, dr, idr2, nr, L, F);
   __syncthreads();
+  if (wcells > 0) {
+    // the window's sums into the box's
+    const int ww = wi1 - wi0 + 1;
+    const int2* wa = reinterpret_cast<const int2*>(area);
+    int2* ga = reinterpret_cast<int2*>(acc);
+    for (int k = tid; k < nsrc * wcells; k += nt) {
+      const int pl = k / wcells, w = k - pl * wcells;
+      const size_t gi = (size_t)pl * cells + (size_t)(wj0 + w / ww - bj0) * bw + (wi0 + w % ww - bi0);
+      const int2 a = wa[k];
+      int2 g = ga[gi];
+      g.x += a.x;
+      g.y += a.y;
+      ga[gi] = g;
+    }
+    __syncthreads();
+  }
   // source box of the next ADI (float2 per cell, in place when the
   // accumulators live in the source buffer itself)
   for (size_t k = tid; k < nacc / 2; k += nt) {
