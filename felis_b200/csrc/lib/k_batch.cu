@@ -237,9 +237,9 @@ __device__ __forceinline__ void axpy_run(float2* __restrict__ v, int st, int a, 
 }
 
 // Source term v_k += f src[(k + 1 - k0) * ss], k in [a, b), along a line of
-// stride st.  The source is read eight points at a time before the stores:
-// it may live in global memory (a box too large to stage), and a generic
-// pointer cannot be moved past the shared-memory stores.
+// stride st, for a source box too large to stage (in global memory): read
+// eight points at a time before the stores, since a generic pointer's loads
+// cannot be moved past the shared-memory stores.
 __device__ __forceinline__ void add_source(float2* __restrict__ v, int st, int a, int b, const float2* src, int k0,
                                            int ss, float2 f) {
   for (int k = a; k < b; k += 8) {
@@ -345,7 +345,14 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       rhs_run<true>(v, P, ka_, kb_, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
       rhs_run<false>(v, P, kb_, r1, r1, ra, rb, rc, ca, cb_, cc, um, u0, up, ul);
       // the source term, on the rows of the slice's source box only
-      if (src && i >= bi0 && i <= bi1) add_source(v, P, max(r0, bj0 - 1), min(r1, bj1), Sc + (i - bi0), bj0, bw, sfac);
+      if (src && i >= bi0 && i <= bi1) {
+        const int ra0 = max(r0, bj0 - 1), ra1 = min(r1, bj1);
+        const float2* sc = Sc + (i - bi0);
+        if (Sc == ssrc)
+          for (int r = ra0; r < ra1; ++r) v[r * P] = cad(v[r * P], cm(sfac, sc[(r + 1 - bj0) * bw]));
+        else
+          add_source(v, P, ra0, ra1, sc, bj0, bw, sfac);
+      }
     }
   }
   __syncthreads();
@@ -401,7 +408,14 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
       rhs_run<false>(row, 1, c0, ka_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
       rhs_run<true>(row, 1, ka_, kb_, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
       rhs_run<false>(row, 1, kb_, c1, c1, ra, rb, rc, ca, cb_, cc, um, u0, up, uin);
-      if (src && j >= bj0 && j <= bj1) add_source(row, 1, max(c0, bi0 - 1), min(c1, bi1), Sc + (j - bj0) * bw, bi0, 1, sfac);
+      if (src && j >= bj0 && j <= bj1) {
+        const int ca0 = max(c0, bi0 - 1), ca1 = min(c1, bi1);
+        const float2* sr = Sc + (j - bj0) * bw;
+        if (Sc == ssrc)
+          for (int c = ca0; c < ca1; ++c) row[c] = cad(row[c], cm(sfac, sr[c + 1 - bi0]));
+        else
+          add_source(row, 1, ca0, ca1, sr, bi0, 1, sfac);
+      }
     }
   }
   __syncthreads();
