@@ -94,7 +94,7 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_workload(name: str, rank: int = 0, slices: int | None = None, grid: int | None = None):
+def make_config(name: str, slices: int | None = None, grid: int | None = None):
     import felis_b200 as fb
     from felis_b200 import workloads
 
@@ -104,8 +104,21 @@ def make_workload(name: str, rank: int = 0, slices: int | None = None, grid: int
         kw["slices"] = slices
     if grid:
         kw["nx"] = grid
-    path = workloads.write_input(os.path.join(d, f"{name}.inp"), **kw)
-    cfg = fb.Config(path)
+    return fb.Config(workloads.write_input(os.path.join(d, f"{name}.inp"), **kw))
+
+
+def workload_config(name: str, p, P: int, W: int, K: int, world: int, precision: str) -> dict:
+    """The line's `config`: the workload, its sizes and the timed iterations."""
+    what = (f"{name}: {precision} time-dependent SASE, {p.slice_n} slices x {P // p.slice_n} particles, "
+            f"{p.nx}x{p.ny} grid, H={p.num_harmony}" if name == "sase"
+            else f"{name}: {precision} static, {P} particles, {p.nx}x{p.ny} grid")
+    return {"workload": what, "slices": p.slice_n, "particles": P, "grid": [p.nx, p.ny], "harmonics": p.num_harmony,
+            "iterations": [W, W + K], "l2": "inputs larger than L2 (particles 403 MB, field 171 MB per pol)",
+            "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
+
+
+def make_workload(name: str, rank: int = 0, slices: int | None = None, grid: int | None = None):
+    cfg = make_config(name, slices, grid)
     beam = cfg.load_beam(0, seed=2 if name == "sase" else 1)
     fields = [cfg.load_seed(h) for h in range(cfg.params.num_harmony)]
     return cfg, beam, fields
@@ -256,12 +269,7 @@ def run_felis(args, dist, rank, world):
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": W,
         "ms_per_step": ms / K, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f64", "data": "synthetic (seeded beam loader of the reference input format)",
-        "config": {"workload": f"{args.workload}: FP64 time-dependent SASE, {p.slice_n} slices x "
-                               f"{P // p.slice_n} particles, {p.nx}x{p.ny} grid, H={p.num_harmony}"
-                   if args.workload == "sase" else f"{args.workload}: FP64 static, {P} particles, {p.nx}x{p.ny} grid",
-                   "slices": p.slice_n, "particles": P, "grid": [p.nx, p.ny], "harmonics": p.num_harmony,
-                   "iterations": [W, W + K], "l2": "inputs larger than L2 (particles 403 MB, field 171 MB per pol)",
-                   "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"},
+        "config": workload_config(args.workload, p, P, W, K, world, "FP64"),
         "adi_cells_per_s": adi_cells,
         "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                      "frac": achieved / peak, "traffic": traffic, "peak_source": peak_kind,
@@ -575,10 +583,14 @@ def main():
         if rank != 0:
             return
         value, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, 20.0, threads)
+        # the config of the mixed-precision arm's line, for the same workload
+        rcfg = make_config(args.workload)
+        P = int(rcfg.beam_counts(0).sum())
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "higher_is_better": True,
             "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "config": {"workload": args.workload},
+            "config": workload_config(args.workload, rcfg.params, P, args.warmup, args.steps, args.gpus,
+                                      "mixed-precision"),
             "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
                              "sample": sample + f"; oracle build '{variant}' (reference compiler flags)"},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},

@@ -244,6 +244,15 @@ class Config:
         arrs["weights"] = w
         return arrs
 
+    def beam_counts(self, species: int = 0) -> np.ndarray:
+        """Particles per slice the loader gives this species (no particle is
+        generated, no GPU is needed; 3D beams)."""
+        counts = np.zeros(self.params.slice_n, dtype=np.int64)
+        st = _lib.felis_config_load_beam_device(self._h, species, 0, counts.ctypes.data_as(_i64p), *([None] * 7))
+        if st != OK:
+            raise FelisError(st, _lib.felis_config_error().decode())
+        return counts
+
     def load_beam_device(self, species: int = 0, seed: int = 0, device: int = 0) -> dict:
         """load_beam with the per-beamlet work on the GPU: x .. gamma as torch
         CUDA tensors (float64), offsets and weights as host arrays."""
