@@ -627,7 +627,7 @@ def main():
     else:
         line.pop("_energy", None)
     if rank == 0:
-        if args.no_cpu_baseline:
+        if args.no_cpu_baseline or world > 1:  # the host baseline is timed once, at one GPU
             line["cpu_baseline"] = None
         else:
             v, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, args.cpu_seconds, threads)
