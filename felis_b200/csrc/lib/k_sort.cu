@@ -1,4 +1,4 @@
-// Stable integer key sort of particles by slice (north-star item (a)).
+// Stable integer key sort of particles by slice.
 //
 // The reference never moves particles between slices in its live loop
 // (rearrangeParticles.cpp:7-75 is commented out); slice order matters when

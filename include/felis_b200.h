@@ -45,7 +45,7 @@ typedef enum felis_status {
   FELIS_OUT_OF_RANGE = 4,   /* theta outside [0, dTh] after the wrap (rearrangeParticles.cpp:105-108) */
   FELIS_NAN = 5,            /* non-finite value found in the particle state */
   FELIS_TIMEOUT = 6,        /* a bounded device wait gave up */
-  FELIS_UNSUPPORTED = 7,    /* configuration this build does not implement */
+  FELIS_UNSUPPORTED = 7,    /* configuration the library does not implement */
   FELIS_NO_DEVICE = 8,      /* no CUDA device */
   FELIS_IO = 9,             /* input file could not be read or parsed */
   FELIS_NOT_FOUND = 10      /* a key or block is missing from the input file */

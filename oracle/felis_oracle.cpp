@@ -1,6 +1,6 @@
 // felis_oracle.cpp — CPU restatement of FELIS's per-step slice loop.
 //
-// TEST INFRASTRUCTURE ONLY.  This file is the checker for the GPU library:
+// TEST INFRASTRUCTURE ONLY.  This file is the test oracle of the GPU library:
 // tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
 // it; the product never does.
 //
