@@ -52,13 +52,11 @@ def _run_ranks(path, world, tmp_path, engine="oracle", ckpt=None):
     return [dict(np.load(o)) for o in outs]
 
 
-@pytest.fixture(scope="module")
-def single(fb, oracle_mod, tmp_path_factory):
+def _single(fb, oracle_mod, tmp, **extra):
     from felis_b200 import workloads
 
-    tmp = tmp_path_factory.mktemp("shard")
     path = workloads.write_input(str(tmp / "s.inp"), kind="sase", slices=11, beamlets=64, per_beamlet=4, nx=21,
-                                 harmonics=(1, 3), total_length=0.2)
+                                 harmonics=(1, 3), total_length=0.2, **extra)
     cfg = fb.Config(path)
     p = cfg.params
     beam = cfg.load_beam(0, seed=2)
@@ -87,6 +85,16 @@ def single(fb, oracle_mod, tmp_path_factory):
     return res
 
 
+@pytest.fixture(scope="module")
+def single(fb, oracle_mod, tmp_path_factory):
+    return _single(fb, oracle_mod, tmp_path_factory.mktemp("shard"))
+
+
+@pytest.fixture(scope="module")
+def single_1d(fb, oracle_mod, tmp_path_factory):
+    return _single(fb, oracle_mod, tmp_path_factory.mktemp("shard1d"), dimension=1)
+
+
 def test_slice_blocks_match_the_decomposition():
     from felis_b200 import shard
 
@@ -113,6 +121,24 @@ def test_sharded_loop_equals_single_process(single, world, tmp_path):
     # the bunching factor is per block; its sums reassemble the whole-bunch value
     tot = sum(r["bsums"] for r in ranks)
     np.testing.assert_allclose(tot[:, :-1] / tot[:, -1:], single["B"], rtol=1e-11, atol=1e-14)
+
+
+def test_sharded_1d_loop_equals_single_process(single_1d, tmp_path):
+    """The 1D model (one field value per slice, harmonic and polarisation)
+    sharded over two processes: the hand-over is one value per plane."""
+    assert single_1d["shifts"] > 4
+    ranks = _run_ranks(single_1d["path"], 2, tmp_path)
+    off = single_1d["offsets"]
+    for r in ranks:
+        lo, hi = int(r["lo"]), int(r["hi"])
+        a, b = int(off[lo]), int(off[hi])
+        for k in ("x", "y", "px", "py", "theta", "gamma"):
+            assert_bits(r[k], single_1d[k][a:b], f"{k} slices {lo}:{hi}")
+        for (h, pol), U in single_1d["fields"].items():
+            assert_bits(r[f"U{h}{pol}"], U[lo:hi], f"field h{h} pol{pol} slices {lo}:{hi}")
+        np.testing.assert_allclose(r["E"], single_1d["E"], rtol=1e-12, atol=1e-300)
+    tot = sum(r["bsums"] for r in ranks)
+    np.testing.assert_allclose(tot[:, :-1] / tot[:, -1:], single_1d["B"], rtol=1e-11, atol=1e-14)
 
 
 def test_sharded_checkpoint_equals_single_process(single, tmp_path):
