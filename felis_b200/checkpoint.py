@@ -75,9 +75,10 @@ def _gather(dist, a: np.ndarray) -> np.ndarray:
 
 
 def field_meta(p) -> dict:
-    """The metadata of saveFieldHDF.cpp:67-88 from a felis_params (3D: the
-    power normalisation uses the cell area dx dy)."""
-    area = p.dx * p.dy
+    """The metadata of saveFieldHDF.cpp:67-88 from a felis_params (the power
+    normalisation uses the cell area dx dy, or in 1D the seed spot area
+    2 pi spotSigR^2)."""
+    area = 2.0 * math.pi * p.spot_sig_r * p.spot_sig_r if p.dimension == 1 else p.dx * p.dy
     coef = E_MASS * VELOCITY_C * VELOCITY_C * p.ks / E_CHARGE
     bucketZ = p.num_slice * p.lambda0
     return {

@@ -32,6 +32,13 @@ def case(fb, tmp_path):
                      total_length=0.4)
 
 
+@pytest.fixture(params=[3, 1], ids=["3d", "1d"])
+def any_case(request, fb, tmp_path):
+    """The same case in the 3D and the 1D model."""
+    return make_case(fb, tmp_path, kind="sase", slices=9, beamlets=32, per_beamlet=4, nx=21, harmonics=(1, 3),
+                     total_length=0.4, dimension=request.param)
+
+
 def _state(o, H):
     q = o.get_particles(0)
     return q, [o.get_field(h, pol)[1:-1] for h in range(H) for pol in (0, 1)]
@@ -44,10 +51,10 @@ def _same(a, b):
         assert_bits(x, y, f"plane {i}")
 
 
-def test_layout_matches_the_reference_dump(case, oracle_mod, tmp_path):
+def test_layout_matches_the_reference_dump(any_case, oracle_mod, tmp_path):
     from felis_b200 import checkpoint
 
-    cfg, beam, fields = case
+    cfg, beam, fields = any_case
     p = cfg.params
     o = _oracle(oracle_mod, cfg, beam, fields)
     o.run(0, RESTART)
@@ -62,7 +69,9 @@ def test_layout_matches_the_reference_dump(case, oracle_mod, tmp_path):
         assert_bits(f["Ux1"][:, 1::2], u.imag, "im")
         assert list(f["harmony"]) == [1, 3] and int(f["sliceN"][0]) == p.slice_n
         coef = checkpoint.E_MASS * checkpoint.VELOCITY_C ** 2 * p.ks / checkpoint.E_CHARGE
-        assert f["powerNorm"][0] == coef * coef / (2.0 * checkpoint.Z0) * (p.dx * p.dy)  # saveFieldHDF.cpp:72-75
+        # saveFieldHDF.cpp:67-72: the cell area, or in 1D the seed spot area
+        area = 2.0 * math.pi * p.spot_sig_r * p.spot_sig_r if p.dimension == 1 else (p.dx * p.dy)
+        assert f["powerNorm"][0] == coef * coef / (2.0 * checkpoint.Z0) * area
     with np.load(tmp_path / f"particle{RESTART}.npz") as f:
         rows = f["0"]
         q = o.get_particles(0)
@@ -76,10 +85,10 @@ def test_layout_matches_the_reference_dump(case, oracle_mod, tmp_path):
         assert f["dPhi"][0] == 2.0 * math.pi * p.num_slice
 
 
-def test_round_trip_is_exact(case, oracle_mod, tmp_path):
+def test_round_trip_is_exact(any_case, oracle_mod, tmp_path):
     from felis_b200 import checkpoint
 
-    cfg, beam, fields = case
+    cfg, beam, fields = any_case
     p = cfg.params
     o = _oracle(oracle_mod, cfg, beam, fields)
     o.run(0, RESTART)
@@ -93,13 +102,13 @@ def test_round_trip_is_exact(case, oracle_mod, tmp_path):
     assert_bits(beams[0]["weights"], beam["weights"], "weights")
 
 
-def test_restart_differs_only_by_the_lattice_state(case, oracle_mod, tmp_path):
+def test_restart_differs_only_by_the_lattice_state(any_case, oracle_mod, tmp_path):
     """A restart resumes from a fresh lattice state, as the reference's does
     (main.cpp:51-58 restores particles and field only); with the lattice state
     of the uninterrupted run put back, the continuation is bit-identical."""
     from felis_b200 import checkpoint
 
-    cfg, beam, fields = case
+    cfg, beam, fields = any_case
     p = cfg.params
     a = _oracle(oracle_mod, cfg, beam, fields)
     a.run(0, RESTART)
