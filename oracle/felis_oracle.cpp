@@ -4,15 +4,18 @@
 // tests/, __graft_entry__.smoke() and bench.py's CPU-baseline leg may load
 // it; the product never does.
 //
-// Parity status: UNPINNED.  The reference (scienter/felis) has no tests,
-// golden vectors or known-answer fixtures, and it cannot be compiled in this
-// environment (its sources need MPI, parallel HDF5 and GSL, none of which is
-// installed), so this restatement cannot be checked against the reference's
-// own outputs.  It is checked instead against analytic properties
-// (tests/test_oracle_*.py): the ADI against a dense solve of the same
-// tridiagonal systems, free-space diffraction of the Gaussian seed, the
-// theta-wrap edge cases, the slice sort against a stable CPU sort, and
-// energy balance between the beam and the field.
+// Parity status: PINNED to the reference itself.  oracle/_ref/felis_ref is
+// the reference's setup and step loop compiled from its unmodified sources
+// (with project-written single-rank MPI and GSL stand-ins, oracle/ref_shim/);
+// tests/test_ref_pin.py runs both builds of this restatement against it from
+// the same initial state (static, SASE, QuadPolar with harmonics 1-3, quads,
+// taper, wake, Gaussian current, 1D) and tests/test_golden_ref.py against its
+// golden outputs for config 1 complete and config 2's leading slices (1539
+// steps).  Measured differences: 1e-16 .. 4e-13 relative, from glibc's
+// sin/cos/atan versus the deterministic ones below and from the reference's
+// two-division complex quotients.  Analytic checks remain in
+// tests/test_oracle_pins.py (ADI against a dense solve, Gaussian diffraction,
+// energy balance, theta-wrap edges, the 1D gain length).
 //
 // What it restates (file:line in the reference):
 //   updateK_quadG         updateK_quadG.cpp:8-94

@@ -2,7 +2,8 @@
 
 TEST INFRASTRUCTURE ONLY: imported by tests/, __graft_entry__.smoke() and
 bench.py's CPU-baseline leg, never by the felis_b200 package.
-Parity status: unpinned (see felis_oracle.cpp).
+Parity status: pinned to the reference's own step loop (oracle/_ref,
+tests/test_ref_pin.py, tests/test_golden_ref.py; see felis_oracle.cpp).
 """
 from __future__ import annotations
 

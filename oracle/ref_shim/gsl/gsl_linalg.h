@@ -1,0 +1,5 @@
+/* Stand-in for <gsl/gsl_linalg.h> (oracle/_ref, test infrastructure): boundary.cpp
+ * includes this header but calls nothing from it, so it is empty. */
+#ifndef FELIS_REF_SHIM_GSL_LINALG_H
+#define FELIS_REF_SHIM_GSL_LINALG_H
+#endif

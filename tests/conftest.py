@@ -57,6 +57,33 @@ def make_case(fb, tmp_path, kind="sase", seed=None, **kw):
     return cfg, beam, fields
 
 
+def ref_case(fb, tmp_path, kind="sase", seed=None, **kw):
+    """make_case for a comparison with the reference (oracle/_ref): also the
+    input path, the loader seed (GSL_RNG_SEED), and the wake energy loss of
+    the loaded beam installed in the parameters (the reference computes it at
+    iteration 0 from the same slice charges, wakeField.cpp:9-50)."""
+    from felis_b200 import workloads
+
+    path = workloads.write_input(str(tmp_path / f"{kind}.inp"), kind=kind, **kw)
+    cfg = fb.Config(path)
+    seed = (1 if kind == "static" else 2) if seed is None else seed
+    beam = cfg.load_beam(0, seed=seed)
+    fields = [cfg.load_seed(h) for h in range(cfg.params.num_harmony)]
+    if cfg.params.wake_on:
+        cfg.wake(beam["weights"] * np.diff(beam["offsets"]))
+    return cfg, beam, fields, path, seed
+
+
+def rel_err(a, b) -> float:
+    """Largest absolute difference relative to the largest magnitude of b."""
+    a = np.asarray(a)
+    b = np.asarray(b)
+    assert a.shape == b.shape
+    scale = float(np.max(np.abs(b))) if b.size else 0.0
+    d = float(np.max(np.abs(a - b))) if b.size else 0.0
+    return d / scale if scale > 0 else d
+
+
 def load_both(fb, oracle_mod, cfg, beam, fields, threads=4):
     """The same initial state in a GPU handle and in the CPU restatement."""
     p = cfg.params
