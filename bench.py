@@ -117,6 +117,24 @@ def workload_config(name: str, p, P: int, W: int, K: int, world: int, precision:
             "parallelism": f"replicas x{world}" if world > 1 else "1 GPU"}
 
 
+def reference_config(name: str) -> dict:
+    """The `config` of the reference arm's line, from the workload table
+    alone (no product code is loaded on that arm)."""
+    wl = _workloads_module()
+    kw = dict(wl.WORKLOADS[name])
+    n = kw.get("nx", 101) + 1
+    if name == "sase":
+        S = kw.get("slices", 1024)
+        P = S * kw.get("beamlets", 2048) * kw.get("per_beamlet", 4)
+        what = (f"{name}: FP64 time-dependent SASE, {S} slices x {P // S} particles, {n}x{n} grid, H=1 "
+                f"(the reference's own CPU step loop; same workload as the GPU arm's line)")
+    else:
+        S, P = 1, kw.get("beamlets", 2048) * kw.get("per_beamlet", 4)
+        what = f"{name}: FP64 static, {P} particles, {n}x{n} grid (the reference's own CPU step loop)"
+    return {"workload": what, "slices": S, "particles": P, "grid": [n, n], "harmonics": 1,
+            "parallelism": "host cores, one rank of the reference's slice decomposition per core"}
+
+
 def make_workload(name: str, rank: int = 0, slices: int | None = None, grid: int | None = None):
     cfg = make_config(name, slices, grid)
     beam = cfg.load_beam(0, seed=2 if name == "sase" else 1)
@@ -155,10 +173,75 @@ def barrier(dist):
         dist.barrier()
 
 
-def cpu_sample(name: str, steps: int, warmup: int, target_s: float, threads: int):
-    """Oracle (reference CPU path restated, reference compiler flags) on a slice
-    subset of the workload; returns particle-steps/s and a description."""
+def _workloads_module():
+    """felis_b200/workloads.py loaded on its own: the reference arm writes the
+    workload's input file without importing the package (which would load
+    the product library)."""
+    import importlib.util
+
+    spec = importlib.util.spec_from_file_location("felis_workloads", os.path.join(ROOT, "felis_b200", "workloads.py"))
+    mod = importlib.util.module_from_spec(spec)
+    spec.loader.exec_module(mod)
+    return mod
+
+
+def host_cores() -> int:
+    try:
+        return len(os.sched_getaffinity(0))
+    except Exception:
+        return os.cpu_count() or 1
+
+
+def reference_cpu(name: str, warmup: int, steps: int, procs: int) -> tuple[float, str, str]:
+    """The reference's own step loop on the host cores: oracle/_ref/
+    felis_ref_fast (the reference's unmodified sources, built with its
+    makefile's flags) from the workload's input file, loading its beam with
+    its own loader.  `procs` processes each play one rank of the reference's
+    slice decomposition (boundary.cpp:33-46; loadBeam's per-rank Halton skip,
+    loadBeam.cpp:78-91), so each computes exactly its rank's share of every
+    step; the one-plane halo message of fieldShareZ.cpp:39-78 does not cross
+    processes (the stand-in MPI drops it).  Value: all ranks' particles x
+    timed iterations / the slowest rank's loop time.  Returns (value,
+    sample description, kind)."""
     sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+    from concurrent.futures import ThreadPoolExecutor
+
+    wl = _workloads_module()
+    kw = dict(wl.WORKLOADS[name])
+    d = tempfile.mkdtemp(prefix="felis_ref_bench_")
+    path = wl.write_input(os.path.join(d, f"{name}.inp"), **kw)
+    with open(path) as f:
+        slices = 1 if "mode=Static" in f.read() else kw.get("slices", 1024)
+    procs = max(1, min(procs, slices))
+    seed = 2 if name == "sase" else 1
+
+    def one(rank):
+        return refrun.run(path, it1=warmup + steps, time_warmup=warmup, final=False, variant="fast", seed=seed,
+                          ranks=(procs, rank), timeout=1800)["timing"]
+
+    with ThreadPoolExecutor(max_workers=procs) as ex:
+        timings = list(ex.map(one, range(procs)))
+    secs = max(t["seconds"] for t in timings)
+    particles = sum(t["particles"] for t in timings)
+    value = particles * steps / secs
+    sample = (f"the whole workload ({int(particles)} particles, {slices} slices), iterations {warmup}..{warmup + steps - 1} "
+              f"after {warmup} untimed, {secs:.2f} s timed (slowest of {procs} rank processes, one per host core); "
+              f"the reference's own loader, tables and step loop (oracle/_ref/felis_ref_fast: unmodified sources, "
+              f"makefile flags with -march=x86-64-v3)")
+    return value, sample, "reference"
+
+
+def cpu_sample(name: str, steps: int, warmup: int, target_s: float, threads: int):
+    """The CPU baseline: the reference's own loop (reference_cpu) when
+    oracle/_ref is built, else the restatement (reference compiler flags) on
+    a slice subset of the workload; returns (particle-steps/s, description,
+    kind)."""
+    sys.path.insert(0, os.path.join(ROOT, "oracle"))
+    import refrun
+
+    if refrun.available("fast"):
+        return reference_cpu(name, min(warmup, 3), max(1, min(steps, 20)), threads)
     import oracle
 
     import felis_b200 as fb
@@ -203,8 +286,9 @@ def cpu_sample(name: str, steps: int, warmup: int, target_s: float, threads: int
     n, dt, p = run(slices, nsteps)
     value = n * nsteps / dt
     sample = (f"{slices} of {total_slices} slices x {n // max(slices, 1)} particles, iterations "
-              f"{warmup}..{warmup + nsteps - 1} after {warmup} untimed, {dt:.1f} s timed on {threads} threads")
-    return value, sample, variant
+              f"{warmup}..{warmup + nsteps - 1} after {warmup} untimed, {dt:.1f} s timed on {threads} threads; "
+              f"CPU restatement, build '{variant}' (reference compiler flags)")
+    return value, sample, "port"
 
 
 def run_felis(args, dist, rank, world):
@@ -435,8 +519,8 @@ def run_mixed_e2e(args, cfg, beam, fields, dist):
 
 def run_ensemble(args, dist, world):
     """The 96-instance batched ensemble: aggregate throughput, and the power
-    error of a sample of instances (the smallest of each grid size) against
-    FP64 plain runs of the same iterations."""
+    error of every instance against an FP64 plain run of the same
+    iterations."""
     import numpy as np
 
     import felis_b200 as fb
@@ -454,16 +538,12 @@ def run_ensemble(args, dist, world):
     b = fb.Batch([c.params for c, _ in cfgs])
     P = 0
     cells = 0
-    sample = {}
     # beams from the device loader; no seed laser, so the fields start at zero
     for k, (c, seed) in enumerate(cfgs):
         beam = c.load_beam_device(0, seed=seed)
         _batch_upload(b, k, beam, None)
         P += int(beam["offsets"][-1])
         cells += c.params.slice_n * c.params.nx * c.params.ny * 2 * c.params.num_harmony
-        key = c.params.nx
-        if key not in sample or c.params.slice_n < cfgs[sample[key]][0].params.slice_n:
-            sample[key] = k
         del beam
     t_setup = time.perf_counter() - t_setup
     W, K = args.warmup, args.ensemble_steps
@@ -477,11 +557,10 @@ def run_ensemble(args, dist, world):
     barrier(dist)
     kinds = batch_kernels(b)
     launches, _ = b.kernel_stats(-1)
-    # per-instance power error: the same instance from the same initial state
-    # through the FP64 plain path for the same iterations
-    errs = {}
-    for nx, k in sorted(sample.items()):
-        c, seed = cfgs[k]
+    # per-instance power error, every instance: the same instance from the same
+    # initial state through the FP64 plain path for the same iterations
+    errs = []
+    for k, (c, seed) in enumerate(cfgs):
         beam = c.load_beam_device(0, seed=seed)  # the instance's initial state
         h = fb.Handle(c.params)
         h.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
@@ -492,8 +571,9 @@ def run_ensemble(args, dist, world):
         P32 = analysis.output_power(b.diagnostics(k, 0, i0 + K + 1)[0])
         ok = P64 > 0
         rel = np.abs(P32[ok] - P64[ok]) / P64[ok]
-        errs[f"instance {k} (slices {c.params.slice_n}, grid {c.params.nx})"] = float(rel.max())
+        errs.append((float(rel.max()), k, c.params.slice_n, c.params.nx))
         h.close()
+    worst = max(errs)
     threads, adi_ctas = b.launch()
     res = {
         "workload": f"{len(spec)} SASE instances (shot noise, no seed laser), slices in {{128..2048}}, "
@@ -504,10 +584,97 @@ def run_ensemble(args, dist, world):
         "steps": K, "iterations": [i0, i0 + K], "setup_s": t_setup,
         "launch": {"push_threads": threads, "adi_ctas_per_sm": adi_ctas},
         "kernels": kinds, "gpu_launches": launches,
-        "power_error_max_rel_sample": errs,
+        "power_error_vs_fp64": {
+            "instances": len(errs), "what": "per instance, the largest relative power error over iterations "
+                                            f"0..{i0 + K} against the FP64 plain path from the same initial state",
+            "max": worst[0], "median": float(np.median([e[0] for e in errs])),
+            "worst_instance": {"index": worst[1], "slices": worst[2], "grid": worst[3]},
+            "per_instance": [e[0] for e in sorted(errs, key=lambda e: e[1])]},
     }
     b.close()
     return res
+
+
+def run_config3(args, dist, world):
+    """A timed prefix of the mixed-precision long run (the Gaussian-current
+    tapered SASE workload "gaussian_taper": 4096 slices, QuadPolar with
+    polarity 0.5, harmonics 1 and 3, copper AC wake, 152 x 152 grid) through
+    the FP64 plain path and the mixed engine from the same initial state:
+    W untimed iterations, K timed from one graph each, the power error of
+    every iteration 0..W+K per harmonic.  Early iterations run faster per
+    step than the run's average (the beam and its deposit box grow along
+    the undulator; the whole 60 m is measured by python -m
+    felis_b200.longrun)."""
+    import numpy as np
+
+    import felis_b200 as fb
+    from felis_b200 import analysis, longrun
+
+    t0 = time.perf_counter()
+    cfg, beam, fields, kw = longrun.prepare("gaussian_taper")
+    p = cfg.params
+    P = int(beam["offsets"][-1])
+    cells = p.slice_n * p.nx * p.ny * 2 * p.num_harmony
+    setup_s = time.perf_counter() - t0
+    W, K = args.warmup, args.config3_steps
+    peak, peak_kind = peaks()
+
+    def timed(obj, stats_kinds, run, diag):
+        run(0, W)
+        obj.profile(True, max_launches=16 * K + 64)
+        barrier(dist)
+        run(W, W + K)
+        ms = max_over_ranks(dist, obj.last_run_ms())
+        kinds = {}
+        for name, k in stats_kinds.items():
+            n, t = obj.kernel_stats(k)
+            kinds[name] = {"launches": n, "ms": t}
+        return ms, kinds, diag(W + K + 1)
+
+    h = fb.Handle(p)
+    h.upload_particles(0, *(beam[k] for k in ("x", "y", "px", "py", "theta", "gamma")), beam["offsets"], beam["weights"])
+    ms64, k64, e64 = timed(h, fb.KERNEL_KINDS, h.run, lambda n: h.diagnostics(0, n)[0])
+    launches64, _ = h.kernel_stats(-1)
+    h.close()
+    b = fb.Batch([p])
+    _batch_upload(b, 0, beam, fields)
+    b.tune(0, 2)
+    launch = b.launch()
+    b.close()
+    b = fb.Batch([p])
+    b.set_launch(*launch)
+    _batch_upload(b, 0, beam, fields)
+    ms32, k32, e32 = timed(b, fb.BATCH_KERNEL_KINDS, b.run, lambda n: b.diagnostics(0, 0, n)[0])
+    launches32, _ = b.kernel_stats(-1)
+    b.close()
+    errs = {}
+    for hidx in range(p.num_harmony):
+        P64, P32 = analysis.output_power(e64, hidx), analysis.output_power(e32, hidx)
+        ok = P64 > 0
+        rel = np.abs(P32[ok] - P64[ok]) / P64[ok]
+        errs[f"H{p.harmony[hidx]}"] = {"max_rel": float(rel.max()) if rel.size else None,
+                                       "final_rel": float(rel[-1]) if rel.size else None}
+    dom = max(("push", "adi"), key=lambda k: k32[k]["ms"])
+    kd = k32[dom]
+    avg_ms = kd["ms"] / max(kd["launches"], 1)
+    bpl = {"push": P * BYTES_PARTICLE_STEP_MIXED, "adi": cells * BYTES_ADI_CELL_MIXED}[dom]
+    achieved = bpl / (avg_ms / 1e3) / 1e9 if avg_ms > 0 else 0.0
+    return {
+        "workload": f"gaussian_taper: {p.slice_n} slices, Gaussian current (rms 600 slices, peak 4 kA, "
+                    f"{P} particles), QuadPolar polarity 0.5, harmonics 1 and 3, copper AC wake, "
+                    f"{p.nx}x{p.ny} grid, linear taper -1 %; timed prefix of the 60 m run",
+        "particles": P, "cells_per_step": cells, "iterations": [W, W + K], "setup_s": setup_s,
+        "fp64": {"ms_per_step": ms64 / K, "value": P * K * world / (ms64 / 1e3),
+                 "adi_cells_per_s": cells * K * world / (ms64 / 1e3), "kernels": k64, "gpu_launches": launches64},
+        "mixed": {"ms_per_step": ms32 / K, "value": P * K * world / (ms32 / 1e3),
+                  "adi_cells_per_s": cells * K * world / (ms32 / 1e3), "kernels": k32, "gpu_launches": launches32,
+                  "launch": {"push_threads": launch[0], "adi_ctas_per_sm": launch[1]},
+                  "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
+                               "frac": achieved / peak, "peak_source": peak_kind, "bytes_per_launch": bpl,
+                               "mean_launch_ms": avg_ms}},
+        "speedup_mixed_vs_fp64": ms64 / ms32,
+        "power_error_vs_fp64": errs,
+    }
 
 
 def run_e2e(args, cfg, beam, fields, dist):
@@ -572,27 +739,24 @@ def main():
     ap.add_argument("--grid", type=int, default=None, help="grid key nx = ny of the workload (profiling captures)")
     ap.add_argument("--ensemble", type=int, default=96, help="instances of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--config3-steps", type=int, default=20,
+                    help="timed iterations of the Gaussian-current tapered run (0: skip)")
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
-    threads = os.cpu_count() or 1
 
     if args.impl == "reference":
         rank = int(os.environ.get("RANK", "0"))
         if rank != 0:
             return
-        value, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, 20.0, threads)
-        # the config of the mixed-precision arm's line, for the same workload
-        rcfg = make_config(args.workload)
-        P = int(rcfg.beam_counts(0).sum())
+        cores = host_cores()
+        value, sample, kind = cpu_sample(args.workload, args.steps, args.warmup, 20.0, cores)
         print(json.dumps({
             "impl": "reference", "metric": METRIC, "value": value, "unit": UNIT, "higher_is_better": True,
-            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup,
-            "config": workload_config(args.workload, rcfg.params, P, args.warmup, args.steps, args.gpus,
-                                      "mixed-precision"),
-            "cpu_baseline": {"value": value, "unit": UNIT, "cores": threads, "kind": "port",
-                             "sample": sample + f"; oracle build '{variant}' (reference compiler flags)"},
+            "n_gpus": args.gpus, "steps": args.steps, "warmup": args.warmup, "dtype": "f64",
+            "config": reference_config(args.workload),
+            "cpu_baseline": {"value": value, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample},
             "e2e": {"value": value, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
         }), flush=True)
         return
@@ -607,6 +771,7 @@ def main():
         e2e = run_mixed_e2e(args, cfg, beam, fields, dist)
         del beam, fields
         ens = run_ensemble(args, dist, world) if args.ensemble > 0 else None
+        c3 = run_config3(args, dist, world) if args.config3_steps > 0 else None
         for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
                   "data", "cpu_baseline"):
             fp64.pop(k, None)
@@ -622,7 +787,7 @@ def main():
             "power_error_vs_fp64": mixed["power_error"],
             "roofline": mixed["roofline"], "step_roofline": mixed["step_roofline"],
             "kernels": mixed["kernels"], "gpu_launches": mixed["gpu_launches"], "clocks": mixed["clocks"],
-            "launch": mixed["launch"], "e2e": e2e, "fp64_plain": fp64, "ensemble": ens,
+            "launch": mixed["launch"], "e2e": e2e, "fp64_plain": fp64, "ensemble": ens, "config3": c3,
         }
     else:
         line.pop("_energy", None)
@@ -630,9 +795,17 @@ def main():
         if args.no_cpu_baseline or world > 1:  # the host baseline is timed once, at one GPU
             line["cpu_baseline"] = None
         else:
-            v, sample, variant = cpu_sample(args.workload, args.steps, args.warmup, args.cpu_seconds, threads)
-            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": threads, "kind": "port",
-                                    "sample": sample + f"; oracle build '{variant}' (reference compiler flags)"}
+            cores = host_cores()
+            v, sample, kind = cpu_sample(args.workload, 5, 2, args.cpu_seconds, cores)
+            line["cpu_baseline"] = {"value": v, "unit": UNIT, "cores": cores, "kind": kind, "sample": sample}
+            if "fp64_plain" in line:
+                fp = line["fp64_plain"]
+                line["precision_matched"] = {
+                    "what": "FP64 against FP64: the GPU's FP64 plain path over the reference's own CPU loop "
+                            "(cpu_baseline), device-timed and end to end",
+                    "fp64_gpu_value": fp["value"], "fp64_gpu_e2e": fp["e2e"]["value"], "cpu_reference_fp64": v,
+                    "ratio_device": fp["value"] / v, "ratio_e2e": fp["e2e"]["value"] / v,
+                    "mixed_over_cpu_reference_fp64": line["value"] / v}
         print(json.dumps(line), flush=True)
     if dist is not None:
         dist.destroy_process_group()

@@ -145,6 +145,7 @@ _sig("felis_mlp_forward", C.c_int, _vp, _fp, C.c_int64, _fp)
 _sig("felis_mlp_gradients", C.c_int, _vp, _fp, _fp, C.c_int64, _fp, _dp)
 _sig("felis_mlp_set_data", C.c_int, _vp, _fp, _fp, C.c_int64)
 _sig("felis_mlp_train", C.c_int, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64, _dp)
+_sig("felis_wait_selftest", C.c_int, C.c_int32, _i32p)
 _sig("felis_config_load", C.c_int, C.c_char_p, C.c_int32, C.c_int32, C.POINTER(_vp))
 _sig("felis_config_free", None, _vp)
 _sig("felis_config_params", C.POINTER(Params), _vp)
@@ -699,6 +700,14 @@ class MLP:
         hist = np.zeros(epochs)
         self._ck(_lib.felis_mlp_train(self._m, epochs, batch, lr, weight_decay, seed, _p(hist)))
         return hist
+
+
+def wait_selftest(limit: int = 1000) -> int:
+    """The library's bounded device wait on a barrier phase that nothing
+    completes (felis_wait_selftest): returns the status (FELIS_TIMEOUT when
+    the wait gave up as designed)."""
+    out = C.c_int32(0)
+    return _lib.felis_wait_selftest(limit, C.byref(out))
 
 
 def device_info() -> tuple[str, int]:

@@ -801,7 +801,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
 #pragma unroll
     for (int h = 0; h < HM; ++h) { bre[h] = 0.0; bim[h] = 0.0; }
     double wsum = 0.0;
-    int bad_over = 0, bad_range = 0, bad_nan = 0;
+    int bad_over = 0, bad_range = 0, bad_nan = 0, bad_radial = 0;
     // the next particle's state is loaded one iteration ahead
     float nxv = 0.f, nyv = 0.f, npx = 0.f, npy = 0.f, ndg = 0.f;
     double nth = 0.0;
@@ -880,6 +880,10 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
                 Em[l] = cad(Em[l], cad(cs(a0, wr0), cs(a1, wr1)));
               }
             }
+          } else {
+            // beyond the radial Ez grid: the reference reuses the previous
+            // particle's Em there (particlePush.cpp:286-304); flagged
+            bad_radial = 1;
           }
           // RK4 in z of (theta, gamma); the theta slope in FP32 relative to
           // the resonance (BStep), theta itself accumulated in FP64
@@ -953,6 +957,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     if (bad_over) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
     if (bad_range) atomicOr(I.err + ERR_OUT_OF_RANGE, 1);
     if (bad_nan) atomicOr(I.err + ERR_NAN, 1);
+    if (bad_radial) atomicOr(I.err + ERR_RADIAL, 1);
     double* out = I.part_b + (size_t)s * stride;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {

@@ -45,8 +45,8 @@ __device__ __forceinline__ void cp_async16(uint32_t dst, const void* src) {
 }
 
 // Bounded wait for the phase `parity` of an mbarrier; false when it ran out.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
-  for (int it = 0; it < kWaitLimit; ++it) {
+__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, int limit = kWaitLimit) {
+  for (int it = 0; it < limit; ++it) {
     uint32_t done;
     asm volatile(
         "{\n\t.reg .pred p;\n\t"
@@ -58,6 +58,22 @@ __device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity) {
     if (done) return true;
   }
   return false;
+}
+
+// The bounded wait on an mbarrier that nothing arrives on: phase 0 never
+// completes, so every thread's wait runs out after `limit` tries and the
+// kernel records that, then returns with nothing in flight.
+__global__ void __launch_bounds__(128) k_wait_selftest(int limit, int* timed_out) {
+  __shared__ __align__(8) uint64_t bar;
+  const uint32_t b = smem_u32(&bar);
+  if (threadIdx.x == 0) {
+    asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(b) : "memory");
+    asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  }
+  __syncthreads();
+  const bool done = mbar_wait(b, 0u, limit);
+  const int all_ran_out = __syncthreads_and(done ? 0 : 1);
+  if (threadIdx.x == 0) *timed_out = all_ran_out;
 }
 
 __device__ __forceinline__ float gelu(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
@@ -286,6 +302,10 @@ void launch_col_sum(const bf16* in, int rows, int cols, float* out, cudaStream_t
 void launch_adamw(float* w, const float* g, float* m, float* v, bf16* w_bf16, int64_t n, float lr, float b1,
                   float b2, float eps, float wd, float bc1, float bc2, cudaStream_t st) {
   if (n > 0) k_adamw<<<grid_for(n), 256, 0, st>>>(w, g, m, v, w_bf16, n, lr, b1, b2, eps, wd, bc1, bc2);
+}
+
+void launch_wait_selftest(int limit, int* timed_out, cudaStream_t st) {
+  k_wait_selftest<<<1, 128, 0, st>>>(limit, timed_out);
 }
 
 }  // namespace felis

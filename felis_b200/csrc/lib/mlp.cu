@@ -444,4 +444,21 @@ felis_status felis_mlp_train(felis_mlp* m, int32_t epochs, int32_t batch, float 
   return check_err(m);
 }
 
+felis_status felis_wait_selftest(int32_t limit, int32_t* timed_out) {
+  if (limit < 1 || !timed_out) return FELIS_BAD_ARG;
+  int* d = nullptr;
+  cudaError_t e = cudaMalloc(&d, sizeof(int));
+  if (e == cudaSuccess) e = cudaMemset(d, 0, sizeof(int));
+  if (e == cudaSuccess) {
+    launch_wait_selftest(limit, d, 0);
+    e = cudaGetLastError();
+  }
+  int h = 0;
+  if (e == cudaSuccess) e = cudaMemcpy(&h, d, sizeof(int), cudaMemcpyDeviceToHost);
+  if (d) cudaFree(d);
+  if (e != cudaSuccess) return FELIS_CUDA_ERROR;
+  *timed_out = h;
+  return h ? FELIS_TIMEOUT : FELIS_OK;
+}
+
 }  // extern "C"

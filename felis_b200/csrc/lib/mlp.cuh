@@ -55,4 +55,9 @@ void launch_col_sum(const bf16* in, int rows, int cols, float* out, cudaStream_t
 void launch_adamw(float* w, const float* g, float* m, float* v, bf16* w_bf16, int64_t n, float lr, float b1,
                   float b2, float eps, float wd, float bc1, float bc2, cudaStream_t st);
 
+// The library's bounded mbarrier wait (the one the GEMM uses) on a barrier
+// phase that nothing completes: *timed_out = 1 when every thread's wait gave
+// up after `limit` tries.
+void launch_wait_selftest(int limit, int* timed_out, cudaStream_t st);
+
 }  // namespace felis

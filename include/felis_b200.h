@@ -354,6 +354,14 @@ felis_status felis_batch_kernel_stats(felis_batch* b, int32_t kind, int64_t* lau
  * n_in <= 256, n_out <= width.  Inputs and outputs are row-major FP32 host
  * arrays, [n][n_in] and [n][n_out]; the loss is the mean squared error over
  * all outputs (normalise the targets beforehand). */
+/* Self-test of the bounded device wait that guards the tensor-core pipeline
+ * (no reference counterpart: the reference has no device waits).  Runs the
+ * library's mbarrier wait, `limit` tries, on a barrier phase that nothing
+ * completes, on the current device: returns FELIS_TIMEOUT with *timed_out = 1
+ * when the wait gave up as designed (the context stays usable), FELIS_OK with
+ * *timed_out = 0 if it did not. */
+felis_status felis_wait_selftest(int32_t limit, int32_t* timed_out);
+
 typedef struct felis_mlp felis_mlp;
 felis_status felis_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64_t seed, felis_mlp** out);
 void felis_mlp_destroy(felis_mlp* m);
