@@ -24,7 +24,7 @@ _lib = C.CDLL(LIB_PATH)
 
 MAX_HARMONY = 8
 MAX_SPECIES = 8
-ABI_VERSION = 2
+ABI_VERSION = 3
 
 OK, BAD_ARG, CUDA_ERROR, THETA_OVERFLOW, OUT_OF_RANGE, NAN, TIMEOUT, UNSUPPORTED, NO_DEVICE, IO, NOT_FOUND = range(11)
 STATUS_NAMES = {0: "OK", 1: "BAD_ARG", 2: "CUDA_ERROR", 3: "THETA_OVERFLOW", 4: "OUT_OF_RANGE", 5: "NAN",
@@ -71,6 +71,8 @@ class Params(C.Structure):
         ("bessel", _dp), ("wake_e", _dp),
         ("undulators", C.POINTER(Undulator)), ("quads", C.POINTER(Quad)),
         ("beam_area", C.c_double * 8),
+        ("num_phase_shifts", C.c_int32), ("pad_ps_", C.c_int32),
+        ("phase_shift_z", _dp), ("phase_shift_phase", _dp),
     ]
 
 
@@ -104,7 +106,7 @@ _sig("felis_set_lattice", C.c_int, _vp, C.POINTER(Lattice))
 for _n in ("felis_update_total_energy", "felis_twiss", "felis_bfactor"):
     _sig(_n, C.c_int, _vp, C.c_int32, _dp)
 for _n in ("felis_solve_field", "felis_transverse_push", "felis_push_theta_gamma", "felis_drift_theta_gamma",
-           "felis_periodic_particles", "felis_shift_field", "felis_step"):
+           "felis_periodic_particles", "felis_phase_shift", "felis_shift_field", "felis_step"):
     _sig(_n, C.c_int, _vp, C.c_int32)
 _sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_set_slice_exchange", C.c_int, _vp, C.c_int32)
@@ -435,6 +437,9 @@ class Handle:
     def drift_theta_gamma(self, it: int = 0):
         self._ck(_lib.felis_drift_theta_gamma(self._h, it))
 
+    def phase_shift(self, it: int = 0):
+        self._ck(_lib.felis_phase_shift(self._h, it))
+
     def periodic_particles(self, it: int = 0):
         self._ck(_lib.felis_periodic_particles(self._h, it))
 
@@ -511,6 +516,7 @@ class Handle:
                 self.push_theta_gamma(it)
             else:
                 self.drift_theta_gamma(it)
+            self.phase_shift(it)
             self.periodic_particles(it)
             if not lat.drift_flag and self.mode == TIME_DEPENDENT:
                 self.shift_field(it)

@@ -254,9 +254,9 @@ struct felis_config {
   double Lz = 0;
   int saveStep = 0, saveStart = 0;
   bool fieldSave = true, particleSave = true;
-  // [Phase_shifter] (README.md:57-70; not read by the reference's parser)
-  int ps_number = 0;
-  double ps_start = 0, ps_interval = 0, ps_phase = 0;
+  // [Phase_shifter] blocks (README.md:57-70; not read by the reference's
+  // parser): every shifter's position [m] and phase [pi]
+  std::vector<double> ps_z, ps_phase;
 };
 
 extern "C" const char* felis_config_error(void) { return g_err.c_str(); }
@@ -688,10 +688,21 @@ felis_status load_config(felis_config* c) {
   OPT("Wake_field", 1, "conductivity", to_dbl, c->cond, 3.03e7);
   if (c->acdc == 1) { OPT("Wake_field", 1, "ctau", to_dbl, c->ctau, 2.4e-6); }
   else c->ctau = 0.0;
-  OPT("Phase_shifter", 1, "number", to_int, c->ps_number, 0);
-  OPT("Phase_shifter", 1, "start_position", to_dbl, c->ps_start, 0.0);
-  OPT("Phase_shifter", 1, "interval_length", to_dbl, c->ps_interval, 0.0);
-  OPT("Phase_shifter", 1, "phase", to_dbl, c->ps_phase, 0.0);
+  // every [Phase_shifter] block: `number` shifters at start_position +
+  // k interval_length, each delaying the electrons by `phase` pi
+  for (int rank = 1;; ++rank) {
+    int number = 0;
+    double start = 0, interval = 0, phase = 0;
+    OPT("Phase_shifter", rank, "number", to_int, number, 0);
+    if (number <= 0) break;
+    OPT("Phase_shifter", rank, "start_position", to_dbl, start, 0.0);
+    OPT("Phase_shifter", rank, "interval_length", to_dbl, interval, 0.0);
+    OPT("Phase_shifter", rank, "phase", to_dbl, phase, 0.0);
+    for (int k = 0; k < number; ++k) {
+      c->ps_z.push_back(start + k * interval);
+      c->ps_phase.push_back(phase);
+    }
+  }
 
   // boundary.cpp:33-46: contiguous slice blocks per rank
   {
@@ -734,6 +745,9 @@ felis_status load_config(felis_config* c) {
   p.num_quads = (int)c->quad_c.size();
   p.undulators = c->und_c.data();
   p.quads = c->quad_c.empty() ? nullptr : c->quad_c.data();
+  p.num_phase_shifts = (int32_t)c->ps_z.size();
+  p.phase_shift_z = c->ps_z.empty() ? nullptr : c->ps_z.data();
+  p.phase_shift_phase = c->ps_phase.empty() ? nullptr : c->ps_phase.data();
   return FELIS_OK;
 }
 

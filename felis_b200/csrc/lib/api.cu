@@ -57,6 +57,7 @@ struct felis_handle {
   felis_lattice lat{};
   std::vector<HostUnd> und;
   std::vector<HostQuad> quad;
+  std::vector<double> ps_z, ps_phase;  // [Phase_shifter] positions [m] and phases [pi]
   // particles
   std::vector<int64_t> counts;   // [nspecies]
   std::vector<int64_t> soff;     // [nspecies][S+1] absolute
@@ -400,9 +401,15 @@ felis_status ensure_ready(felis_handle* h) {
   return FELIS_OK;
 }
 
-felis_status run_particles(felis_handle* h, unsigned ops, const felis_lattice* l0, const felis_lattice* l1) {
+double theta_shift(const felis_handle* h, int it) {
+  return phase_shift_of((int)h->ps_z.size(), h->ps_z.data(), h->ps_phase.data(), it, h->p.dz);
+}
+
+felis_status run_particles(felis_handle* h, unsigned ops, const felis_lattice* l0, const felis_lattice* l1,
+                           double shift = 0.0) {
   ParticleLaunch a = base_launch(h);
   a.ops = ops;
+  a.theta_shift = shift;
   if (ops & OP_T0)
     if (!trans_coef(h, *l0, &a.t0)) return fail(h, FELIS_BAD_ARG, "transversePush: no undulator_mode");
   if (ops & OP_T1)
@@ -663,6 +670,13 @@ felis_status felis_create(const felis_params* p, felis_handle** out) {
     o.g.assign(Q.g, Q.g + Q.numbers);
     h->quad.push_back(o);
   }
+  if (p->num_phase_shifts > 0) {
+    h->ps_z.assign(p->phase_shift_z, p->phase_shift_z + p->num_phase_shifts);
+    h->ps_phase.assign(p->phase_shift_phase, p->phase_shift_phase + p->num_phase_shifts);
+  }
+  h->p.num_phase_shifts = (int32_t)h->ps_z.size();
+  h->p.phase_shift_z = nullptr;
+  h->p.phase_shift_phase = nullptr;
   h->p.undulators = nullptr;
   h->p.quads = nullptr;
   h->bessel_host.assign(p->bessel, p->bessel + (size_t)p->bessel_rows * p->bessel_cols);
@@ -1130,6 +1144,18 @@ felis_status felis_drift_theta_gamma(felis_handle* h, int32_t it) {
   return check_err(h);
 }
 
+felis_status felis_phase_shift(felis_handle* h, int32_t it) {
+  if (!h) return FELIS_BAD_ARG;
+  felis_status s = ensure_ready(h);
+  if (s != FELIS_OK) return s;
+  const double dth = theta_shift(h, it);
+  if (dth == 0.0) return FELIS_OK;
+  s = run_particles(h, OP_PHASE, nullptr, nullptr, dth);
+  if (s != FELIS_OK) return s;
+  invalidate_particles(h);
+  return check_err(h);
+}
+
 felis_status felis_periodic_particles(felis_handle* h, int32_t it) {
   if (!h) return FELIS_BAD_ARG;
   (void)it;
@@ -1174,7 +1200,8 @@ static felis_status step_impl_1d(felis_handle* h, int it) {
     s = run_1d_push(h, l1);
     if (s != FELIS_OK) return s;
   }
-  s = run_particles(h, OP_WRAP, nullptr, nullptr);
+  const double dth = theta_shift(h, it);
+  s = run_particles(h, dth != 0.0 ? (OP_PHASE | OP_WRAP) : OP_WRAP, nullptr, nullptr, dth);
   if (s != FELIS_OK) return s;
   h->prep_valid = false;
   if (!l1.drift_flag && h->p.mode == FELIS_TIME_DEPENDENT) {
@@ -1214,7 +1241,9 @@ static felis_status step_impl(felis_handle* h, int it) {
   unsigned ops = OP_T0 | OP_T1 | OP_WRAP | OP_DIAG;
   ops |= l1.drift_flag ? OP_DRIFT : OP_PUSH;
   if (l1.current_flag) ops |= OP_PREP;
-  s = run_particles(h, ops, &l0, &l1);
+  const double dth = theta_shift(h, it);
+  if (dth != 0.0) ops |= OP_PHASE;
+  s = run_particles(h, ops, &l0, &l1, dth);
   if (s != FELIS_OK) return s;
   h->prep_valid = l1.current_flag != 0;
   const bool shift = !l1.drift_flag && h->p.mode == FELIS_TIME_DEPENDENT;

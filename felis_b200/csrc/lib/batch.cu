@@ -40,6 +40,7 @@ struct Inst {
   felis_params p{};
   std::vector<HUnd> und;
   std::vector<HQuad> quad;
+  std::vector<double> ps_z, ps_phase;  // [Phase_shifter] positions [m] and phases [pi]
   felis_lattice lat{};
   int ring_base = 0;
   int64_t count = 0;
@@ -480,6 +481,7 @@ felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& o
       T.current = dl.current_flag;
       T.drift = l1.drift_flag;
       T.shift = !l1.drift_flag && p.mode == FELIS_TIME_DEPENDENT;
+      T.theta_shift = phase_shift_of((int)I.ps_z.size(), I.ps_z.data(), I.ps_phase.data(), it, p.dz);
       if (T.shift) I.ring_base = (I.ring_base - 1 + p.slice_n) % p.slice_n;
       if (l0.und_type != FELIS_BIPOLAR && l0.und_type != FELIS_QUADPOLAR) return bfail(b, FELIS_BAD_ARG, "no undulator_mode");
       transverse_maps(I, l0, l1, T);
@@ -708,6 +710,13 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
       o.g.assign(Q.g, Q.g + Q.numbers);
       I.quad.push_back(o);
     }
+    if (p->num_phase_shifts > 0) {
+      I.ps_z.assign(p->phase_shift_z, p->phase_shift_z + p->num_phase_shifts);
+      I.ps_phase.assign(p->phase_shift_phase, p->phase_shift_phase + p->num_phase_shifts);
+    }
+    I.p.num_phase_shifts = (int32_t)I.ps_z.size();
+    I.p.phase_shift_z = nullptr;
+    I.p.phase_shift_phase = nullptr;
     I.lat.K0 = p->K0_init; I.lat.ue = p->ue_init; I.lat.lambdaU = p->lambdaU_init;
     I.lat.ku = 2.0 * M_PI / p->lambdaU_init; I.lat.K0_alpha = p->K0_alpha_init; I.lat.und_type = p->und_type_init;
     I.bessel.assign(p->bessel, p->bessel + (size_t)p->bessel_rows * p->bessel_cols);

@@ -73,6 +73,7 @@ struct BStep {
   // R0 = ku - A0 Q0 and AQ0 = A0 Q0 formed in FP64 on the host.
   float R0, A0, AQ0, c1, c2, K0, ue, K0a, Phi_half, cxi, sq, ksK0, e_mc2, dPhi;
   double ku, A0d;  // drift: theta += (ku - A0d (1 + px^2 + py^2 + sumU2)) dz, FP64
+  double theta_shift;  // [Phase_shifter] delay added to theta before the wrap
   float2 etaX, etaY;
   BDep dep;       // deposit done by this launch
   float2 sfac[FELIS_MAX_HARMONY][2];  // ADI source factor per harmonic and polarisation

@@ -2,6 +2,7 @@
 #pragma once
 
 #include <cuda_runtime.h>
+#include <math.h>
 #include <stdint.h>
 
 #include "../detmath.h"
@@ -16,6 +17,17 @@ namespace felis {
 #define K_ECHARGE 1.60217662e-19
 #define K_MC2 0.510998918
 #define K_Z0 376.730313668
+
+// [Phase_shifter] (README.md:57-70): the theta delay of iteration it, minus
+// pi times the phases of the shifters at z in [it dz, (it+1) dz), summed in
+// list order; 0 when none sits in that step.
+inline double phase_shift_of(int n, const double* z, const double* phase, int it, double dz) {
+  double d = 0.0;
+  const double z0 = it * dz, z1 = (it + 1) * dz;
+  for (int k = 0; k < n; ++k)
+    if (z[k] >= z0 && z[k] < z1) d -= M_PI * phase[k];
+  return d;
+}
 
 // ---- complex arithmetic ----------------------------------------------------
 // Same operand order as std::complex<double> in the reference; division is

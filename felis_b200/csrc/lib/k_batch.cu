@@ -768,6 +768,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     const double dz = I.dz;
     const float dwake = (float)(dz * wakeE);
     const double dTh = I.numSlice * 2 * M_PI, idTh = 1.0 / dTh;
+    const double thshift = T.theta_shift;
     const float dzf = (float)dz;
     const float2* __restrict__ Ubase = I.U + (size_t)plane * N;
     const size_t hpstride = (size_t)S * N;
@@ -930,6 +931,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
           th -= dz * wakeE;
         }
       }
+      th += thshift;  // [Phase_shifter] (0 when no shifter sits in this step)
       // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
       if (th >= dTh || th < 0) {
         th -= dTh * floor(th * idTh);

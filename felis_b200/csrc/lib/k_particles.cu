@@ -371,11 +371,12 @@ __global__ void __launch_bounds__(256) k_particles(ParticleLaunch a) {
     if (ops & OP_T1) transverse_one(a.t1, x, y, px, py, ga);
     if (ops & OP_PUSH) push_one(a, s, wakeE, x, y, px, py, th, ga);
     else if (ops & OP_DRIFT) drift_one(a, s, wakeE, x, y, px, py, th);
+    if (ops & OP_PHASE) th += a.theta_shift;
     if (ops & OP_WRAP) wrap_one(G.numSlice * 2 * M_PI, th, a.err);
     if (ops & (OP_T0 | OP_T1)) {
       a.P.x[n] = x; a.P.y[n] = y; a.P.px[n] = px; a.P.py[n] = py;
     }
-    if (ops & (OP_PUSH | OP_DRIFT | OP_WRAP)) a.P.th[n] = th;
+    if (ops & (OP_PUSH | OP_DRIFT | OP_PHASE | OP_WRAP)) a.P.th[n] = th;
     if (ops & OP_PUSH) a.P.ga[n] = ga;
     if (!(x - x == 0.0) || !(y - y == 0.0) || !(th - th == 0.0) || !(ga - ga == 0.0)) set_flag(a.err, ERR_NAN);
     if (ops & OP_PREP) prep_one(a, n, macro, x, y, px, py, th, ga);

@@ -20,6 +20,7 @@
 #include <stdint.h>
 #include <stdio.h>
 
+#include <cuda.h>
 #include <mutex>
 #include <vector>
 
@@ -180,9 +181,43 @@ constexpr size_t kNaBytes = (size_t)4 * kNaMax * 4 + (size_t)256 * kNaTiles * 4;
 
 static __device__ __align__(256) unsigned char g_sort_scratch[kNaBytes];
 
-// Device address of g_sort_scratch per device, resolved once per device.
+// Device address of g_sort_scratch per CUDA context.  The address belongs to
+// the context that loaded the module: it is resolved again on every call made
+// outside stream capture (so a context recreated after cudaDeviceReset, or
+// another context made current on the device, gets its own), and a call made
+// during capture uses the address last resolved in the current context.
 std::mutex g_na_mu;
-void* g_na_ptr[64] = {nullptr};
+struct NaEntry {
+  CUcontext ctx;
+  void* ptr;
+};
+NaEntry g_na_cache[64];
+int g_na_count = 0;
+typedef CUresult (*CtxGetCurrentFn)(CUcontext*);
+CtxGetCurrentFn g_ctx_get_current = nullptr;
+
+CUcontext current_context() {
+  if (!g_ctx_get_current) {
+    void* fn = nullptr;
+    cudaDriverEntryPointQueryResult q;
+    if (cudaGetDriverEntryPoint("cuCtxGetCurrent", &fn, cudaEnableDefault, &q) != cudaSuccess ||
+        q != cudaDriverEntryPointSuccess || !fn)
+      return nullptr;
+    g_ctx_get_current = reinterpret_cast<CtxGetCurrentFn>(fn);
+  }
+  CUcontext c = nullptr;
+  return g_ctx_get_current(&c) == CUDA_SUCCESS ? c : nullptr;
+}
+
+// Caller-owned buffers must be device (or managed) memory of device `dev`.
+bool on_device(const void* p, int dev) {
+  cudaPointerAttributes a;
+  if (cudaPointerGetAttributes(&a, p) != cudaSuccess) {
+    cudaGetLastError();
+    return false;
+  }
+  return (a.type == cudaMemoryTypeDevice || a.type == cudaMemoryTypeManaged) && a.device == dev;
+}
 
 __global__ void k_iota32(int32_t* v, int64_t n) {
   for (int64_t i = (int64_t)blockIdx.x * blockDim.x + threadIdx.x; i < n; i += (int64_t)gridDim.x * blockDim.x)
@@ -245,20 +280,41 @@ extern "C" felis_status felis_sort_by_slice_noalloc(const int32_t* keys_dev, int
   }
   if (n == 0) return FELIS_OK;
   int dev = 0;
-  if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) return FELIS_NO_DEVICE;
+  if (cudaGetDevice(&dev) != cudaSuccess) return FELIS_NO_DEVICE;
+  cudaStream_t st = static_cast<cudaStream_t>(stream);
+  cudaStreamCaptureStatus cap = cudaStreamCaptureStatusNone;
+  if (cudaStreamIsCapturing(st, &cap) != cudaSuccess) return FELIS_CUDA_ERROR;
+  const bool capturing = cap != cudaStreamCaptureStatusNone;
+  if (!capturing && (!on_device(keys_dev, dev) || !on_device(perm_dev, dev))) {
+    fprintf(stderr, "felis_sort_by_slice_noalloc: keys_dev and perm_dev must be device memory of the current "
+                    "device (%d)\n", dev);
+    return FELIS_BAD_ARG;
+  }
   void* base = nullptr;
   {
     std::lock_guard<std::mutex> lock(g_na_mu);
-    if (!g_na_ptr[dev]) {
-      // first call on this device: resolve the array's device address (the
-      // host-side symbol is only a stand-in, not a device address)
+    const CUcontext ctx = current_context();
+    if (!ctx) return FELIS_CUDA_ERROR;
+    int slot = -1;
+    for (int i = 0; i < g_na_count; ++i)
+      if (g_na_cache[i].ctx == ctx) slot = i;
+    if (!capturing) {
+      // resolve the array's device address in this context (the host-side
+      // symbol is only a stand-in, not a device address)
       void* p = nullptr;
       if (cudaGetSymbolAddress(&p, g_sort_scratch) != cudaSuccess || !p) return FELIS_CUDA_ERROR;
-      g_na_ptr[dev] = p;
+      if (slot < 0) {
+        if (g_na_count == 64) return FELIS_UNSUPPORTED;
+        slot = g_na_count++;
+        g_na_cache[slot].ctx = ctx;
+      }
+      g_na_cache[slot].ptr = p;
+    } else if (slot < 0) {
+      fprintf(stderr, "felis_sort_by_slice_noalloc: the first call in a context must come before stream capture\n");
+      return FELIS_BAD_ARG;
     }
-    base = g_na_ptr[dev];
+    base = g_na_cache[slot].ptr;
   }
-  cudaStream_t st = static_cast<cudaStream_t>(stream);
   int32_t* K0 = reinterpret_cast<int32_t*>(base);
   int32_t* K1 = K0 + kNaMax;
   int32_t* V0 = K1 + kNaMax;

@@ -8,8 +8,9 @@ namespace felis {
 
 // Operation bits of one particle-kernel launch.  A launch applies, in this
 // order: transverse push with t0, transverse push with t1, push_theta_gamma
-// or drift, theta wrap, deposit records for the next solveField, and the
-// twiss / bFactor partial sums of the resulting state.
+// or drift, the phase shifter's theta delay, theta wrap, deposit records for
+// the next solveField, and the twiss / bFactor partial sums of the resulting
+// state.
 enum ParticleOps : unsigned {
   OP_T0 = 1u << 0,
   OP_T1 = 1u << 1,
@@ -17,7 +18,8 @@ enum ParticleOps : unsigned {
   OP_DRIFT = 1u << 3,
   OP_WRAP = 1u << 4,
   OP_PREP = 1u << 5,
-  OP_DIAG = 1u << 6
+  OP_DIAG = 1u << 6,
+  OP_PHASE = 1u << 7
 };
 
 // particlePush.cpp:42-68 scalars of one transversePush call.
@@ -51,6 +53,7 @@ struct ParticleLaunch {
   DevDeposit dep;
   double* diag;       // [ntiles][diag_stride]
   int diag_stride;
+  double theta_shift;  // OP_PHASE: added to theta before the wrap
   int* err;
 };
 

@@ -44,7 +44,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
                noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
                linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
                in_air: bool = True, k_list=None, sigma_slices: float | None = None, profile_nodes: int = 65,
-               K_und: float | None = None, dimension: int = 3) -> str:
+               K_und: float | None = None, dimension: int = 3, phase_shifters=()) -> str:
     """Input text of one workload.  `sigma_slices` switches the flat-top
     current to a Gaussian of that rms length (in slices) centred on the bunch,
     written as a `profile_nodes`-node Polygon so that the energy-spread nodes
@@ -52,7 +52,9 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
     the photon energy by the planar resonance; `K_und` (default K0) is the
     undulator's K, e.g. K0 / sqrt(1 + polarity^2) for an elliptical undulator
     on the same resonance (parameterSetting.cpp's default K0).  `dimension` 1
-    selects the 1D model (the grid collapses to one cell per slice)."""
+    selects the 1D model (the grid collapses to one cell per slice).
+    `phase_shifters` lists [Phase_shifter] blocks as (number, start_position
+    [m], interval_length [m], phase [pi]) tuples (README.md:57-70)."""
     static = kind == "static"
     if noise is None:
         noise = not static
@@ -91,7 +93,15 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  quad_end = 5.7
  g = -10
 """
+    ps_blocks = "".join(f"""
+[Phase_shifter]
+ number={n}
+ start_position={z0!r}
+ interval_length={dzs!r}
+ phase={ph!r}
+""" for n, z0, dzs, ph in phase_shifters)
     return f"""// generated by felis_b200.workloads ({kind})
+{ps_blocks}
 [Save]
  field_save=OFF
  particle_save=OFF

@@ -33,7 +33,7 @@
 extern "C" {
 #endif
 
-#define FELIS_ABI_VERSION 2
+#define FELIS_ABI_VERSION 3
 #define FELIS_MAX_HARMONY 8
 #define FELIS_MAX_SPECIES 8
 
@@ -128,6 +128,17 @@ typedef struct felis_params {
   /* 1D model: the area 2 pi sigX sigY of each species' matched beam, which
    * normalises its source and space-charge field (solveField.cpp:455-470) */
   double beam_area[FELIS_MAX_SPECIES];
+  /* [Phase_shifter] blocks (README.md:57-70; the reference documents them but
+   * its parser does not read them): shifter k sits at z = phase_shift_z[k]
+   * [m] and delays the electrons against the field by phase_shift_phase[k]
+   * * pi of the ponderomotive phase: theta -= phase * pi for every particle,
+   * after the push or drift of the iteration whose step [it dz, (it+1) dz)
+   * contains z, before the wrap (felis_phase_shift in the per-function
+   * sequence).  Arrays of num_phase_shifts entries; may be NULL when 0. */
+  int32_t num_phase_shifts;
+  int32_t pad_ps_;
+  const double* phase_shift_z;
+  const double* phase_shift_phase;
 } felis_params;
 
 /* Lattice state that updateK_quadG() leaves in Domain (updateK_quadG.cpp:8-94). */
@@ -194,6 +205,11 @@ felis_status felis_push_theta_gamma(felis_handle* h, int32_t iteration);
 /* particlePush.cpp:119-195 (drift_theta_gamma). */
 felis_status felis_drift_theta_gamma(felis_handle* h, int32_t iteration);
 /* rearrangeParticles.cpp:77-114 (periodicParticles). */
+/* [Phase_shifter] (README.md:57-70): theta -= phase * pi for every particle
+ * when a shifter sits in this iteration's step (see felis_params); a no-op
+ * otherwise.  No reference counterpart in the loop: call it between the push
+ * or drift and felis_periodic_particles. */
+felis_status felis_phase_shift(felis_handle* h, int32_t iteration);
 felis_status felis_periodic_particles(felis_handle* h, int32_t iteration);
 /* solveField.cpp:19-47 + fieldShareZ.cpp:39-78 at one rank (shiftField). */
 felis_status felis_shift_field(felis_handle* h, int32_t iteration);
@@ -273,10 +289,15 @@ felis_status felis_sort_by_slice(const int32_t* keys, int64_t n, int64_t* perm);
  * `stream` (a cudaStream_t, NULL for the default stream) and the call returns
  * without waiting for it.  Scratch is a fixed array inside the library
  * (about 4 MB on every GPU that loads it, kept until exit), so n is limited
- * to FELIS_SORT_NOALLOC_MAX_KEYS; larger n returns FELIS_BAD_ARG.  The first
- * call on a device resolves the array's device address; make that first call
- * before any stream capture.  Calls that overlap on the GPU share the array
- * and race: serialise them (one stream, or events). */
+ * to FELIS_SORT_NOALLOC_MAX_KEYS; larger n returns FELIS_BAD_ARG.  keys_dev
+ * and perm_dev must be device (or managed) memory of the current device;
+ * other pointers return FELIS_BAD_ARG (checked outside stream capture).  The
+ * array's device address belongs to the current CUDA context: every call made
+ * outside stream capture resolves it in that context, and a call made during
+ * capture uses the address resolved by an earlier call in the same context,
+ * so make one call in a context (after any cudaDeviceReset, and in every
+ * context you make current) before capturing.  Calls that overlap on the GPU
+ * share the array and race: serialise them (one stream, or events). */
 #define FELIS_SORT_NOALLOC_MAX_KEYS 262144
 felis_status felis_sort_by_slice_noalloc(const int32_t* keys_dev, int64_t n, int64_t* perm_dev, void* stream);
 

@@ -29,6 +29,8 @@
 //   solve_Sc_3D           solveField.cpp:187-403
 //   shiftField            solveField.cpp:19-47 (+ fieldShareZ.cpp:39-78, a no-op at one rank)
 //   periodicParticles     rearrangeParticles.cpp:77-114
+//   [Phase_shifter]       README.md:57-70 (the block the reference documents
+//                         but does not read; the project's reading of it)
 //   updateTotalEnergy     updateTotalEnergy.cpp:7-45
 //   calculate_twiss       twiss.cpp:7-99
 //   updatebFactor         saveFile.cpp:109-172
@@ -177,6 +179,7 @@ struct orc {
   bool currentFlag, driftFlag;
   std::vector<Und> und;
   std::vector<Quad> quad;
+  std::vector<double> psZ, psPhase;  // [Phase_shifter] positions [m], phases [pi]
   // tables
   std::vector<cd> alpha, alphaP, beta, betaP;
   std::vector<double> bessel;  // [bn][bcols]
@@ -1006,6 +1009,23 @@ static void solve_field(orc* D) {
   solve_field_U(D, D->Uy, D->ScUy);
 }
 
+// [Phase_shifter] (README.md:57-70; the reference's parser does not read the
+// block, so this follows the project's reading of it): the shifters whose z
+// lies in [it dz, (it+1) dz) delay every electron by phase * pi of theta,
+// applied after the push or drift and before the wrap.
+static void phase_shift(orc* D, int it) {
+  double d = 0.0;
+  const double z0 = it * D->dz, z1 = (it + 1) * D->dz;
+  for (size_t k = 0; k < D->psZ.size(); ++k)
+    if (D->psZ[k] >= z0 && D->psZ[k] < z1) d -= M_PI * D->psPhase[k];
+  if (d == 0.0) return;
+  for (int s = 0; s < D->nSpecies; ++s) {
+    Species& P = D->sp[s];
+    const int64_t cnt = P.off[D->subSliceN];
+    for (int64_t n = 0; n < cnt; ++n) P.theta[n] += d;
+  }
+}
+
 // rearrangeParticles.cpp:77-114
 static void periodic_particles(orc* D) {
   const double dTh = D->numSlice * 2 * M_PI;
@@ -1166,6 +1186,10 @@ orc* orc_create(const felis_params* p, int threads) {
   D->bn = p->bessel_rows; D->bcols = p->bessel_cols;
   D->abcN = p->abc_n; D->abcSig = p->abc_sig;
   D->wakeON = p->wake_on; D->maxStep = p->max_step;
+  if (p->num_phase_shifts > 0) {
+    D->psZ.assign(p->phase_shift_z, p->phase_shift_z + p->num_phase_shifts);
+    D->psPhase.assign(p->phase_shift_phase, p->phase_shift_phase + p->num_phase_shifts);
+  }
   D->ks = p->ks; D->lambda0 = p->lambda0; D->dz = p->dz; D->dx = p->dx; D->dy = p->dy; D->dr = p->dr;
   D->minX = p->min_x; D->minY = p->min_y; D->minZ = p->min_z; D->maxZ = p->max_z;
   D->gamma0 = p->gamma0; D->gamR = p->gam_r; D->dBessel = p->d_bessel;
@@ -1298,6 +1322,7 @@ int orc_push_theta_gamma(orc* D) { ORC_CALL(push_theta_gamma(D)); }
 int orc_drift_theta_gamma(orc* D) { ORC_CALL(drift_theta_gamma(D)); }
 int orc_solve_field(orc* D) { ORC_CALL(solve_field(D)); }
 int orc_periodic_particles(orc* D) { ORC_CALL(periodic_particles(D)); }
+int orc_phase_shift(orc* D, int it) { ORC_CALL(phase_shift(D, it)); }
 int orc_shift_field(orc* D) { ORC_CALL(shift_field(D)); }
 void orc_total_energy(orc* D, double* out) { total_energy(D, out); }
 void orc_twiss(orc* D, double* out) { twiss(D, out); }
@@ -1321,6 +1346,7 @@ int orc_run(orc* D, int it0, int it1, double* energy, double* tw, double* bf) {
     transverse_push(D);
     if (!D->driftFlag) push_theta_gamma(D);
     else drift_theta_gamma(D);
+    phase_shift(D, it);
     periodic_particles(D);
     if (!D->driftFlag && D->mode == FELIS_TIME_DEPENDENT) shift_field(D);
     if (D->err) return D->err;

@@ -61,6 +61,7 @@ def load(variant: str = "strict", out_dir: str | None = None) -> C.CDLL:
         "orc_drift_theta_gamma": (C.c_int, [vp]),
         "orc_solve_field": (C.c_int, [vp]),
         "orc_periodic_particles": (C.c_int, [vp]),
+        "orc_phase_shift": (C.c_int, [vp, C.c_int]),
         "orc_shift_field": (C.c_int, [vp]),
         "orc_total_energy": (None, [vp, _dp]),
         "orc_twiss": (None, [vp, _dp]),
@@ -173,6 +174,9 @@ class Oracle:
 
     def periodic_particles(self):
         self._ck(self.lib.orc_periodic_particles(self.h))
+
+    def phase_shift(self, it: int):
+        self._ck(self.lib.orc_phase_shift(self.h, it))
 
     def shift_field(self):
         self._ck(self.lib.orc_shift_field(self.h))

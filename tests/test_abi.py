@@ -56,3 +56,13 @@ def test_no_device_is_reported_not_crashed(fb, tmp_path):
     with pytest.raises(fb.FelisError) as e:
         fb.Handle(cfg.params)
     assert e.value.status == fb.NO_DEVICE
+
+
+def test_noalloc_limit_matches_the_header(fb):
+    """The Python binding's copy of the allocation-free sort's key limit is the
+    header's FELIS_SORT_NOALLOC_MAX_KEYS."""
+    import re
+
+    with open(os.path.join(ROOT, "include", "felis_b200.h")) as f:
+        m = re.search(r"#define\s+FELIS_SORT_NOALLOC_MAX_KEYS\s+(\d+)", f.read())
+    assert m and int(m.group(1)) == fb.SORT_NOALLOC_MAX_KEYS

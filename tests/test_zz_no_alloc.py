@@ -45,3 +45,6 @@ def test_noalloc_sort_limits(fb):
     kd = torch.zeros(fb.SORT_NOALLOC_MAX_KEYS + 1, dtype=torch.int32, device="cuda")
     pd = torch.zeros(fb.SORT_NOALLOC_MAX_KEYS + 1, dtype=torch.int64, device="cuda")
     assert fb.sort_by_slice_noalloc(kd.data_ptr(), kd.numel(), pd.data_ptr(), 0) == fb.BAD_ARG
+    # host buffers are refused before anything is queued
+    hk, hp = np.zeros(16, dtype=np.int32), np.zeros(16, dtype=np.int64)
+    assert fb.sort_by_slice_noalloc(hk.ctypes.data, 16, hp.ctypes.data, 0) == fb.BAD_ARG
