@@ -109,6 +109,8 @@ for _n in ("felis_solve_field", "felis_transverse_push", "felis_push_theta_gamma
            "felis_periodic_particles", "felis_phase_shift", "felis_shift_field", "felis_step"):
     _sig(_n, C.c_int, _vp, C.c_int32)
 _sig("felis_run", C.c_int, _vp, C.c_int32, C.c_int32)
+_sig("felis_first_planes_device", C.c_int, _vp, C.POINTER(_vp))
+_sig("felis_get_stream", C.c_int, _vp, C.POINTER(_vp))
 _sig("felis_set_slice_exchange", C.c_int, _vp, C.c_int32)
 _sig("felis_get_first_planes", C.c_int, _vp, _dp)
 _sig("felis_set_first_planes", C.c_int, _vp, _dp)
@@ -144,6 +146,7 @@ _sig("felis_mlp_param_count", C.c_int, _vp, _i64p)
 _sig("felis_mlp_get_params", C.c_int, _vp, _fp)
 _sig("felis_mlp_set_params", C.c_int, _vp, _fp)
 _sig("felis_mlp_forward", C.c_int, _vp, _fp, C.c_int64, _fp)
+_sig("felis_mlp_last_forward", C.c_int, _vp, _dp, _dp)
 _sig("felis_mlp_gradients", C.c_int, _vp, _fp, _fp, C.c_int64, _fp, _dp)
 _sig("felis_mlp_set_data", C.c_int, _vp, _fp, _fp, C.c_int64)
 _sig("felis_mlp_train", C.c_int, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64, _dp)
@@ -469,6 +472,19 @@ class Handle:
         self._ck(_lib.felis_get_first_planes(self._h, _p(buf)))
         return (buf[0::2] + 1j * buf[1::2]).reshape(self.H, 2, self.ny, self.nx)
 
+    def first_planes_device(self) -> list[int]:
+        """Device addresses of the first slice's 2 H planes ([h][pol] order,
+        ny*nx complex128 each), valid until the next shift."""
+        ptrs = (_vp * (2 * self.H))()
+        self._ck(_lib.felis_first_planes_device(self._h, ptrs))
+        return [int(p) for p in ptrs]
+
+    def stream(self) -> int:
+        """The cudaStream_t the handle queues its work on."""
+        s = _vp()
+        self._ck(_lib.felis_get_stream(self._h, C.byref(s)))
+        return int(s.value or 0)
+
     def set_first_planes(self, planes: np.ndarray):
         buf = _cplx_to_interleaved(planes)
         self._ck(_lib.felis_set_first_planes(self._h, _p(buf)))
@@ -681,6 +697,12 @@ class MLP:
             k += r
             out.append((W, b))
         return out
+
+    def last_forward(self) -> tuple[float, float]:
+        """(device ms, FLOPs) of the GEMM chain of the last forward chunk."""
+        ms, fl = C.c_double(), C.c_double()
+        self._ck(_lib.felis_mlp_last_forward(self._m, C.byref(ms), C.byref(fl)))
+        return ms.value, fl.value
 
     def forward(self, x) -> np.ndarray:
         x = _f32(x).reshape(-1, self.n_in)

@@ -38,6 +38,7 @@ UNITS = [
     ("lib/k_batch.cu", ["--use_fast_math"]),
     ("lib/mlp.cu", []),
     ("lib/k_mlp.cu", []),
+    ("lib/k_gemm.cu", []),
     ("host/config.cpp", []),
 ]
 

@@ -1393,6 +1393,26 @@ felis_status felis_get_first_planes(felis_handle* h, double* out) {
   return FELIS_OK;
 }
 
+// Device addresses of the first slice's planes, [h][pol] order (2H
+// pointers to ny*nx interleaved complex): the same planes as
+// felis_get_first_planes, for an exchange that stays in device memory.
+felis_status felis_first_planes_device(felis_handle* h, double** planes) {
+  if (!h || !planes) return FELIS_BAD_ARG;
+  const int S = h->p.slice_n, H = h->p.num_harmony;
+  const size_t N = (size_t)h->p.nx * h->p.ny;
+  for (int hh = 0; hh < H; ++hh)
+    for (int pol = 0; pol < 2; ++pol)
+      planes[hh * 2 + pol] = reinterpret_cast<double*>(h->U + field_plane(S, hh, pol, 0, h->ring_base) * N);
+  h->diag_valid = false;
+  return FELIS_OK;
+}
+
+felis_status felis_get_stream(felis_handle* h, void** stream) {
+  if (!h || !stream) return FELIS_BAD_ARG;
+  *stream = static_cast<void*>(h->st);
+  return FELIS_OK;
+}
+
 // Sets the first slice's planes (the slice received from the previous
 // process; zeros on the first process).
 felis_status felis_set_first_planes(felis_handle* h, const double* in) {

@@ -24,6 +24,7 @@ namespace {
 
 constexpr int kLayers = 4;
 constexpr int kChunk = 65536;  // rows per device pass (a multiple of 128)
+constexpr int kFwdChunk = 1 << 20;  // rows per inference pass (felis_mlp_forward)
 
 int round_up(int v, int m) { return (v + m - 1) / m * m; }
 
@@ -35,6 +36,8 @@ struct felis_mlp {
   cudaStream_t st = nullptr;
   std::string err;
   int* d_err = nullptr;
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the GEMM chain of the last forward chunk
+  double fwd_ms = 0.0, fwd_flops = 0.0;
   // per layer: rows (outputs) x cols (inputs), padded
   int rows[kLayers], cols[kLayers], rows_real[kLayers], cols_real[kLayers];
   size_t w_off[kLayers], b_off[kLayers], n_param = 0;
@@ -136,16 +139,24 @@ felis_status ensure_cap(felis_mlp* m, int rows) {
 void gemm(felis_mlp* m, const bf16* A, const bf16* B, int M, int N, int K, int lda, int ldb, const float* bias,
           float* out_f32, bf16* out_bf16, int ldc, int n_valid, int gelu) {
   GemmArgs g{A, B, M, N, K, lda, ldb, bias, out_f32, out_bf16, ldc, n_valid, gelu, m->d_err};
-  launch_gemm_tc(g, m->st);
+  if (launch_gemm_tma(g, m->st) != cudaSuccess) {
+    // shapes the network never produces (M % 128, N > 256, unaligned rows):
+    // reported through the error word like a device failure
+    cudaMemsetAsync(m->d_err, 0xff, sizeof(int), m->st);
+  }
 }
 
-// Forward pass of rows [0, M) of xb (M a multiple of 128).
-void forward(felis_mlp* m, int M) {
+// Forward pass of rows [0, M) of xb (M a multiple of 128).  Training keeps
+// every layer's FP32 pre-activation z (the backward pass needs it);
+// inference writes the hidden layers' BF16 activations and the last layer's
+// FP32 output only.
+void forward(felis_mlp* m, int M, bool keep_z = true) {
   const bf16* in = m->xb;
   int ld_in = m->in_p;
   for (int l = 0; l < kLayers; ++l) {
     const bool last = l == kLayers - 1;
-    gemm(m, in, m->wb[l], M, m->rows[l], m->cols[l], ld_in, m->cols[l], m->p + m->b_off[l], m->z[l], m->a[l],
+    gemm(m, in, m->wb[l], M, m->rows[l], m->cols[l], ld_in, m->cols[l], m->p + m->b_off[l],
+         (keep_z || last) ? m->z[l] : nullptr, (keep_z || !last) ? m->a[l] : nullptr,
          m->rows[l], m->rows_real[l], last ? 0 : 1);
     in = m->a[l];
     ld_in = m->rows[l];
@@ -272,7 +283,9 @@ felis_status felis_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64
     e = cudaMalloc(&m->wb[l], (size_t)r[l] * c[l] * sizeof(bf16));
     if (e == cudaSuccess) e = cudaMalloc(&m->wt[l], (size_t)r[l] * c[l] * sizeof(bf16));
   }
-  if (e == cudaSuccess) e = gemm_tc_prepare();
+  if (e == cudaSuccess) e = gemm_tma_prepare();
+  if (e == cudaSuccess) e = cudaEventCreate(&m->ev0);
+  if (e == cudaSuccess) e = cudaEventCreate(&m->ev1);
   if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
   // He-style initialisation for GELU layers (std sqrt(2 / fan_in)), zero biases
   std::mt19937_64 rng(seed ? seed : 1);
@@ -299,6 +312,8 @@ void felis_mlp_destroy(felis_mlp* m) {
     void* q[] = {m->wb[l], m->wt[l], m->z[l], m->a[l]};
     for (void* x : q) if (x) cudaFree(x);
   }
+  if (m->ev0) cudaEventDestroy(m->ev0);
+  if (m->ev1) cudaEventDestroy(m->ev1);
   if (m->st) cudaStreamDestroy(m->st);
   delete m;
 }
@@ -344,21 +359,30 @@ felis_status felis_mlp_set_params(felis_mlp* m, const float* in) {
 
 felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y) {
   if (!m || n < 0 || (n > 0 && (!x || !y))) return mfail(m, FELIS_BAD_ARG, "bad argument");
-  felis_status s = ensure_cap(m, (int)std::min<int64_t>(round_up((int)std::min<int64_t>(n, kChunk), 128), kChunk));
+  felis_status s =
+      ensure_cap(m, (int)std::min<int64_t>(round_up((int)std::min<int64_t>(n, kFwdChunk), 128), kFwdChunk));
   if (s != FELIS_OK) return s;
   std::vector<float> hy;
-  for (int64_t r0 = 0; r0 < n; r0 += kChunk) {
-    const int nr = (int)std::min<int64_t>(kChunk, n - r0);
+  for (int64_t r0 = 0; r0 < n; r0 += kFwdChunk) {
+    const int nr = (int)std::min<int64_t>(kFwdChunk, n - r0);
     const int M = round_up(nr, 128);
     MCK(cudaMemsetAsync(m->xf, 0, (size_t)M * m->in_p * sizeof(float), m->st));
     s = upload_rows(m, x + (size_t)r0 * m->n_in, nr, m->n_in, m->in_p, m->xf);
     if (s != FELIS_OK) return s;
     launch_f32_to_bf16(m->xf, m->xb, (int64_t)M * m->in_p, m->st);
-    forward(m, M);
+    MCK(cudaEventRecord(m->ev0, m->st));
+    forward(m, M, false);
+    MCK(cudaEventRecord(m->ev1, m->st));
     hy.resize((size_t)nr * m->out_p);
     MCK(cudaMemcpyAsync(hy.data(), m->z[kLayers - 1], hy.size() * sizeof(float), cudaMemcpyDeviceToHost, m->st));
     MCK(cudaStreamSynchronize(m->st));
     for (int r = 0; r < nr; ++r) memcpy(y + (size_t)(r0 + r) * m->n_out, &hy[(size_t)r * m->out_p], m->n_out * sizeof(float));
+    float ms = 0.f;
+    MCK(cudaEventElapsedTime(&ms, m->ev0, m->ev1));
+    m->fwd_ms = ms;
+    double fl = 0.0;
+    for (int l = 0; l < kLayers; ++l) fl += 2.0 * M * m->rows[l] * m->cols[l];
+    m->fwd_flops = fl;
   }
   return check_err(m);
 }
@@ -442,6 +466,13 @@ felis_status felis_mlp_train(felis_mlp* m, int32_t epochs, int32_t batch, float 
     if (loss_per_epoch) loss_per_epoch[ep] = sse / ((double)m->n_data * m->n_out);
   }
   return check_err(m);
+}
+
+felis_status felis_mlp_last_forward(const felis_mlp* m, double* ms, double* flops) {
+  if (!m || !ms || !flops) return FELIS_BAD_ARG;
+  *ms = m->fwd_ms;
+  *flops = m->fwd_flops;
+  return FELIS_OK;
 }
 
 felis_status felis_wait_selftest(int32_t limit, int32_t* timed_out) {

@@ -31,9 +31,11 @@ struct GemmArgs {
   int gelu;
   int* err;
 };
-void launch_gemm_tc(const GemmArgs& g, cudaStream_t st);
-// Shared-memory limit of the GEMM kernel (call once per device before use).
-cudaError_t gemm_tc_prepare();
+// Computed by the TMA-fed, warp-specialised persistent kernel of k_gemm.cu
+// (N <= 256; 16-byte aligned A and B); cudaErrorInvalidValue for shapes
+// outside that.  gemm_tma_prepare() once per device before use.
+cudaError_t launch_gemm_tma(const GemmArgs& g, cudaStream_t st);
+cudaError_t gemm_tma_prepare();
 
 // Elementwise and reduction helpers (row-major [rows][cols] unless stated).
 void launch_f32_to_bf16(const float* in, bf16* out, int64_t n, cudaStream_t st);

@@ -9,10 +9,16 @@ reduced as the reference reduces them: the field energies and the twiss sums
 are summed over processes (updateTotalEnergy.cpp:56-68, twiss.cpp:62-64), the
 bunching factor stays process-local (saveFile.cpp:109-172).
 
-The exchange is one send and one receive of 2 H planes per shifted iteration
-through torch.distributed (any backend; host buffers are moved to the GPU for
-NCCL).  Engines: `GpuEngine` (felis_b200.Handle in exchange mode) and
-`OracleEngine` (the CPU restatement, used by the multi-process tests).
+The exchange is one send and one receive of 2 H planes per shifted iteration.
+With the NCCL backend and GPU engines it stays in device memory: the planes
+are read and written where the handle keeps them (felis_first_planes_device),
+and the send, the receive and the copies are queued on the handle's own
+stream, so nothing waits on the host and the planes cross NVLink once.  With
+any other backend (gloo on CPU) the planes go through host buffers.
+`exchange_in_process` does the same hand-over in device memory for blocks
+held by one process.  Engines: `GpuEngine` (felis_b200.Handle in exchange
+mode) and `OracleEngine` (the CPU restatement, used by the multi-process
+tests).
 """
 from __future__ import annotations
 
@@ -63,6 +69,14 @@ def twiss_from_sums(s: np.ndarray, species: int) -> np.ndarray:
     return out
 
 
+class _DeviceArray:
+    """A complex128 vector in device memory, for torch.as_tensor (no copy)."""
+
+    def __init__(self, ptr: int, n: int):
+        self.__cuda_array_interface__ = {"shape": (n,), "typestr": "<c16", "data": (ptr, False), "version": 3,
+                                         "strides": None}
+
+
 class GpuEngine:
     """felis_b200.Handle of one slice block, in exchange mode."""
 
@@ -70,6 +84,19 @@ class GpuEngine:
         self.h = handle
         self.h.set_slice_exchange(True)
         self.H, self.species, self.mode = handle.H, handle.species, handle.mode
+
+    def plane_views(self):
+        """torch views of the block's first-slice planes in device memory
+        ([h][pol] order), valid until the next shift."""
+        import torch
+
+        n = self.h.nx * self.h.ny
+        return [torch.as_tensor(_DeviceArray(p, n), device="cuda") for p in self.h.first_planes_device()]
+
+    def stream(self):
+        import torch
+
+        return torch.cuda.ExternalStream(self.h.stream())
 
     def energy(self, it: int) -> np.ndarray:
         return self.h.total_energy(it)
@@ -160,6 +187,8 @@ class ShardedLoop:
         return t.cpu().numpy()
 
     def exchange(self):
+        if self.device is not None and isinstance(self.e, GpuEngine):
+            return self._exchange_device()
         out = self.e.outgoing()
         buf = np.ascontiguousarray(out.view(np.float64))
         req = None
@@ -173,6 +202,31 @@ class ShardedLoop:
         if req is not None:
             req.wait()
         self.e.incoming(recv.view(np.complex128).reshape(out.shape))
+
+    def _exchange_device(self):
+        """MPI_Transfer1F_Zplus in device memory over NCCL, on the handle's
+        stream: the outgoing planes packed into one buffer and sent to rank +
+        1; the planes of rank - 1 received and copied into place (zeros on
+        rank 0)."""
+        import torch
+
+        views = self.e.plane_views()
+        with torch.cuda.stream(self.e.stream()):
+            ops, recv = [], None
+            if self.rank + 1 < self.world:
+                send = torch.view_as_real(torch.stack(views))
+                ops.append(self.dist.P2POp(self.dist.isend, send, self.rank + 1))
+            if self.rank > 0:
+                recv = torch.empty((len(views), views[0].numel(), 2), dtype=torch.float64, device=views[0].device)
+                ops.append(self.dist.P2POp(self.dist.irecv, recv, self.rank - 1))
+            if ops:
+                for req in self.dist.batch_isend_irecv(ops):
+                    req.wait()
+            for k, v in enumerate(views):
+                if recv is None:
+                    v.zero_()
+                else:
+                    v.copy_(torch.view_as_complex(recv[k]))
 
     def run(self, it0: int, it1: int):
         """Returns per-iteration (energy, twiss, bfactor) of the state at the
@@ -194,3 +248,32 @@ class ShardedLoop:
                 self.exchange()
         self.bunching_sums = np.array(self.bunching_sums)
         return np.array(E), np.array(T), np.array(B)
+
+
+def exchange_in_process(engines: list) -> None:
+    """The slippage hand-over between consecutive slice blocks held by one
+    process (GpuEngines on one GPU, or on several with peer access), in
+    device memory: every block's outgoing planes are copied on its own stream,
+    block r + 1 waits for that copy and takes it, block 0 takes zeros."""
+    import torch
+
+    outs, events = [], []
+    for e in engines:
+        st = e.stream()
+        with torch.cuda.stream(st):
+            outs.append(torch.stack(e.plane_views()))
+            ev = torch.cuda.Event()
+            ev.record(st)
+        events.append(ev)
+    for r, e in enumerate(engines):
+        st = e.stream()
+        with torch.cuda.stream(st):
+            views = e.plane_views()
+            if r == 0:
+                for v in views:
+                    v.zero_()
+            else:
+                st.wait_event(events[r - 1])
+                outs[r - 1].record_stream(st)  # read on this stream: keep it until then
+                for k, v in enumerate(views):
+                    v.copy_(outs[r - 1][k], non_blocking=True)

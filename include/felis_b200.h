@@ -265,6 +265,16 @@ felis_status felis_set_slice_exchange(felis_handle* h, int32_t enable);
 /* [H][2][ny*nx] interleaved complex, host buffers. */
 felis_status felis_get_first_planes(felis_handle* h, double* out);
 felis_status felis_set_first_planes(felis_handle* h, const double* in);
+/* The same planes as felis_get_first_planes, as device addresses: planes
+ * receives 2 H pointers ([h][pol] order) to ny*nx interleaved complex
+ * values in this handle's device memory, valid until the next shift.  A
+ * caller that exchanges them in device memory (NCCL send/recv over NVLink,
+ * peer copies) orders its work after the step on the handle's stream
+ * (felis_get_stream) and before the next step, and writes zeros on the
+ * first process (MPI_Transfer1F_Zplus of fieldShareZ.cpp:39-78). */
+felis_status felis_first_planes_device(felis_handle* h, double** planes);
+/* The CUDA stream (cudaStream_t) on which the handle queues all its work. */
+felis_status felis_get_stream(felis_handle* h, void** stream);
 /* Unfinished sums of the current state for reductions across processes
  * (twiss.cpp:46-64 per species: sum x^2, y^2, x'^2, y'^2, x x', y y', count;
  * then saveFile.cpp:126-137 per harmonic: sum w cos(H theta), sum w
@@ -393,6 +403,11 @@ felis_status felis_mlp_get_params(felis_mlp* m, float* out);
 /* Sets the parameters and resets the optimiser state. */
 felis_status felis_mlp_set_params(felis_mlp* m, const float* in);
 felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y);
+/* Device time (CUDA events on the network's stream) and floating-point
+ * operations (2 M N K summed over the four layers, M the padded rows) of the
+ * GEMM chain of the last chunk of the last felis_mlp_forward (chunks are up
+ * to 1,048,576 rows). */
+felis_status felis_mlp_last_forward(const felis_mlp* m, double* ms, double* flops);
 /* Gradient of the loss over n <= 65536 samples, in the parameter layout, and
  * the loss itself. */
 felis_status felis_mlp_gradients(felis_mlp* m, const float* x, const float* t, int64_t n, float* grads,

@@ -142,3 +142,22 @@ def test_training_fits_a_smooth_map(fb):
     err = np.mean((m.forward(xt) - f(xt)) ** 2) / np.mean(f(xt) ** 2)
     assert err < 0.1, err
     m.close()
+
+
+def test_large_batch_forward_and_timing(net):
+    """200,000 rows: 1,563 tiles of 128 rows over the persistent GEMM's CTAs,
+    so every CTA alternates its two tensor-memory accumulators and wraps its
+    shared-memory stage ring many times.  Rows spread over the batch match
+    the CPU product; the GEMM chain's device time is reported."""
+    rng = np.random.default_rng(15)
+    p = random_params(net, rng)
+    net.set_params(p)
+    x = rng.normal(0, 1, (200_000, N_IN)).astype(np.float32)
+    y = net.forward(x)
+    ms, flops = net.last_forward()
+    assert ms > 0 and flops == 2.0 * 200_064 * (WIDTH * 48 + 2 * WIDTH * WIDTH + 48 * WIDTH)
+    pick = np.concatenate([np.arange(0, 200_000, 997), np.arange(199_872, 200_000)])
+    zs, _ = cpu_forward(net.unflatten(p), x[pick])
+    ref = zs[-1]
+    np.testing.assert_allclose(y[pick], ref, rtol=0, atol=FWD_ATOL * np.abs(ref).max())
+    print(f"forward GEMM chain, 200,000 rows: {ms:.3f} ms, {flops / ms / 1e9:.1f} TFLOP/s")

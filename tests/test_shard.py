@@ -160,10 +160,12 @@ def test_sharded_checkpoint_equals_single_process(single, tmp_path):
 
 
 @pytest.mark.gpu
-def test_gpu_blocks_equal_single_process(fb, single):
+@pytest.mark.parametrize("exchange", ["host", "device"])
+def test_gpu_blocks_equal_single_process(fb, single, exchange):
     """Two felis_b200.Handle blocks in exchange mode on one GPU, the slipping
-    slice handed over on the host after every shift, against the single-process
-    CPU run: the FP64 path is bit-exact, so the blocks are too."""
+    slice handed over after every shift -- through host buffers, or in device
+    memory on the handles' streams (felis_first_planes_device) -- against the
+    single-process CPU run: the FP64 path is bit-exact, so the blocks are too."""
     from felis_b200 import shard
 
     path, world = single["path"], 2
@@ -190,7 +192,9 @@ def test_gpu_blocks_equal_single_process(fb, single):
         np.testing.assert_allclose(S[7 * ns:-1] / S[-1], single["B"][k], rtol=1e-9, atol=1e-14)
         shifted = [e.step(it) for e in engines]
         assert len(set(shifted)) == 1
-        if shifted[0]:
+        if shifted[0] and exchange == "device":
+            shard.exchange_in_process(engines)
+        elif shifted[0]:
             out = [e.outgoing() for e in engines]
             engines[0].incoming(np.zeros_like(out[0]))
             for r in range(1, world):
