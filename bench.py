@@ -54,6 +54,49 @@ def peaks() -> tuple[float, str]:
         return 6650.0, "fallback"
 
 
+def tensor_peak() -> tuple[float, str]:
+    """Dense BF16 TFLOP/s: the measured burst figure, else the fallback."""
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    try:
+        with open(path) as f:
+            return float(json.load(f)["bf16_tflops"]), "measured"
+    except Exception:
+        return 1590.0, "fallback"
+
+
+def run_surrogate_gemm(rows: int) -> dict:
+    """The taper surrogate ranking `rows` candidate tapers: the forward GEMM
+    chain (38 -> 256 -> 256 -> 256 -> 33, BF16 operands, FP32 accumulation on
+    the tensor cores) timed with CUDA events on the network's stream, after
+    one untimed pass."""
+    import numpy as np
+
+    import felis_b200 as fb
+
+    m = fb.MLP(38, 256, 33, seed=3)
+    x = np.random.default_rng(1).standard_normal((rows, 38)).astype(np.float32)
+    m.forward(x)
+    best = None
+    for _ in range(3):
+        m.forward(x)
+        ms, flops = m.last_forward()
+        best = ms if best is None else min(best, ms)
+    m.close()
+    peak, kind = tensor_peak()
+    tf = flops / (best / 1e3) / 1e12
+    # HBM bytes of the chain: each layer reads its BF16 input and writes its
+    # output (BF16 for hidden layers, FP32 for the last); padded widths 48/256
+    M = (rows + 127) // 128 * 128
+    hbm = M * (48 * 2 + 256 * 2) + 2 * M * (256 * 2 + 256 * 2) + M * (256 * 2 + 48 * 4)
+    hpeak, hkind = peaks()
+    return {"workload": f"surrogate ranking: {rows} candidates through 38-256-256-256-33 (padded 48 / 48)",
+            "ms": best, "flops": flops, "tflops": tf,
+            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                         "peak_source": kind},
+            "hbm": {"algorithmic_bytes": hbm, "achieved_gbs": hbm / (best / 1e3) / 1e9,
+                    "frac": hbm / (best / 1e3) / 1e9 / hpeak}}
+
+
 class ClockSampler:
     """nvidia-smi clocks and throttle reasons sampled during the timed region."""
 
@@ -739,6 +782,8 @@ def main():
     ap.add_argument("--grid", type=int, default=None, help="grid key nx = ny of the workload (profiling captures)")
     ap.add_argument("--ensemble", type=int, default=96, help="instances of the batched ensemble (0: skip)")
     ap.add_argument("--ensemble-steps", type=int, default=10)
+    ap.add_argument("--surrogate-rows", type=int, default=1_000_000,
+                    help="candidates of the timed surrogate ranking (0: skip)")
     ap.add_argument("--config3-steps", type=int, default=20,
                     help="timed iterations of the Gaussian-current tapered run (0: skip)")
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
@@ -772,6 +817,7 @@ def main():
         del beam, fields
         ens = run_ensemble(args, dist, world) if args.ensemble > 0 else None
         c3 = run_config3(args, dist, world) if args.config3_steps > 0 else None
+        sg = run_surrogate_gemm(args.surrogate_rows) if args.surrogate_rows > 0 else None
         for k in ("metric", "unit", "n_gpus", "steps", "warmup", "higher_is_better", "scaling", "vs_baseline",
                   "data", "cpu_baseline"):
             fp64.pop(k, None)
@@ -788,6 +834,7 @@ def main():
             "roofline": mixed["roofline"], "step_roofline": mixed["step_roofline"],
             "kernels": mixed["kernels"], "gpu_launches": mixed["gpu_launches"], "clocks": mixed["clocks"],
             "launch": mixed["launch"], "e2e": e2e, "fp64_plain": fp64, "ensemble": ens, "config3": c3,
+            "surrogate_gemm": sg,
         }
     else:
         line.pop("_energy", None)
