@@ -6,11 +6,12 @@ wrapped phase leaves [0, dTh] (rearrangeParticles.cpp:105-108), MPI_Abort on
 an unknown polarisation.  The library raises device error words instead and
 returns a status; these tests make each failure on the host (bad values
 uploaded through the C ABI), check the status, and check that the handle
-keeps working after a clean re-upload: the rerun equals a fresh handle's run
-bit for bit (FP64) or exactly (the mixed engine is deterministic).  Every
-kernel involved returns on its own; the one device wait of the library (the
-tensor-core pipeline's mbarrier wait) is bounded, and its self-test makes it
-run out on a barrier that nothing completes.
+keeps working after a clean re-upload: the continued run equals, bit for bit
+(FP64) or exactly (the mixed engine is deterministic), that of a handle whose
+first iteration succeeded and that was re-uploaded the same way.  Every
+kernel involved returns on its own; the library's device waits (the
+tensor-core pipeline's mbarrier waits) are bounded, and the self-test makes
+one run out on a barrier that nothing completes.
 """
 from fractions import Fraction
 
@@ -92,7 +93,8 @@ def _bad_state(kind, cfg, beam, field, batch=False):
         # |U|^2 / 2 of 50 makes the phase step dz ks / (2 gamma^2) * 50 ~ 70 > 2 pi
         ux[1:-1] = 10.0
     elif kind == "radial":
-        beam["x"][5], beam["y"][5] = 150e-6, 0.0  # inside the +-300 um grid, beyond 10 radial cells
+        # inside the +-300 um grid, beyond 10 radial cells of 20.2 um
+        beam["x"][5], beam["y"][5] = 250e-6, 0.0
     return beam, (ux, uy)
 
 
@@ -108,11 +110,14 @@ def test_fp64_handle_reports_and_recovers(fb, tmp_path, kind):
     with pytest.raises(fb.FelisError) as e:
         h.run(0, 1)  # every failure shows in the first step
     assert e.value.status == getattr(fb, STATUS[kind]), str(e.value)
-    # a clean re-upload runs as a fresh handle does
+    # a clean re-upload continues as a handle whose first iteration succeeded
+    # does (the lattice flags of iteration 0 carry into iteration 1 either way)
     _upload(h, beam, field)
-    h.run(0, n)
+    h.run(1, n)
     ref = _handle(fb, cfg, beam, field)
-    ref.run(0, n)
+    ref.run(0, 1)
+    _upload(ref, beam, field)
+    ref.run(1, n)
     a, b = h.download_particles(0), ref.download_particles(0)
     for k in KEYS:
         assert np.array_equal(a[k], b[k]), k
@@ -131,9 +136,11 @@ def test_mixed_engine_reports_and_recovers(fb, tmp_path, kind):
         b.run(0, 1)
     assert e.value.status == getattr(fb, STATUS[kind]), str(e.value)
     _upload(b, beam, field, batch=True)
-    b.run(0, n)
+    b.run(1, n)
     ref = _batch(fb, cfg, beam, field)
-    ref.run(0, n)
+    ref.run(0, 1)
+    _upload(ref, beam, field, batch=True)
+    ref.run(1, n)
     x, y = b.download_particles(0), ref.download_particles(0)
     for k in KEYS:
         assert np.array_equal(x[k], y[k]), k

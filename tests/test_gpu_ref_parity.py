@@ -54,7 +54,7 @@ def _report(tag, errs):
 def _errors(parts, ux, uy, energy, ref_parts, ref_ux, ref_uy, ref_energy, n_particles=None, planes=None):
     n = n_particles if n_particles is not None else ref_parts["x"].size
     errs = {k: rel_err(parts[k][:n], ref_parts[k]) for k in refrun.KEYS}
-    sl = slice(1, None if planes is None else planes + 1)
+    sl = slice(1, -1) if planes is None else slice(1, planes + 1)
     errs["Ux"] = rel_err(ux[sl], ref_ux[1:-1])
     errs["Uy"] = rel_err(uy[sl], ref_uy[1:-1]) if np.any(ref_uy) else float(np.max(np.abs(uy[sl])))
     if energy is not None:
