@@ -132,6 +132,7 @@ _sig("felis_batch_upload_field", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, 
 _sig("felis_batch_download_field", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp)
 _sig("felis_batch_run", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_batch_get_diagnostics", C.c_int, _vp, C.c_int32, C.c_int32, C.c_int32, _dp, _dp, _dp)
+_sig("felis_batch_spectral_moments", C.c_int, _vp, C.c_int32, _dp)
 _sig("felis_batch_set_launch", C.c_int, _vp, C.c_int32, C.c_int32)
 _sig("felis_batch_get_launch", C.c_int, _vp, _i32p, _i32p)
 _sig("felis_batch_tune", C.c_int, _vp, C.c_int32, C.c_int32, _i32p)
@@ -612,6 +613,13 @@ class Batch:
         b = np.zeros(n * 2 * H)
         self._ck(_lib.felis_batch_get_diagnostics(self._b, inst, it0, it1, _p(e), _p(t), _p(b)))
         return e.reshape(n, 2 * H), t.reshape(n, 6), b.reshape(n, 2 * H)
+
+    def spectral_moments(self, hidx: int = 0) -> np.ndarray:
+        """[n, 3]: sum |U|^2, Re and Im of sum conj(U_s) U_{s+1} per instance
+        (felis_batch_spectral_moments)."""
+        out = np.zeros(3 * self.n)
+        self._ck(_lib.felis_batch_spectral_moments(self._b, hidx, _p(out)))
+        return out.reshape(self.n, 3)
 
     def set_launch(self, push_threads: int, adi_ctas: int):
         self._ck(_lib.felis_batch_set_launch(self._b, push_threads, adi_ctas))

@@ -53,3 +53,16 @@ def spectral_moments(field: np.ndarray) -> tuple[float, float]:
     w = p / p.sum()
     c = float((nu * w).sum())
     return c, float(np.sqrt(((nu - c) ** 2 * w).sum()))
+
+
+def lag_moments(r) -> tuple[float, float]:
+    """(centroid, rms width), in units of the slice frequency, from the
+    first-lag moments (R0, Re R1, Im R1) of felis_batch_spectral_moments:
+    R1 / R0 = <e^{2 pi i nu}> over the slice spectrum, so the centroid is its
+    circular mean arg(R1) / (2 pi) and the width that of the Gaussian line
+    with the same |R1| / R0, sqrt(-2 ln(|R1| / R0)) / (2 pi)."""
+    r0, re, im = (float(v) for v in r)
+    c = np.arctan2(im, re) / (2.0 * np.pi)
+    q = min(np.hypot(re, im) / r0, 1.0) if r0 > 0 else 0.0
+    w = np.sqrt(-2.0 * np.log(q)) / (2.0 * np.pi) if q > 0 else float("inf")
+    return float(c), float(w)

@@ -930,6 +930,28 @@ felis_status felis_batch_download_field(felis_batch* b, int32_t inst, int32_t hi
   return FELIS_OK;
 }
 
+felis_status felis_batch_spectral_moments(felis_batch* b, int32_t hidx, double* out) {
+  if (!b || !out || hidx < 0 || hidx >= FELIS_MAX_HARMONY) return bfail(b, FELIS_BAD_ARG, "bad argument");
+  const int n = (int)b->in.size();
+  std::vector<int> ring(n);
+  for (int k = 0; k < n; ++k) ring[k] = b->in[k].ring_base;
+  int* d_ring = nullptr;
+  double* d_out = nullptr;
+  BCK(cudaMalloc(&d_ring, n * sizeof(int)));
+  cudaError_t e = cudaMalloc(&d_out, (size_t)3 * n * sizeof(double));
+  if (e == cudaSuccess) e = cudaMemcpyAsync(d_ring, ring.data(), n * sizeof(int), cudaMemcpyHostToDevice, b->st);
+  if (e == cudaSuccess) {
+    launch_batch_spectrum(b->d_inst, n, d_ring, hidx, d_out, b->st);
+    e = cudaGetLastError();
+  }
+  if (e == cudaSuccess) e = cudaMemcpyAsync(out, d_out, (size_t)3 * n * sizeof(double), cudaMemcpyDeviceToHost, b->st);
+  if (e == cudaSuccess) e = cudaStreamSynchronize(b->st);
+  cudaFree(d_ring);
+  if (d_out) cudaFree(d_out);
+  if (e != cudaSuccess) return bfail(b, FELIS_CUDA_ERROR, cudaGetErrorString(e));
+  return FELIS_OK;
+}
+
 felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas) {
   if (!b || (push_threads != 128 && push_threads != 256) || adi_ctas < 1 || adi_ctas > 2)
     return bfail(b, FELIS_BAD_ARG, "bad launch shape (push threads 128 or 256, ADI CTAs per SM 1 or 2)");

@@ -103,6 +103,9 @@ cudaError_t launch_field_to_f32(const double* src, float2* U, int s0, int ns, in
 // H: the largest harmonic count of the ensemble (selects the kernel instance).
 void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st);
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);
+// Per instance {sum |U|^2, Re, Im sum conj(U_s) U_{s+1}} of harmonic index
+// hidx over slices (bunch order from ring[i]), cells and polarisations.
+void launch_batch_spectrum(const BInst* inst, int ninst, const int* ring, int hidx, double* out, cudaStream_t st);
 void launch_batch_reduce(const BInst* inst, int ninst, const BStep* step, double* hist_e, double* hist_t,
                          double* hist_b, int hist_stride_e, int hist_stride_t, int hist_stride_b, cudaStream_t st);
 // Threads of the ADI launch of one grid size: four chunk groups of the

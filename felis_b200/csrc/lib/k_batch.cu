@@ -1168,6 +1168,39 @@ __global__ void __launch_bounds__(256) k_batch_reduce(const BInst* inst, const B
   }
 }
 
+// First-lag moments of the field over the slices, per instance (one CTA
+// each): R0 = sum |U_s|^2 and R1 = sum conj(U_s) U_{s+1} over the slices in
+// bunch order (the ring read from ring[i]), every cell and both
+// polarisations of harmonic index hidx, FP64 sums in a fixed order.
+__global__ void __launch_bounds__(256) k_batch_spectrum(const BInst* inst, const int* ring, int hidx, double* out) {
+  __shared__ double red[8];
+  const BInst& I = inst[blockIdx.x];
+  double r0 = 0.0, r1re = 0.0, r1im = 0.0;
+  if (hidx < I.H) {
+    const int S = I.S, N = I.N, rb = ring[blockIdx.x];
+    const int64_t tot = (int64_t)S * N;
+    for (int pol = 0; pol < 2; ++pol) {
+      const float2* U = I.U + (size_t)(hidx * 2 + pol) * S * N;
+      for (int64_t k = threadIdx.x; k < tot; k += blockDim.x) {
+        const int s = (int)(k / N), c = (int)(k - (int64_t)s * N);
+        const float2 a = U[(size_t)((s + rb) % S) * N + c];
+        r0 += (double)a.x * a.x + (double)a.y * a.y;
+        if (s + 1 < S) {
+          const float2 b = U[(size_t)((s + 1 + rb) % S) * N + c];
+          r1re += (double)a.x * b.x + (double)a.y * b.y;
+          r1im += (double)a.x * b.y - (double)a.y * b.x;
+        }
+      }
+    }
+  }
+  const double t0 = block_sum_d(r0, red), t1 = block_sum_d(r1re, red), t2 = block_sum_d(r1im, red);
+  if (threadIdx.x == 0) {
+    out[3 * blockIdx.x] = t0;
+    out[3 * blockIdx.x + 1] = t1;
+    out[3 * blockIdx.x + 2] = t2;
+  }
+}
+
 // Instances by the largest harmonic count (sizes of the register arrays).
 typedef void (*PushKernel)(BatchLaunch);
 PushKernel push_kernel(int H) {
@@ -1278,6 +1311,10 @@ void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work
 void launch_batch_reduce(const BInst* inst, int ninst, const BStep* step, double* hist_e, double* hist_t,
                          double* hist_b, int se, int st_, int sb, cudaStream_t st) {
   k_batch_reduce<<<ninst, 256, 0, st>>>(inst, step, hist_e, hist_t, hist_b, se, st_, sb);
+}
+
+void launch_batch_spectrum(const BInst* inst, int ninst, const int* ring, int hidx, double* out, cudaStream_t st) {
+  if (ninst > 0) k_batch_spectrum<<<ninst, 256, 0, st>>>(inst, ring, hidx, out);
 }
 
 }  // namespace felis

@@ -351,6 +351,15 @@ felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1);
  * same meaning as felis_get_diagnostics. */
 felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t it0, int32_t it1,
                                          double* energy, double* twiss, double* bfactor);
+/* First-lag spectral moments of every instance's field, harmonic index hidx:
+ * out[3 i + 0] = sum |U_s|^2, out[3 i + 1] + i out[3 i + 2] = sum conj(U_s)
+ * U_{s+1}, over the slices s in bunch order, every cell and both
+ * polarisations (FP64 sums).  With the slice spectrum P(nu) of the field,
+ * R1 / R0 = <e^{2 pi i nu}>: arg(R1) / (2 pi) is the spectral centroid and
+ * sqrt(-2 ln(|R1| / R0)) / (2 pi) the rms bandwidth of a Gaussian line, in
+ * units of the slice frequency.  Instances without harmonic index hidx give
+ * zeros.  (No reference counterpart: the reference writes fields to disk.) */
+felis_status felis_batch_spectral_moments(felis_batch* b, int32_t hidx, double* out);
 /* Launch shape: threads per CTA of the push launch (128 or 256) and the CTAs
  * per SM that the ADI launch sizes its shared memory for (1 or 2; the rest of
  * the shared memory stages the slice's source box). */

@@ -281,3 +281,34 @@ def test_grid_classes_and_uneven_instances(fb, tmp_path):
         P32 = analysis.output_power(b.diagnostics(k, 0, steps + 1)[0])
         rel = np.abs(P32 - P64) / P64
         assert rel.max() < POWER_RTOL, (k, rel.max())
+
+
+def test_spectral_moments_match_the_downloaded_field(fb, tmp_path):
+    """felis_batch_spectral_moments against the same sums over the downloaded
+    fields (slices in bunch order, both polarisations), two instances of
+    different length after slippage shifts."""
+    from felis_b200 import analysis, workloads
+
+    cfgs, beams = [], []
+    for k, S in enumerate((24, 40)):
+        path = workloads.write_input(str(tmp_path / f"s{k}.inp"), kind="sase", slices=S, beamlets=64, nx=33,
+                                     total_length=1.0, seed_power=1e6)
+        cfgs.append(fb.Config(path))
+        beams.append(cfgs[-1].load_beam(0, seed=2 + k))
+    b = fb.Batch([c.params for c in cfgs])
+    for k, (c, beam) in enumerate(zip(cfgs, beams)):
+        b.upload_particles(k, *(beam[x] for x in ("x", "y", "px", "py", "theta", "gamma")), beam["offsets"],
+                           beam["weights"])
+        ux, uy = c.load_seed(0)
+        b.upload_field(k, 0, 0, ux)
+        b.upload_field(k, 0, 1, uy)
+    b.run(0, 17)
+    got = b.spectral_moments(0)
+    for k in range(2):
+        U = [b.download_field(k, 0, pol)[1:-1] for pol in (0, 1)]
+        r0 = sum(float(np.sum(np.abs(u) ** 2)) for u in U)
+        r1 = sum(complex(np.sum(np.conj(u[:-1]) * u[1:])) for u in U)
+        np.testing.assert_allclose(got[k], [r0, r1.real, r1.imag], rtol=1e-9, atol=1e-12 * r0)
+        c, w = analysis.lag_moments(got[k])
+        assert np.isfinite(c) and w >= 0
+    b.close()
