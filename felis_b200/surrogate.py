@@ -7,9 +7,13 @@ parameters.  It then ranks many candidate tapers for a given beam; the best
 ones are re-run by the plain FP64 method, which judges the network's error and
 takes over as a plain scan where that error exceeds 5 %.
 
-Runs.  Steady-state (Static) FELIS runs: 1 GeV class beam, 4096 quiet-start
-particles, 32 undulator segments of 40 periods (lambda_u 2.6 cm, no gaps,
-33.3 m, 1280 iterations), a Gaussian seed, grid key nx = 65.  Taper: per
+Runs (the ensemble of the workload table's surrogate case): time-dependent
+FELIS runs of 256 slices with 2048 particles each (512 beamlets x 4, shot
+noise), grid key nx = 65, a 1 GeV class flat-top beam and a long Gaussian
+seed; each slice spans 4 resonant wavelengths and each step 4 undulator
+periods (slices_in_bucket = lambdaUs_in_iteration = 4), so the 640-slice
+slippage of the 16.6 m undulator (32 segments of 20 periods, lambda_u 2.6 cm,
+no gaps, 160 iterations) stays inside the 1024-wavelength bunch.  Taper: per
 segment K_i = K0 (1 - a max(0, z_i - z0)^2) + N(0, 1e-4), z_i the segment's
 start, a in [0, 2e-4], z0 in [5, 30] m.  Beam parameters: peak current,
 relative energy spread, normalised emittance, matched beta, beam energy (the
@@ -18,8 +22,9 @@ undulator stays resonant at the segment-0 K), seed power.
 Features (38): the 32 K_i / K0 - 1 and the 6 beam parameters (seed power as
 log10).  Targets (33): log10 of the field energy at the end of each segment
 (the per-iteration power sums of updateTotalEnergy.cpp:25-36, unscaled) and
-the final bunching |b1| (a steady-state run has one slice, hence no spectrum;
-the bunching stands in for the spectral bandwidth of a time-dependent run).
+the rms spectral bandwidth of the final field over the slices (from its
+first-lag moments, felis_b200.analysis.lag_moments, in units of the slice
+frequency).
 """
 from __future__ import annotations
 
@@ -30,11 +35,15 @@ import time
 import numpy as np
 
 SEGMENTS = 32
-PERIODS = 40
+PERIODS = 20
+BUCKET = 4          # wavelengths per slice = undulator periods per step
+SLICES = 256
+BEAMLETS = 512      # x 4 particles: 2048 per slice
 LAMBDA_U_CM = 2.6
 SEG_LEN = PERIODS * LAMBDA_U_CM / 100.0
 K0 = 2.6
-STEPS = SEGMENTS * PERIODS
+STEPS = SEGMENTS * PERIODS // BUCKET
+SEG_STEPS = PERIODS // BUCKET
 N_FEATURES = SEGMENTS + 6
 N_TARGETS = SEGMENTS + 1
 
@@ -77,64 +86,94 @@ def _input(beam: dict, k: np.ndarray, path: str) -> str:
     from felis_b200 import workloads
 
     return workloads.write_input(
-        path, kind="static", beamlets=1024, per_beamlet=4, nx=65, total_length=(STEPS + 0.5) * LAMBDA_U_CM / 100.0,
-        energy_mev=beam["energy_mev"], spread_pct=beam["spread"] * 100.0, emit_um=beam["emit_um"],
-        beta=beam["beta"], current=beam["current"], K0=K0, lambda_u_cm=LAMBDA_U_CM, units=SEGMENTS,
-        unit_len=SEG_LEN, und_len=SEG_LEN, seed_power=10.0 ** beam["log_seed_w"], in_air=False, k_list=k)
+        path, kind="sase", slices=SLICES, bucket=BUCKET, beamlets=BEAMLETS, per_beamlet=4, nx=65,
+        total_length=(STEPS + 0.5) * BUCKET * LAMBDA_U_CM / 100.0, energy_mev=beam["energy_mev"],
+        spread_pct=beam["spread"] * 100.0, emit_um=beam["emit_um"], beta=beam["beta"], current=beam["current"],
+        K0=K0, lambda_u_cm=LAMBDA_U_CM, units=SEGMENTS, unit_len=SEG_LEN, und_len=SEG_LEN,
+        seed_power=10.0 ** beam["log_seed_w"], in_air=False, k_list=k)
 
 
-def _targets(energy: np.ndarray, bfac: np.ndarray) -> np.ndarray:
-    """energy[it, 2] (Ux, Uy sums), bfac[it, 2] -> the 33 targets."""
+def _targets(energy: np.ndarray, moments) -> np.ndarray:
+    """energy[it, 2] (Ux, Uy sums) and the final field's first-lag moments ->
+    the 33 targets."""
+    from felis_b200 import analysis
+
     p = energy[:, 0] + energy[:, 1]
-    seg = p[np.arange(1, SEGMENTS + 1) * PERIODS]
-    return np.concatenate([np.log10(np.maximum(seg, 1e-300)), [np.hypot(bfac[-1, 0], bfac[-1, 1])]])
+    seg = p[np.arange(1, SEGMENTS + 1) * SEG_STEPS]
+    return np.concatenate([np.log10(np.maximum(seg, 1e-300)), [analysis.lag_moments(moments)[1]]])
 
 
-def simulate(cases: list, chunk: int = 4096, workdir: str | None = None) -> np.ndarray:
+def _moments(ux: np.ndarray, uy: np.ndarray) -> tuple[float, float, float]:
+    """First-lag moments of downloaded fields (physical slices [S, ny, nx])."""
+    r0 = float(np.sum(np.abs(ux) ** 2) + np.sum(np.abs(uy) ** 2))
+    r1 = complex(np.sum(np.conj(ux[:-1]) * ux[1:]) + np.sum(np.conj(uy[:-1]) * uy[1:]))
+    return r0, r1.real, r1.imag
+
+
+def _prepare(cases: list, d: str, first: int):
+    """Configs and seed fields of a chunk of cases, parsed on host threads."""
+    from concurrent.futures import ThreadPoolExecutor
+
+    import felis_b200 as fb
+
+    def one(i):
+        b, k = cases[i]
+        c = fb.Config(_input(b, k, os.path.join(d, f"c{first + i}.inp")))
+        return c, c.load_seed(0)
+
+    with ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1)) as ex:
+        return list(ex.map(one, range(len(cases))))
+
+
+def simulate(cases: list, chunk: int = 512, workdir: str | None = None, seed0: int = 1) -> np.ndarray:
     """Full simulations of (beam, taper) cases on the batched mixed-precision
-    engine, `chunk` instances per ensemble; returns targets [n, 33]."""
+    engine, `chunk` instances per ensemble (beams from the device loader, shot
+    noise seeded seed0 + case index); returns targets [n, 33]."""
     import felis_b200 as fb
 
     d = workdir or tempfile.mkdtemp(prefix="felis_taper_")
     out = np.zeros((len(cases), N_TARGETS))
     for c0 in range(0, len(cases), chunk):
         part = cases[c0:c0 + chunk]
-        cfgs = [fb.Config(_input(b, k, os.path.join(d, f"c{c0 + i}.inp"))) for i, (b, k) in enumerate(part)]
-        ens = fb.Batch([c.params for c in cfgs])
-        for i, c in enumerate(cfgs):
-            beam = c.load_beam(0, seed=1)
-            ux, uy = c.load_seed(0)
+        prep = _prepare(part, d, c0)
+        ens = fb.Batch([c.params for c, _ in prep])
+        for i, (c, (ux, uy)) in enumerate(prep):
+            beam = c.load_beam_device(0, seed=seed0 + c0 + i)
             ens.upload_particles(i, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
                                  beam["offsets"], beam["weights"])
+            del beam
             ens.upload_field(i, 0, 0, ux)
             ens.upload_field(i, 0, 1, uy)
         ens.run(0, STEPS)
+        mom = ens.spectral_moments(0)
         for i in range(len(part)):
-            e, _, bf = ens.diagnostics(i, 0, STEPS + 1)
-            out[c0 + i] = _targets(e, bf)
+            e, _, _ = ens.diagnostics(i, 0, STEPS + 1)
+            out[c0 + i] = _targets(e, mom[i])
         ens.close()
-        for c in cfgs:
+        for c, _ in prep:
             c.close()
     return out
 
 
-def simulate_plain(beam: dict, k: np.ndarray, workdir: str | None = None) -> np.ndarray:
+def simulate_plain(beam: dict, k: np.ndarray, workdir: str | None = None, seed: int = 1) -> np.ndarray:
     """The plain FP64 method (felis_create / felis_run) on one case."""
     import felis_b200 as fb
 
     d = workdir or tempfile.mkdtemp(prefix="felis_taper_")
     c = fb.Config(_input(beam, k, os.path.join(d, "plain.inp")))
     h = fb.Handle(c.params)
-    b = c.load_beam(0, seed=1)
+    b = c.load_beam_device(0, seed=seed)
     ux, uy = c.load_seed(0)
     h.upload_particles(0, b["x"], b["y"], b["px"], b["py"], b["theta"], b["gamma"], b["offsets"], b["weights"])
+    del b
     h.upload_field(0, 0, ux)
     h.upload_field(0, 1, uy)
     h.run(0, STEPS)
-    e, _, bf = h.diagnostics(0, STEPS + 1)
+    e, _, _ = h.diagnostics(0, STEPS + 1)
+    mom = _moments(h.download_field(0, 0)[1:-1], h.download_field(0, 1)[1:-1])
     h.close()
     c.close()
-    return _targets(e, bf)
+    return _targets(e, mom)
 
 
 class Surrogate:
@@ -169,11 +208,11 @@ class Surrogate:
         self.net.close()
 
 
-def dataset(n: int, seed: int = 1, chunk: int = 4096) -> tuple[np.ndarray, np.ndarray, list]:
+def dataset(n: int, seed: int = 1, chunk: int = 512) -> tuple[np.ndarray, np.ndarray, list]:
     rng = np.random.default_rng(seed)
     cases = [(random_beam(rng), random_taper(rng)) for _ in range(n)]
     X = np.stack([features(b, k) for b, k in cases])
-    Y = simulate(cases, chunk=chunk)
+    Y = simulate(cases, chunk=chunk, seed0=seed * 1_000_000 + 1)
     return X, Y, cases
 
 

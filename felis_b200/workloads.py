@@ -44,7 +44,7 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
                noise: bool | None = None, undulator: str = "BiPolar", polarity: float = 0.0,
                linear_taper: float = 0.0, wake: bool = False, quads: bool = False, abc_n: int = 10,
                in_air: bool = True, k_list=None, sigma_slices: float | None = None, profile_nodes: int = 65,
-               K_und: float | None = None, dimension: int = 3, phase_shifters=()) -> str:
+               K_und: float | None = None, dimension: int = 3, phase_shifters=(), bucket: int = 1) -> str:
     """Input text of one workload.  `sigma_slices` switches the flat-top
     current to a Gaussian of that rms length (in slices) centred on the bunch,
     written as a `profile_nodes`-node Polygon so that the energy-spread nodes
@@ -54,20 +54,23 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
     on the same resonance (parameterSetting.cpp's default K0).  `dimension` 1
     selects the 1D model (the grid collapses to one cell per slice).
     `phase_shifters` lists [Phase_shifter] blocks as (number, start_position
-    [m], interval_length [m], phase [pi]) tuples (README.md:57-70)."""
+    [m], interval_length [m], phase [pi]) tuples (README.md:57-70).
+    `bucket` sets slices_in_bucket = lambdaUs_in_iteration: each slice spans
+    `bucket` wavelengths and one step `bucket` undulator periods, so the field
+    still slips one slice per step."""
     static = kind == "static"
     if noise is None:
         noise = not static
     photon = resonant_photon_energy(energy_mev, lambda_u_cm, K0)
     lam0_um = PLANCK_H * C_LIGHT / photon * 1e6
-    minZ, maxZ = 0.0, (slices + 0.5) * lam0_um
+    minZ, maxZ = 0.0, (slices + 0.5) * bucket * lam0_um
     k_line = "" if k_list is None else " K0_list=" + ",".join(repr(float(k)) for k in k_list) + "\n"
     harm = "\n".join(f" harmony{i} = {h}" for i, h in enumerate(harmonics))
     zspan = 1.0e-3
     if sigma_slices is None:
         z_nodes = f" z_nodes=2\n z0={-zspan}\n z1={zspan}\n z_n0=1\n z_n1=1"
     else:
-        lam0 = lam0_um * 1e-6
+        lam0 = lam0_um * 1e-6 * bucket  # slice length
         centre, sig = 0.5 * slices * lam0, sigma_slices * lam0
         zs = [(-1.0 + (slices + 2.0) * k / (profile_nodes - 1)) * lam0 for k in range(profile_nodes)]
         lines = [f" z_nodes={profile_nodes}"]
@@ -123,8 +126,8 @@ def input_text(kind: str = "sase", *, slices: int = 1024, beamlets: int = 2048, 
  photon_energy={photon!r}
  num_harmony={len(harmonics)}
 {harm}
- slices_in_bucket=1
- lambdaUs_in_iteration=1
+ slices_in_bucket={bucket}
+ lambdaUs_in_iteration={bucket}
  ABC_N={abc_n}
  ABC_coef=1
 
