@@ -491,10 +491,10 @@ def run_mixed(args, cfg, beam, fields, dist, world, fp64_energy):
                 traffic = json.load(f).get(args.workload + "_mixed", {}).get(dom)
         except Exception:
             traffic = None
-    threads, adi_ctas = b.launch()
+    box, adi_ctas = b.launch()
     res = {
         "value": P * K * world / sec, "ms_per_step": ms / K, "adi_cells_per_s": cells * K * world / sec,
-        "launch": {"push_threads": threads, "adi_ctas_per_sm": adi_ctas},
+        "launch": {"push_box_cells": box, "adi_ctas_per_sm": adi_ctas},
         "power_error": {"max_rel": float(rel.max()) if rel.size else None,
                         "final_rel": float(rel[-1]) if rel.size else None,
                         "iterations": [0, W + K], "reference": "FP64 plain GPU path, same initial state"},
@@ -617,7 +617,7 @@ def run_ensemble(args, dist, world):
         errs.append((float(rel.max()), k, c.params.slice_n, c.params.nx))
         h.close()
     worst = max(errs)
-    threads, adi_ctas = b.launch()
+    box, adi_ctas = b.launch()
     res = {
         "workload": f"{len(spec)} SASE instances (shot noise, no seed laser), slices in {{128..2048}}, "
                     f"grids {{66, 102, 152}}, 4096 particles per slice, 2-4 kA, spread 0.5-2e-4, mixed precision; "
@@ -625,7 +625,7 @@ def run_ensemble(args, dist, world):
         "value": P * K * world / (ms / 1e3), "unit": UNIT, "ms_per_step": ms / K,
         "adi_cells_per_s": cells * K * world / (ms / 1e3), "particles": P, "cells": cells,
         "steps": K, "iterations": [i0, i0 + K], "setup_s": t_setup,
-        "launch": {"push_threads": threads, "adi_ctas_per_sm": adi_ctas},
+        "launch": {"push_box_cells": box, "adi_ctas_per_sm": adi_ctas},
         "kernels": kinds, "gpu_launches": launches,
         "power_error_vs_fp64": {
             "instances": len(errs), "what": "per instance, the largest relative power error over iterations "
@@ -711,7 +711,7 @@ def run_config3(args, dist, world):
                  "adi_cells_per_s": cells * K * world / (ms64 / 1e3), "kernels": k64, "gpu_launches": launches64},
         "mixed": {"ms_per_step": ms32 / K, "value": P * K * world / (ms32 / 1e3),
                   "adi_cells_per_s": cells * K * world / (ms32 / 1e3), "kernels": k32, "gpu_launches": launches32,
-                  "launch": {"push_threads": launch[0], "adi_ctas_per_sm": launch[1]},
+                  "launch": {"push_box_cells": launch[0], "adi_ctas_per_sm": launch[1]},
                   "roofline": {"bound": "hbm", "kernel": dom, "achieved": achieved, "peak": peak, "unit": "GB/s",
                                "frac": achieved / peak, "peak_source": peak_kind, "bytes_per_launch": bpl,
                                "mean_launch_ms": avg_ms}},

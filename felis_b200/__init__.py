@@ -621,10 +621,14 @@ class Batch:
         self._ck(_lib.felis_batch_spectral_moments(self._b, hidx, _p(out)))
         return out.reshape(self.n, 3)
 
-    def set_launch(self, push_threads: int, adi_ctas: int):
-        self._ck(_lib.felis_batch_set_launch(self._b, push_threads, adi_ctas))
+    def set_launch(self, push_box: int, adi_ctas: int):
+        """Launch shape: source cells the push stages in shared memory (512 ..
+        6144; 3072 lets seven one-harmonic CTAs share an SM) and ADI CTAs per
+        SM (1 or 2).  Results do not depend on it."""
+        self._ck(_lib.felis_batch_set_launch(self._b, push_box, adi_ctas))
 
     def launch(self) -> tuple[int, int]:
+        """(push_box cells, adi_ctas)."""
         t, c = C.c_int32(), C.c_int32()
         self._ck(_lib.felis_batch_get_launch(self._b, C.byref(t), C.byref(c)))
         return t.value, c.value

@@ -13,6 +13,9 @@
 #include <string.h>
 
 #include <algorithm>
+#include <sys/stat.h>
+#include <mutex>
+#include <array>
 #include <cmath>
 #include <initializer_list>
 #include <complex>
@@ -321,7 +324,7 @@ struct felis_batch {
   int device = 0, sms = 0, dev_smem = 0;
   cudaStream_t st = nullptr;
   std::string err;
-  int nx_max = 0, ny_max = 0, H_max = 1, LF_max = 1, nr_max = 1, N_max = 0, nsrc_max = 1;
+  int nx_max = 0, ny_max = 0, H_max = 1, L_max = 1, LF_max = 1, nr_max = 1, N_max = 0, nsrc_max = 1;
   BInst* d_inst = nullptr;
   int4* d_adi_work = nullptr;
   int4* d_push_work = nullptr;
@@ -331,7 +334,9 @@ struct felis_batch {
   double *d_he = nullptr, *d_ht = nullptr, *d_hb = nullptr;
   int hist_n = 0;
   int adi_smem_max = 0;
-  int push_threads = 128, push_smem = 0, adi_ctas = 2;
+  // launch shape: source cells the push stages in shared memory (which sets
+  // how many push CTAs share an SM) and ADI CTAs per SM
+  int push_box = 3072, push_smem = 0, adi_ctas = 2;
   bool layout_ready = false;
   int src_valid_it = -1;  // iteration whose solveField source is in the buffers
   double last_run_ms = 0.0;
@@ -574,8 +579,10 @@ felis_status prepare(felis_batch* b) {
 
 // Shared memory of both launches: the ADI holds its interior plane, 16 tables and as
 // much of the source box as fits beside adi_ctas CTAs per SM (more cells are
-// read from global memory); the push holds the accumulators of up to 6144 source
-// cells (larger boxes accumulate in the source buffer in global memory).
+// read from global memory); the push holds the staged field and the
+// accumulators of up to push_box source cells (the central window of larger
+// boxes; the rest accumulates in the source buffer in global memory).  The
+// push kernel's limit is set for the largest choice, 6144 cells.
 felis_status ensure_launch(felis_batch* b) {
   b->adi_smem_max = 0;
   for (AdiClass& c : b->adi_classes) {
@@ -594,9 +601,9 @@ felis_status ensure_launch(felis_batch* b) {
     c.smem = (int)batch_adi_smem(c.nx, c.ny, (int)src_cells);
     b->adi_smem_max = std::max(b->adi_smem_max, c.smem);
   }
-  const int box = std::min(b->N_max, 6144);
-  b->push_smem = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, box);
-  if (batch_set_smem(b->H_max, b->adi_smem_max, b->push_smem) != cudaSuccess)
+  b->push_smem = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, std::min(b->N_max, b->push_box));
+  const int push_max = (int)batch_push_smem(b->nsrc_max, b->LF_max, b->nr_max, std::min(b->N_max, 6144));
+  if (batch_set_smem(b->H_max, b->L_max, b->adi_smem_max, push_max) != cudaSuccess)
     return bfail(b, FELIS_UNSUPPORTED, "shared memory of the ensemble launches exceeds the device limit");
   return FELIS_OK;
 }
@@ -618,7 +625,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
     d.inst = b->d_inst; d.step = row_d0; d.work = b->d_push_work; d.nwork = b->n_push;
     d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY;
     BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
-    launch_batch_push(d, b->H_max, b->push_threads, b->st);
+    launch_batch_push(d, b->H_max, b->L_max, b->st);
   }
   for (int it = it0; it < it1; ++it) {
     const BStep* T = b->d_steps + (size_t)(it - it0) * n;
@@ -633,7 +640,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
       p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
       p.mode = BATCH_PUSH;
       BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
-      launch_batch_push(p, b->H_max, b->push_threads, b->st);
+      launch_batch_push(p, b->H_max, b->L_max, b->st);
     }
     if (it + 1 < b->hist_n) {
       BatchScope ks(b, FELIS_BATCH_KERNEL_REDUCE);
@@ -725,6 +732,7 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
     b->N_max = std::max(b->N_max, p->nx * p->ny);
     b->H_max = std::max(b->H_max, p->num_harmony);
     b->LF_max = std::max(b->LF_max, p->scl_mode * p->scf_mode);
+    b->L_max = std::max(b->L_max, p->scl_mode);
     b->nr_max = std::max(b->nr_max, p->nr);
     max_step = std::max(max_step, p->max_step);
     const int S = p->slice_n, N = p->nx * p->ny, H = p->num_harmony, M = std::max(p->nx, p->ny);
@@ -783,7 +791,7 @@ felis_status felis_batch_create(const felis_params* const* instances, int32_t n,
   if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
   for (auto& I : b->in) { I.p.abc_alpha = I.p.abc_alpha_p = I.p.abc_beta = I.p.abc_beta_p = nullptr; }
   if (std::max(b->nx_max, b->ny_max) > 256) return bad(FELIS_UNSUPPORTED, "grid wider than 256 points");
-  b->push_threads = 128;
+  b->push_box = 3072;
   b->adi_ctas = 2;
   *out = b;
   return FELIS_OK;
@@ -952,17 +960,17 @@ felis_status felis_batch_spectral_moments(felis_batch* b, int32_t hidx, double* 
   return FELIS_OK;
 }
 
-felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas) {
-  if (!b || (push_threads != 128 && push_threads != 256) || adi_ctas < 1 || adi_ctas > 2)
-    return bfail(b, FELIS_BAD_ARG, "bad launch shape (push threads 128 or 256, ADI CTAs per SM 1 or 2)");
-  b->push_threads = push_threads;
+felis_status felis_batch_set_launch(felis_batch* b, int32_t push_box, int32_t adi_ctas) {
+  if (!b || push_box < 512 || push_box > 6144 || adi_ctas < 1 || adi_ctas > 2)
+    return bfail(b, FELIS_BAD_ARG, "bad launch shape (push box 512..6144 cells, ADI CTAs per SM 1 or 2)");
+  b->push_box = push_box;
   b->adi_ctas = adi_ctas;
   return FELIS_OK;
 }
 
-felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas) {
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_box, int32_t* adi_ctas) {
   if (!b) return FELIS_BAD_ARG;
-  if (push_threads) *push_threads = b->push_threads;
+  if (push_box) *push_box = b->push_box;
   if (adi_ctas) *adi_ctas = b->adi_ctas;
   return FELIS_OK;
 }
@@ -1025,26 +1033,75 @@ felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1) {
   return check_batch_err(b);
 }
 
-// Online launch-shape tuner.  The particle state and the fields after a step
-// do not depend on the launch shape (fixed-point deposit, ADI chunks fixed by
-// the grid, one thread per particle), so the tuner advances the
-// ensemble through real iterations, each candidate shape for `steps` of
-// them, and keeps the fastest.  Results are cached per ensemble geometry.
+namespace {
+// Launch shapes found by felis_batch_tune, per ensemble geometry: in memory,
+// and in a text file (FELIS_TUNE_CACHE, or $HOME/.cache/felis_b200_batch_tune_v2.txt)
+// so that later processes on the same kind of GPU skip the trials.  One line
+// per geometry: SMs nx ny H L LF nr instances particles/65536 push_box adi_ctas.
+typedef std::array<long long, 9> TuneKey;
+std::mutex g_tune_mu;
+std::map<TuneKey, std::pair<int, int>> g_tune;
+bool g_tune_loaded = false;
+
+std::string tune_path() {
+  const char* e = getenv("FELIS_TUNE_CACHE");
+  if (e && *e) return e;
+  const char* home = getenv("HOME");
+  return std::string(home && *home ? home : "/tmp") + "/.cache/felis_b200_batch_tune_v2.txt";
+}
+
+void tune_load() {
+  if (g_tune_loaded) return;
+  g_tune_loaded = true;
+  FILE* f = fopen(tune_path().c_str(), "r");
+  if (!f) return;
+  TuneKey k;
+  int box, adi;
+  while (fscanf(f, "%lld %lld %lld %lld %lld %lld %lld %lld %lld %d %d", &k[0], &k[1], &k[2], &k[3], &k[4], &k[5],
+                &k[6], &k[7], &k[8], &box, &adi) == 11)
+    if (box >= 512 && box <= 6144 && adi >= 1 && adi <= 2) g_tune[k] = std::make_pair(box, adi);
+  fclose(f);
+}
+
+void tune_store(const TuneKey& k, std::pair<int, int> v) {
+  const std::string path = tune_path();
+  const size_t slash = path.rfind('/');
+  if (slash != std::string::npos && slash > 0) mkdir(path.substr(0, slash).c_str(), 0755);
+  FILE* f = fopen(path.c_str(), "a");
+  if (!f) return;  // the cache is optional
+  fprintf(f, "%lld %lld %lld %lld %lld %lld %lld %lld %lld %d %d\n", k[0], k[1], k[2], k[3], k[4], k[5], k[6], k[7],
+          k[8], v.first, v.second);
+  fclose(f);
+}
+}  // namespace
+
+// Launch shapes are tuned on the running ensemble: the push's staged source
+// area (3072 cells: seven one-harmonic CTAs per SM; 6144: four, fewer cells
+// through global memory on wide beams) and the ADI's CTAs per SM (1: more of
+// the source box beside the plane; 2: more planes in flight).  Results do
+// not depend on the shape, so the tuner advances the ensemble through real
+// iterations, each candidate for `steps` of them, and keeps the fastest.
 felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it) {
   if (!b || steps < 1 || !next_it) return FELIS_BAD_ARG;
   *next_it = it0;
-  static std::map<std::tuple<int, int, int, int, int, int, int64_t>, std::pair<int, int>> cache;
   int64_t total = 0;
   for (auto& I : b->in) total += I.count;
-  const auto key = std::make_tuple(b->nx_max, b->ny_max, b->H_max, b->LF_max, b->nr_max, (int)b->in.size(),
-                                   total >> 16);
-  auto hit = cache.find(key);
-  if (hit != cache.end()) {
-    std::tie(b->push_threads, b->adi_ctas) = hit->second;
-    return FELIS_OK;
+  int dev = 0, sms = 0;
+  BCK(cudaGetDevice(&dev));
+  BCK(cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, dev));
+  const TuneKey key = {sms, b->nx_max, b->ny_max, b->H_max, b->L_max, b->LF_max, b->nr_max, (long long)b->in.size(),
+                       (long long)(total >> 16)};
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    tune_load();
+    auto hit = g_tune.find(key);
+    if (hit != g_tune.end()) {
+      std::tie(b->push_box, b->adi_ctas) = hit->second;
+      return FELIS_OK;
+    }
   }
   double best = 1e300;
-  std::pair<int, int> pick(b->push_threads, b->adi_ctas);
+  std::pair<int, int> pick(b->push_box, b->adi_ctas);
   int it = it0;
   // the first run after an upload also deposits: spend it outside the timing
   if (b->src_valid_it != it) {
@@ -1052,18 +1109,24 @@ felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_
     if (s != FELIS_OK) return s;
     it += 1;
   }
-  for (int t : {128, 256})
+  for (int box : {3072, 6144}) {
+    if (box > 3072 && b->N_max <= 3072) continue;  // the same launch as 3072
     for (int c : {1, 2}) {
-      b->push_threads = t;
+      b->push_box = box;
       b->adi_ctas = c;
       felis_status s = felis_batch_run(b, it, it + steps);
       if (s != FELIS_OK) return s;
       it += steps;
       const double per = b->last_run_ms / steps;
-      if (per < best) { best = per; pick = std::make_pair(t, c); }
+      if (per < best) { best = per; pick = std::make_pair(box, c); }
     }
-  std::tie(b->push_threads, b->adi_ctas) = pick;
-  cache[key] = pick;
+  }
+  std::tie(b->push_box, b->adi_ctas) = pick;
+  {
+    std::lock_guard<std::mutex> lock(g_tune_mu);
+    g_tune[key] = pick;
+    tune_store(key, pick);
+  }
   *next_it = it;
   return FELIS_OK;
 }

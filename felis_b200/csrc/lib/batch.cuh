@@ -79,6 +79,8 @@ struct BStep {
   float2 sfac[FELIS_MAX_HARMONY][2];  // ADI source factor per harmonic and polarisation
 };
 
+constexpr int kPushThreads = 128;  // threads per CTA of the push launch
+
 struct BatchLaunch {
   const BInst* inst;
   const BStep* step;  // [ninst] for this iteration
@@ -101,7 +103,9 @@ cudaError_t launch_f32_to_f64(const float* src, double* dst, int64_t n, double o
 cudaError_t launch_field_to_f32(const double* src, float2* U, int s0, int ns, int S, int N, int ring_base,
                                 cudaStream_t st);
 // H: the largest harmonic count of the ensemble (selects the kernel instance).
-void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st);
+// The push launch: 128 threads per CTA (kPushThreads), the instance of the
+// ensemble's largest harmonic count H and Ez mode count L.
+void launch_batch_push(const BatchLaunch& a, int H, int L, cudaStream_t st);
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st);
 // Per instance {sum |U|^2, Re, Im sum conj(U_s) U_{s+1}} of harmonic index
 // hidx over slices (bunch order from ring[i]), cells and polarisations.
@@ -117,9 +121,8 @@ size_t batch_adi_smem(int nx, int ny, int src_cells);
 // Shared memory of the push launch with room for the accumulators of
 // `box_cells` source cells of every source plane.
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells);
-cudaError_t batch_set_smem(int H, int adi_bytes, int push_bytes);
+cudaError_t batch_set_smem(int H, int L, int adi_bytes, int push_bytes);
 // CTAs of each kernel that fit on one SM with this shape.
 int batch_resident_adi(int threads, int smem_bytes);
-int batch_resident_push(int H, int threads, int smem_bytes);
 
 }  // namespace felis

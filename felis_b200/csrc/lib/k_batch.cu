@@ -672,8 +672,17 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
   }
 }
 
+// One register budget per (harmonic class, Ez-mode class) instance, the same
+// for every launch shape: 128 threads per CTA and as many CTAs per SM as a
+// 1024-slice step needs to run in one wave on 148 SMs where the registers
+// allow it (seven for one harmonic: 72 registers).
 template <int HM>
-__global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
+struct PushBlocks {
+  static constexpr int value = HM == 1 ? 7 : (HM == 2 ? 5 : 4);
+};
+
+template <int HM, int LM>
+__global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_push(BatchLaunch a) {
   extern __shared__ __align__(16) unsigned char sm[];
   __shared__ double redd[8];
   __shared__ float redf[8];
@@ -797,10 +806,12 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     }
     __syncthreads();
     const float4* m4 = reinterpret_cast<const float4*>(smap);
-    double acc7[7] = {0, 0, 0, 0, 0, 0, 0};
-    double bre[HM], bim[HM];
+    // twiss / bunching partial sums: FP32 over a thread's particles (64 per
+    // thread on the 8192-particle slices), FP64 across threads
+    float acc7[7] = {0, 0, 0, 0, 0, 0, 0};
+    float bre[HM], bim[HM];
 #pragma unroll
-    for (int h = 0; h < HM; ++h) { bre[h] = 0.0; bim[h] = 0.0; }
+    for (int h = 0; h < HM; ++h) { bre[h] = 0.f; bim[h] = 0.f; }
     double wsum = 0.0;
     int bad_over = 0, bad_range = 0, bad_nan = 0, bad_radial = 0;
     // the next particle's state is loaded one iteration ahead
@@ -868,12 +879,14 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
           }
           const float r = sqrtf(r2);
           const int ir = (int)(r / dr + 0.5f);
-          float2 Em[4] = {make_float2(0, 0), make_float2(0, 0), make_float2(0, 0), make_float2(0, 0)};
+          float2 Em[LM];
+#pragma unroll
+          for (int l = 0; l < LM; ++l) Em[l] = make_float2(0.f, 0.f);
           if (ir >= 0 && ir < nr) {
             const float wr1 = ir > 0 ? (r2 * idr2 - (float)(ir * ir)) / (2.f * ir) : 1.f;
             const float wr0 = ir > 0 ? 1.f - wr1 : 1.f;
 #pragma unroll
-            for (int l = 0; l < 4; ++l) {
+            for (int l = 0; l < LM; ++l) {
               if (l >= L) break;
               for (int f = 0; f < F; ++f) {
                 const float2 a0 = sEz[(l * F + f) * nr + ir];
@@ -899,7 +912,7 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
             const float inv2 = 1.f / ((1.f + d) * (1.f + d));
             float sumEz = 0.f, sumTh = 0.f, sumG = 0.f;
 #pragma unroll
-            for (int l = 0; l < 4; ++l) {
+            for (int l = 0; l < LM; ++l) {
               if (l >= L) break;
               const float2 e = expif((l + 1.f) * tm);
               sumEz += 2.f * (Em[l].x * e.x - Em[l].y * e.y);
@@ -943,15 +956,15 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
       xs[n] = x; ys[n] = y; pxs[n] = px; pys[n] = py; dgs[n] = dg; ths[n] = th;
       // twiss / bFactor partial sums of the new state (twiss.cpp, saveFile.cpp)
       const float ig = 1.f / (gRf + dg), xp = px * ig, yp = py * ig;
-      acc7[0] += (double)(x * x); acc7[1] += (double)(y * y); acc7[2] += (double)(xp * xp);
-      acc7[3] += (double)(yp * yp); acc7[4] += (double)(x * xp); acc7[5] += (double)(y * yp); acc7[6] += 1.0;
+      acc7[0] += x * x; acc7[1] += y * y; acc7[2] += xp * xp;
+      acc7[3] += yp * yp; acc7[4] += x * xp; acc7[5] += y * yp; acc7[6] += 1.f;
       const float thn = theta_red(th);
 #pragma unroll
       for (int h = 0; h < HM; ++h) {
         if (h >= H) break;
         const float2 e = expif((float)hh[h] * thn);
-        bre[h] += (double)e.x;
-        bim[h] += (double)e.y;
+        bre[h] += e.x;
+        bim[h] += e.y;
       }
       if (dep) stats(gx, gy, ii, jj, x, y, px, py, gRf + dg);
     }
@@ -963,13 +976,13 @@ __global__ void __launch_bounds__(256, 2) k_batch_push(BatchLaunch a) {
     double* out = I.part_b + (size_t)s * stride;
 #pragma unroll
     for (int k = 0; k < 7; ++k) {
-      const double t = block_sum_d(acc7[k], redd);
+      const double t = block_sum_d((double)acc7[k], redd);
       if (tid == 0) out[k] = t;
     }
 #pragma unroll
     for (int h = 0; h < HM; ++h) {
       if (h >= H) break;
-      const double tr = block_sum_d(bre[h], redd), ti = block_sum_d(bim[h], redd);
+      const double tr = block_sum_d((double)bre[h], redd), ti = block_sum_d((double)bim[h], redd);
       if (tid == 0) { out[7 + 2 * h] = tr * weight; out[8 + 2 * h] = ti * weight; }
     }
     const double tw = block_sum_d(wsum, redd);
@@ -1201,14 +1214,17 @@ __global__ void __launch_bounds__(256) k_batch_spectrum(const BInst* inst, const
   }
 }
 
-// Instances by the largest harmonic count (sizes of the register arrays).
+// Instances by the largest harmonic count and the largest number of
+// longitudinal Ez modes (sizes of the register arrays).
 typedef void (*PushKernel)(BatchLaunch);
-PushKernel push_kernel(int H) {
-  if (H <= 1) return k_batch_push<1>;
-  if (H <= 2) return k_batch_push<2>;
-  if (H <= 4) return k_batch_push<4>;
-  return k_batch_push<FELIS_MAX_HARMONY>;
+template <int LM>
+PushKernel push_kernel_l(int H) {
+  if (H <= 1) return k_batch_push<1, LM>;
+  if (H <= 2) return k_batch_push<2, LM>;
+  if (H <= 4) return k_batch_push<4, LM>;
+  return k_batch_push<FELIS_MAX_HARMONY, LM>;
 }
+PushKernel push_kernel(int H, int L) { return L <= 1 ? push_kernel_l<1>(H) : push_kernel_l<4>(H); }
 
 }  // namespace
 
@@ -1232,21 +1248,15 @@ size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
   return head + area;
 }
 
-cudaError_t batch_set_smem(int H, int adi_bytes, int push_bytes) {
+cudaError_t batch_set_smem(int H, int L, int adi_bytes, int push_bytes) {
   cudaError_t e = cudaFuncSetAttribute(k_batch_adi, cudaFuncAttributeMaxDynamicSharedMemorySize, adi_bytes);
-  if (e == cudaSuccess) e = cudaFuncSetAttribute(push_kernel(H), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
+  if (e == cudaSuccess) e = cudaFuncSetAttribute(push_kernel(H, L), cudaFuncAttributeMaxDynamicSharedMemorySize, push_bytes);
   return e;
 }
 
 int batch_resident_adi(int threads, int smem_bytes) {
   int n = 0;
   if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, k_batch_adi, threads, smem_bytes) != cudaSuccess) return 0;
-  return n;
-}
-
-int batch_resident_push(int H, int threads, int smem_bytes) {
-  int n = 0;
-  if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&n, push_kernel(H), threads, smem_bytes) != cudaSuccess) return 0;
   return n;
 }
 
@@ -1300,8 +1310,8 @@ void launch_batch_adi(const BatchLaunch& a, int threads, cudaStream_t st) {
   if (a.nwork > 0) k_batch_adi<<<a.nwork, threads, a.smem_bytes, st>>>(a);
 }
 
-void launch_batch_push(const BatchLaunch& a, int H, int threads, cudaStream_t st) {
-  if (a.nwork > 0) push_kernel(H)<<<a.nwork, threads, a.smem_bytes, st>>>(a);
+void launch_batch_push(const BatchLaunch& a, int H, int L, cudaStream_t st) {
+  if (a.nwork > 0) push_kernel(H, L)<<<a.nwork, kPushThreads, a.smem_bytes, st>>>(a);
 }
 
 void launch_batch_measure(const BInst* inst, const BStep* step, const int4* work, int nwork, cudaStream_t st) {

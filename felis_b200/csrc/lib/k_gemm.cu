@@ -12,11 +12,11 @@
 //              aligned); one lane issues tcgen05.mma (M = 128, N, K = 16; four
 //              per chunk) and commits each stage back to the producer and each
 //              finished accumulator to the epilogue
-//   warps 2-5  the epilogue: warp w reads lanes 32 (w % 4) .. + 31 of the
-//              accumulator (tcgen05.ld, one row per thread, 32 columns at a
-//              time), applies bias / GELU, stages the 32 x 32 block in its
-//              own shared memory and writes it back one row per instruction
-//              (coalesced), then frees the accumulator
+//   warps 2-9  the epilogue: warp w reads lanes 32 (w % 4) .. + 31 of the
+//              accumulator (tcgen05.ld, one row per thread), two warps per
+//              lane quarter taking alternate 32-column chunks; each thread
+//              applies bias / GELU to its 32 values and writes them with
+//              16-byte stores, then the warps free the accumulator
 // The two accumulators alternate, so a tile's epilogue overlaps the next
 // tile's loads and MMAs.  Every mbarrier wait is bounded: one that runs out
 // sets the error word and the flag that stops the other roles; the MMA lane
@@ -35,8 +35,8 @@ namespace {
 constexpr int kBM = 128;          // rows of a C tile (the MMA M)
 constexpr int kBK = 64;           // K columns per stage: 128 bytes of BF16, the swizzle span
 constexpr int kStages = 4;
-constexpr int kThreads = 192;     // 6 warps
-constexpr int kEpiPitch = 33;     // epilogue staging row pitch (floats): conflict-free columns
+constexpr int kEpiWarps = 8;
+constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr int kWaitTries = 1 << 20;
 constexpr uint32_t kABytes = kBM * kBK * 2;  // 16 KB
 
@@ -146,7 +146,6 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tma(const __grid_constant_
   const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
   const int N = g.N;
   const uint32_t stage_bytes = kABytes + (uint32_t)N * kBK * 2;
-  float* epi = reinterpret_cast<float*>(sm + (size_t)kStages * stage_bytes);
   const int ntiles = g.M / kBM;
   const int nk = (g.K + kBK - 1) / kBK;
   volatile int* abort_v = &abort_flag;
@@ -158,7 +157,7 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tma(const __grid_constant_
     }
     for (int b = 0; b < 2; ++b) {
       mbar_init(sa(&tfull[b]), 1);
-      mbar_init(sa(&tempty[b]), 4 * 32);
+      mbar_init(sa(&tempty[b]), kEpiWarps * 32);
     }
     abort_flag = 0;
     asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
@@ -236,8 +235,8 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tma(const __grid_constant_
     }
     __syncwarp();
   } else {
-    const int q = warp & 3;  // tensor-memory lane quarter this warp may read
-    float* stg = epi + (size_t)(warp - 2) * 32 * kEpiPitch;
+    const int q = warp & 3;            // tensor-memory lane quarter this warp may read
+    const int half = (warp - 2) >> 2;  // which of the two warps of that quarter
     int it = 0;
     for (int t = blockIdx.x; t < ntiles; t += gridDim.x, ++it) {
       const int b = it & 1;
@@ -245,26 +244,45 @@ __global__ void __launch_bounds__(kThreads, 1) k_gemm_tma(const __grid_constant_
       if (!mbar_wait(sa(&tfull[b]), bph, abort_v)) { give_up(); break; }
       asm volatile("tcgen05.fence::after_thread_sync;\n" ::: "memory");
       const uint32_t tbase = tmem + ((uint32_t)(q * 32) << 16) + (uint32_t)(b * g.acc_stride);
-      const size_t row0 = (size_t)t * kBM + (size_t)q * 32;
-      for (int c0 = 0; c0 < N; c0 += 32) {
+      const size_t row = (size_t)t * kBM + (size_t)q * 32 + lane;
+      for (int c0 = 32 * half; c0 < N; c0 += 64) {
         uint32_t r[32];
         TMEM_LD32X32(tbase + (uint32_t)c0, r);
         asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
+        const int ncol = N - c0 < 32 ? N - c0 : 32;  // 16 or 32 (N is a multiple of 16)
+        float v[32];
 #pragma unroll
-        for (int j = 0; j < 32; ++j) stg[lane * kEpiPitch + j] = __uint_as_float(r[j]);
-        __syncwarp();
-        const int col = c0 + lane;
-        if (col < N) {
+        for (int j = 0; j < 32; ++j) {
+          const int col = c0 + j;
           const bool valid = col < g.n_valid;
-          const float bb = (valid && g.bias) ? g.bias[col] : 0.f;
-          for (int rr = 0; rr < 32; ++rr) {
-            const float v = valid ? stg[rr * kEpiPitch + lane] + bb : 0.f;
-            const size_t o = (row0 + rr) * (size_t)g.ldc + col;
-            if (g.out_f32) g.out_f32[o] = v;
-            if (g.out_bf16) g.out_bf16[o] = __float2bfloat16_rn(g.gelu && valid ? gelu_f(v) : v);
+          v[j] = valid ? __uint_as_float(r[j]) + (g.bias ? __ldg(g.bias + col) : 0.f) : 0.f;
+        }
+        const size_t o = row * (size_t)g.ldc + c0;
+        if (g.out_f32) {
+          float4* dst = reinterpret_cast<float4*>(g.out_f32 + o);
+#pragma unroll
+          for (int j = 0; j < 8; ++j)
+            if (4 * j < ncol) dst[j] = make_float4(v[4 * j], v[4 * j + 1], v[4 * j + 2], v[4 * j + 3]);
+        }
+        if (g.out_bf16) {
+          uint4* dst = reinterpret_cast<uint4*>(g.out_bf16 + o);
+#pragma unroll
+          for (int j = 0; j < 4; ++j) {
+            if (8 * j >= ncol) break;
+            uint32_t w[4];
+#pragma unroll
+            for (int k = 0; k < 4; ++k) {
+              float x0 = v[8 * j + 2 * k], x1 = v[8 * j + 2 * k + 1];
+              if (g.gelu) {
+                if (c0 + 8 * j + 2 * k < g.n_valid) x0 = gelu_f(x0);
+                if (c0 + 8 * j + 2 * k + 1 < g.n_valid) x1 = gelu_f(x1);
+              }
+              const __nv_bfloat162 p2 = __floats2bfloat162_rn(x0, x1);
+              w[k] = *reinterpret_cast<const uint32_t*>(&p2);
+            }
+            dst[j] = make_uint4(w[0], w[1], w[2], w[3]);
           }
         }
-        __syncwarp();
       }
       asm volatile("tcgen05.fence::before_thread_sync;\n" ::: "memory");
       mbar_arrive(sa(&tempty[b]));
@@ -282,9 +300,7 @@ typedef CUresult (*EncodeTiledFn)(CUtensorMap*, CUtensorMapDataType, cuuint32_t,
 EncodeTiledFn g_encode = nullptr;
 int g_sms = 0;
 
-size_t tma_smem(int N) {
-  return 1024 + (size_t)kStages * (kABytes + (size_t)N * kBK * 2) + (size_t)4 * 32 * kEpiPitch * sizeof(float);
-}
+size_t tma_smem(int N) { return 1024 + (size_t)kStages * (kABytes + (size_t)N * kBK * 2); }
 
 // Row-major BF16 matrix [rows][ld] read in (64 x box_rows) tiles of its
 // first `cols` columns; out-of-range elements read as zero.

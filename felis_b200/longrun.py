@@ -128,7 +128,7 @@ def run_mixed(cfg, beam, fields, steps: int, chunk: int, tune_steps: int = 4) ->
         spec = _spectra(lambda k, pol: b.download_field(0, k, pol), p.num_harmony)
     finally:
         b.close()
-    return {"energy": e, "spectra": spec, "ms": ms, "launch": {"push_threads": launch[0], "adi_ctas_per_sm": launch[1]}}
+    return {"energy": e, "spectra": spec, "ms": ms, "launch": {"push_box_cells": launch[0], "adi_ctas_per_sm": launch[1]}}
 
 
 def compare(ref: dict, mix: dict, H: int, harmonics: list[int], dz: float) -> dict:

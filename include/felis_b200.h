@@ -360,15 +360,20 @@ felis_status felis_batch_get_diagnostics(felis_batch* b, int32_t inst, int32_t i
  * units of the slice frequency.  Instances without harmonic index hidx give
  * zeros.  (No reference counterpart: the reference writes fields to disk.) */
 felis_status felis_batch_spectral_moments(felis_batch* b, int32_t hidx, double* out);
-/* Launch shape: threads per CTA of the push launch (128 or 256) and the CTAs
- * per SM that the ADI launch sizes its shared memory for (1 or 2; the rest of
- * the shared memory stages the slice's source box). */
-felis_status felis_batch_set_launch(felis_batch* b, int32_t push_threads, int32_t adi_ctas);
-felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_threads, int32_t* adi_ctas);
+/* Launch shape: the source cells the push launch stages in shared memory
+ * (512 .. 6144, default 3072: seven one-harmonic push CTAs of 128 threads share
+ * an SM; larger areas take fewer cells of wide beams through global memory)
+ * and the CTAs per SM the ADI launch sizes its shared memory for (1 or 2; the
+ * rest stages the slice's source box).  Results do not depend on it. */
+felis_status felis_batch_set_launch(felis_batch* b, int32_t push_box, int32_t adi_ctas);
+felis_status felis_batch_get_launch(felis_batch* b, int32_t* push_box, int32_t* adi_ctas);
 /* Tries each launch shape for `steps` real iterations starting at it0 (the
  * ensemble advances; results do not depend on the shape), keeps the fastest
  * and returns the next iteration to run in *next_it.  Shapes are cached per
- * ensemble geometry: a second call on a matching ensemble runs nothing. */
+ * ensemble geometry and GPU kind, in memory and in the text file named by
+ * FELIS_TUNE_CACHE ($HOME/.cache/felis_b200_batch_tune_v2.txt by default): a
+ * later call on a matching ensemble, in this process or another, runs
+ * nothing. */
 felis_status felis_batch_tune(felis_batch* b, int32_t it0, int32_t steps, int32_t* next_it);
 /* Device time of the last felis_batch_run graph launch. */
 felis_status felis_batch_last_run_ms(felis_batch* b, double* ms);

@@ -163,7 +163,7 @@ def test_instances_independent(fb, tmp_path):
 def test_launch_shape_and_rerun_invariant(fb, seeded):
     cfg, beam, fields = seeded
     res = []
-    for shape in ((256, 2), (128, 1), (128, 2)):
+    for shape in ((6144, 2), (3072, 1), (1024, 2)):
         b = fb.Batch([cfg.params])
         _upload(fb, b, 0, cfg, beam, fields)
         b.set_launch(*shape)
@@ -175,7 +175,7 @@ def test_launch_shape_and_rerun_invariant(fb, seeded):
     # the same shape twice: every bit, diagnostics included
     b = fb.Batch([cfg.params])
     _upload(fb, b, 0, cfg, beam, fields)
-    b.set_launch(256, 2)
+    b.set_launch(6144, 2)
     b.run(0, 40)
     _same(res[0][0], _state(b, 0, 1), "rerun")
     for x, y in zip(res[0][1], b.diagnostics(0, 0, 41)):
