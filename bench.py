@@ -787,6 +787,8 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=20,
                     help="timed iterations of the Gaussian-current tapered run (0: skip)")
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
+    ap.add_argument("--surrogate-only", action="store_true",
+                    help="the surrogate ranking GEMM chain alone (profiling captures)")
     args = ap.parse_args()
     if args.warmup < 3:
         ap.error("--warmup must be >= 3")
@@ -806,6 +808,9 @@ def main():
         }), flush=True)
         return
 
+    if args.surrogate_only:
+        print(json.dumps(run_surrogate_gemm(args.surrogate_rows)), flush=True)
+        return
     dist, rank, world = dist_init()
     line = run_felis(args, dist, rank, world)
     if not args.fp64_only:
