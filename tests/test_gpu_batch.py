@@ -219,7 +219,9 @@ def test_tune_advances_and_caches(fb, seeded):
     b = fb.Batch([cfg.params])
     _upload(fb, b, 0, cfg, beam, fields)
     nxt = b.tune(0, 2)
-    assert nxt >= 8  # 4 shapes x 2 iterations, after the first deposit
+    # the first deposit, then 2 iterations under each of ADI CTAs/SM 1 and 2 at the
+    # one staged source area a 42 x 42 grid needs
+    assert nxt == 1 + 2 * 2
     b.run(nxt, nxt + 4)
     ref = fb.Batch([cfg.params])
     _upload(fb, ref, 0, cfg, beam, fields)
