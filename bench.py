@@ -137,7 +137,9 @@ class ClockSampler:
                 "reasons": sorted(reasons), "samples": len(sm)}
 
 
-def make_config(name: str, slices: int | None = None, grid: int | None = None):
+def make_config(name: str, slices: int | None = None, grid: int | None = None, world: int = 1, rank: int = 0):
+    """The workload's input file parsed for `rank` of `world` slice blocks
+    (one block: the whole bunch)."""
     import felis_b200 as fb
     from felis_b200 import workloads
 
@@ -147,7 +149,7 @@ def make_config(name: str, slices: int | None = None, grid: int | None = None):
         kw["slices"] = slices
     if grid:
         kw["nx"] = grid
-    return fb.Config(workloads.write_input(os.path.join(d, f"{name}.inp"), **kw))
+    return fb.Config(workloads.write_input(os.path.join(d, f"{name}.inp"), **kw), world, rank)
 
 
 def workload_config(name: str, p, P: int, W: int, K: int, world: int, precision: str) -> dict:
@@ -332,6 +334,87 @@ def cpu_sample(name: str, steps: int, warmup: int, target_s: float, threads: int
               f"{warmup}..{warmup + nsteps - 1} after {warmup} untimed, {dt:.1f} s timed on {threads} threads; "
               f"CPU restatement, build '{variant}' (reference compiler flags)")
     return value, sample, "port"
+
+
+def run_sharded(args, dist, rank, world):
+    """One FP64 run of the workload with its slices split into contiguous
+    blocks, one per rank (boundary.cpp:33-46; strong scaling: the bunch is
+    fixed, each rank steps 1/N of it).  After every shifted iteration the
+    slipping slice's planes go to the next rank in device memory
+    (fieldShareZ.cpp:39-78: NCCL send / receive on the handle's stream,
+    felis_b200.shard), rank 0 takes zeros.  Each step is one drop-in
+    felis_step call; the diagnostics stay on the device in the timed region
+    and are reduced over the ranks afterwards (updateTotalEnergy.cpp:56-68)."""
+    import numpy as np
+    import torch
+
+    import felis_b200 as fb
+    from felis_b200 import shard
+
+    cfg = make_config(args.workload, args.slices, args.grid, world, rank)
+    p = cfg.params
+    beam = cfg.load_beam(0, seed=2 if args.workload == "sase" else 1)
+    fields = [cfg.load_seed(h) for h in range(p.num_harmony)]
+    P = int(beam["offsets"][-1])
+    h = fb.Handle(p)
+    h.upload_particles(0, beam["x"], beam["y"], beam["px"], beam["py"], beam["theta"], beam["gamma"],
+                       beam["offsets"], beam["weights"])
+    for hh, (ux, uy) in enumerate(fields):
+        h.upload_field(hh, 0, ux)
+        h.upload_field(hh, 1, uy)
+    del beam, fields
+    eng = shard.GpuEngine(h)
+    loop = shard.ShardedLoop(eng, dist, rank, world) if dist is not None else None
+    st = eng.stream()
+
+    def advance(it0, it1):
+        for it in range(it0, it1):
+            if eng.step(it):
+                if loop is not None:
+                    loop.exchange()
+                else:
+                    shard.exchange_in_process([eng])  # one block: the first slice takes zeros
+
+    W, K = args.warmup, args.steps
+    advance(0, W)
+    h.sync()
+    h.profile(True, max_launches=16 * K + 64)  # launch counts of the timed region
+    barrier(dist)
+    torch.cuda.synchronize()
+    clocks = ClockSampler(int(os.environ.get("LOCAL_RANK", "0")))
+    time.sleep(0.3)
+    e0, e1 = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    e0.record(st)
+    advance(W, W + K)
+    e1.record(st)
+    h.sync()
+    torch.cuda.synchronize()
+    clk = clocks.stop()
+    barrier(dist)
+    ms = max_over_ranks(dist, e0.elapsed_time(e1))
+    e, _, _ = h.diagnostics(W, W + K)
+    total = np.array([float(P)] + list(e[-1]), dtype=np.float64)
+    if dist is not None:
+        t = torch.from_numpy(total).cuda()
+        dist.all_reduce(t)
+        total = t.cpu().numpy()
+    particles = int(total[0])
+    value = particles * K / (ms / 1e3)
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": world, "steps": K, "warmup": args.warmup,
+        "ms_per_step": ms / K, "higher_is_better": True, "scaling": "strong", "vs_baseline": None,
+        "dtype": "f64", "data": "synthetic (seeded beam loader of the reference input format, per slice block)",
+        "config": {"workload": f"{args.workload}: FP64 time-dependent SASE, {p.global_slice_n} slices split into "
+                               f"{world} blocks, {particles} particles, {p.nx}x{p.ny} grid, H={p.num_harmony}",
+                   "slices": p.global_slice_n, "particles": particles, "grid": [p.nx, p.ny],
+                   "iterations": [W, W + K], "parallelism": f"slice blocks x{world}",
+                   "exchange": "device memory, NCCL send/recv on the library stream" if world > 1 else "none",
+                   "l2": "inputs larger than L2"},
+        "final_power_units": float(total[1]), "clocks": clk, "gpu_launches": h.kernel_stats(-1)[0],
+        "cpu_baseline": None, "e2e": None,
+    }
+    h.close()
+    return line
 
 
 def run_felis(args, dist, rank, world):
@@ -787,6 +870,8 @@ def main():
     ap.add_argument("--config3-steps", type=int, default=20,
                     help="timed iterations of the Gaussian-current tapered run (0: skip)")
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
+    ap.add_argument("--sharded", action="store_true",
+                    help="one FP64 run with its slices split over the ranks (strong scaling, device halo exchange)")
     ap.add_argument("--surrogate-only", action="store_true",
                     help="the surrogate ranking GEMM chain alone (profiling captures)")
     args = ap.parse_args()
@@ -812,6 +897,13 @@ def main():
         print(json.dumps(run_surrogate_gemm(args.surrogate_rows)), flush=True)
         return
     dist, rank, world = dist_init()
+    if args.sharded:
+        line = run_sharded(args, dist, rank, world)
+        if rank == 0:
+            print(json.dumps(line), flush=True)
+        if dist is not None:
+            dist.destroy_process_group()
+        return
     line = run_felis(args, dist, rank, world)
     if not args.fp64_only:
         cfg, beam, fields = make_workload(args.workload, rank, args.slices, args.grid)

@@ -148,6 +148,7 @@ _sig("felis_mlp_get_params", C.c_int, _vp, _fp)
 _sig("felis_mlp_set_params", C.c_int, _vp, _fp)
 _sig("felis_mlp_forward", C.c_int, _vp, _fp, C.c_int64, _fp)
 _sig("felis_mlp_last_forward", C.c_int, _vp, _dp, _dp)
+_sig("felis_mlp_set_fused", C.c_int, _vp, C.c_int32)
 _sig("felis_mlp_gradients", C.c_int, _vp, _fp, _fp, C.c_int64, _fp, _dp)
 _sig("felis_mlp_set_data", C.c_int, _vp, _fp, _fp, C.c_int64)
 _sig("felis_mlp_train", C.c_int, _vp, C.c_int32, C.c_int32, C.c_float, C.c_float, C.c_uint64, _dp)
@@ -715,6 +716,11 @@ class MLP:
         ms, fl = C.c_double(), C.c_double()
         self._ck(_lib.felis_mlp_last_forward(self._m, C.byref(ms), C.byref(fl)))
         return ms.value, fl.value
+
+    def set_fused(self, enable: bool):
+        """Inference by the fused four-layer kernel (the default where the
+        shape allows it) or by the layer-by-layer GEMM chain."""
+        self._ck(_lib.felis_mlp_set_fused(self._m, 1 if enable else 0))
 
     def forward(self, x) -> np.ndarray:
         x = _f32(x).reshape(-1, self.n_in)

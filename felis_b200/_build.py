@@ -39,6 +39,7 @@ UNITS = [
     ("lib/mlp.cu", []),
     ("lib/k_mlp.cu", []),
     ("lib/k_gemm.cu", []),
+    ("lib/k_mlp_fused.cu", []),
     ("host/config.cpp", []),
 ]
 

@@ -660,6 +660,7 @@ felis_status check_batch_err(felis_batch* b) {
     else if (b->h_err[ERR_OUT_OF_RANGE]) s = bfail(b, FELIS_OUT_OF_RANGE, "theta outside [0, dTh] after the wrap");
     else if (b->h_err[ERR_NAN]) s = bfail(b, FELIS_NAN, "non-finite particle state");
     else if (b->h_err[ERR_RADIAL]) s = bfail(b, FELIS_UNSUPPORTED, "particle outside the radial Ez grid");
+    else if (b->h_err[ERR_TIMEOUT]) s = bfail(b, FELIS_TIMEOUT, "a bounded device wait ran out");
     if (s != FELIS_OK) {
       BCK(cudaMemset(I.err, 0, ERR_SLOTS * sizeof(int)));
       return s;

@@ -69,6 +69,7 @@ enum ErrSlot {
   ERR_RADIAL = 3,          // in-grid particle outside the radial Ez grid (Em carry-over case)
   ERR_EDGE_DEPOSIT = 4,    // q6 edge cells (count)
   ERR_DEPOSIT_CAPACITY = 5,
+  ERR_TIMEOUT = 6,         // a bounded device wait ran out
   ERR_SLOTS = 8
 };
 

@@ -105,6 +105,38 @@ __device__ __forceinline__ void cp_async8(void* dst_smem, const void* src) {
 }
 __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wait_all;\n" ::: "memory"); }
 
+// Bulk copies (the TMA engine's untiled form): one instruction moves a whole
+// row, both addresses 16-byte aligned and the size a multiple of 16 bytes; the
+// bytes are counted on an mbarrier whose wait is bounded.
+__device__ __forceinline__ unsigned smem_u32(const void* p) { return (unsigned)__cvta_generic_to_shared(p); }
+__device__ __forceinline__ void bar_init_tx(unsigned bar, unsigned bytes) {
+  asm volatile("mbarrier.init.shared::cta.b64 [%0], 1;\n" ::"r"(bar) : "memory");
+  asm volatile("fence.mbarrier_init.release.cluster;\n" ::: "memory");
+  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
+}
+__device__ __forceinline__ void bulk_g2s(void* dst_smem, const void* src, unsigned bytes, unsigned bar) {
+  asm volatile("cp.async.bulk.shared::cluster.global.mbarrier::complete_tx::bytes [%0], [%1], %2, [%3];\n" ::"r"(
+                   smem_u32(dst_smem)),
+               "l"(src), "r"(bytes), "r"(bar)
+               : "memory");
+}
+// Wait for phase 0 of the barrier, at most `tries` polls; false when it ran out.
+__device__ __forceinline__ bool bar_wait0(unsigned bar, int tries) {
+  for (int it = 0; it < tries; ++it) {
+    unsigned done;
+    asm volatile(
+        "{\n\t.reg .pred p;\n\t"
+        "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], 0;\n\t"
+        "selp.u32 %0, 1, 0, p;\n\t}\n"
+        : "=r"(done)
+        : "r"(bar)
+        : "memory");
+    if (done) return true;
+  }
+  return false;
+}
+constexpr int kBulkWaitTries = 1 << 20;
+
 // ---- fixed-point accumulation ------------------------------------------------
 constexpr int kAccBits = 31;
 
@@ -272,7 +304,18 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   float2* cb = cf + 3 * NL;                    // backward start values of chunks 1-3
   float2* ce = cb + 3 * NL;                    // backward end values of chunks 0-2 (x sweep)
   float2* ssrc = ce + 3 * NL;
-  for (int k = tid; k < 16 * Mx; k += nt) cp_async8(tb + k, ad + k);
+  // the 16 coefficient tables are one contiguous run: one bulk copy when both
+  // ends are 16-byte aligned (an even number of staged plane cells)
+  const bool tb_bulk = ((my * P) & 1) == 0 && (reinterpret_cast<uintptr_t>(ad) & 15) == 0;
+  __shared__ __align__(8) unsigned long long tbar;
+  if (tb_bulk) {
+    if (tid == 0) {
+      bar_init_tx(smem_u32(&tbar), (unsigned)(16 * Mx * sizeof(float2)));
+      bulk_g2s(tb, ad, (unsigned)(16 * Mx * sizeof(float2)), smem_u32(&tbar));
+    }
+  } else {
+    for (int k = tid; k < 16 * Mx; k += nt) cp_async8(tb + k, ad + k);
+  }
   {
     const int lane = tid & 31, warp = tid >> 5, nwarp = nt >> 5;
     for (int r = warp; r < my; r += nwarp)
@@ -303,6 +346,10 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   }
   const bool src = Sc != nullptr;
   cp_async_wait_all();
+  if (tb_bulk && !bar_wait0(smem_u32(&tbar), kBulkWaitTries)) {
+    atomicOr(I.err + ERR_TIMEOUT, 1);
+    bar_wait0(smem_u32(&tbar), kBulkWaitTries);  // once more for the copy in flight
+  }
   __syncthreads();
   const float2 zero = make_float2(0.f, 0.f);
   const int* K8 = I.adi_k[h];
@@ -688,6 +735,7 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   __shared__ float redf[8];
   __shared__ int redi[8];
   __shared__ __align__(16) float smap[48];  // transverse map: D0, M1, M2 (row-major 4x4 each)
+  __shared__ __align__(8) unsigned long long fbar;  // bulk staging of the field box
   const int4 wi = a.work[blockIdx.x];
   const BInst& I = a.inst[wi.x];
   const BStep& T = a.step[wi.x];
@@ -789,20 +837,52 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
     const float2* sF = reinterpret_cast<const float2*>(area);
     {
       const int4 b = I.sbox[s];
+      // On an even-width grid every row of every plane starts on a 16-byte
+      // boundary (the planes hold an even number of cells): the box, widened
+      // to an even first and an odd last column, is staged by the bulk-copy
+      // engine, one copy per row.  Otherwise by 8-byte cp.async per cell.
+      const bool bulk = (nx & 1) == 0 && ((reinterpret_cast<uintptr_t>(Ubase) & 15) == 0);
+      bool bulk_used = false;
       if (b.y >= b.x && b.w >= b.z) {
         int i0 = max(0, b.x - 3), i1 = min(nx - 1, b.y + 3), j0 = max(0, b.z - 3), j1 = min(ny - 1, b.w + 3);
         // a box too large for the area: its central window (the beam's core)
-        shrink_window(i0, i1, j0, j1, (int)(area_bytes / ((size_t)2 * H * sizeof(float2))));
-        const int w = i1 - i0 + 1, cells = w * (j1 - j0 + 1);
+        const int cap = (int)(area_bytes / ((size_t)2 * H * sizeof(float2)));
+        if (bulk) {
+          i0 &= ~1; i1 |= 1;
+          if ((i1 - i0 + 1) * (j1 - j0 + 1) > cap) {
+            // re-widening the window adds at most one column either side
+            shrink_window(i0, i1, j0, j1, cap - 2 * (j1 - j0 + 1));
+            if (i1 >= i0) { i0 &= ~1; i1 |= 1; }
+          }
+        } else {
+          shrink_window(i0, i1, j0, j1, cap);
+        }
+        const int w = i1 - i0 + 1, rows = j1 - j0 + 1, cells = w * rows;
         if (i1 >= i0 && j1 >= j0) {
           fi0 = i0; fi1 = i1; fj0 = j0; fj1 = j1; fbw = w; fcells = cells;
           float2* dst = reinterpret_cast<float2*>(area);
-          for (int hp = 0; hp < 2 * H; ++hp)
-            for (int k = tid; k < cells; k += nt)
-              cp_async8(dst + (size_t)hp * cells + k, Ubase + hp * hpstride + (size_t)(j0 + k / w) * nx + i0 + k % w);
+          if (bulk) {
+            bulk_used = true;
+            if (tid == 0) bar_init_tx(smem_u32(&fbar), (unsigned)(2 * H * cells * sizeof(float2)));
+            __syncthreads();
+            for (int k = tid; k < 2 * H * rows; k += nt) {
+              const int hp = k / rows, r = k - hp * rows;
+              bulk_g2s(dst + (size_t)hp * cells + (size_t)r * w, Ubase + hp * hpstride + (size_t)(j0 + r) * nx + i0,
+                       (unsigned)(w * sizeof(float2)), smem_u32(&fbar));
+            }
+          } else {
+            for (int hp = 0; hp < 2 * H; ++hp)
+              for (int k = tid; k < cells; k += nt)
+                cp_async8(dst + (size_t)hp * cells + k,
+                          Ubase + hp * hpstride + (size_t)(j0 + k / w) * nx + i0 + k % w);
+          }
         }
       }
       cp_async_wait_all();
+      if (bulk_used && !bar_wait0(smem_u32(&fbar), kBulkWaitTries)) {
+        atomicOr(I.err + ERR_TIMEOUT, 1);
+        bar_wait0(smem_u32(&fbar), kBulkWaitTries);  // once more for the copies in flight
+      }
     }
     __syncthreads();
     const float4* m4 = reinterpret_cast<const float4*>(smap);

@@ -27,102 +27,20 @@
 #include <stdint.h>
 
 #include "mlp.cuh"
+#include "tc.cuh"
 
 namespace felis {
 
 namespace {
+
+using namespace tc;
 
 constexpr int kBM = 128;          // rows of a C tile (the MMA M)
 constexpr int kBK = 64;           // K columns per stage: 128 bytes of BF16, the swizzle span
 constexpr int kStages = 4;
 constexpr int kEpiWarps = 8;
 constexpr int kThreads = 32 * (2 + kEpiWarps);
-constexpr int kWaitTries = 1 << 20;
 constexpr uint32_t kABytes = kBM * kBK * 2;  // 16 KB
-
-__device__ __forceinline__ uint32_t sa(const void* p) { return (uint32_t)__cvta_generic_to_shared(p); }
-
-__device__ __forceinline__ void mbar_init(uint32_t bar, uint32_t count) {
-  asm volatile("mbarrier.init.shared::cta.b64 [%0], %1;\n" ::"r"(bar), "r"(count) : "memory");
-}
-
-__device__ __forceinline__ bool mbar_try(uint32_t bar, uint32_t parity) {
-  uint32_t done;
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "mbarrier.try_wait.parity.shared::cta.b64 p, [%1], %2;\n\t"
-      "selp.u32 %0, 1, 0, p;\n\t}\n"
-      : "=r"(done)
-      : "r"(bar), "r"(parity)
-      : "memory");
-  return done != 0;
-}
-
-// Bounded wait; false when it ran out or another role gave up.
-__device__ __forceinline__ bool mbar_wait(uint32_t bar, uint32_t parity, volatile int* abort_flag) {
-  for (int it = 0; it < kWaitTries; ++it) {
-    if (mbar_try(bar, parity)) return true;
-    if ((it & 255) == 255 && *abort_flag) return false;
-  }
-  return false;
-}
-
-__device__ __forceinline__ void mbar_arrive(uint32_t bar) {
-  asm volatile("mbarrier.arrive.shared::cta.b64 _, [%0];\n" ::"r"(bar) : "memory");
-}
-
-__device__ __forceinline__ void mbar_expect_tx(uint32_t bar, uint32_t bytes) {
-  asm volatile("mbarrier.arrive.expect_tx.shared::cta.b64 _, [%0], %1;\n" ::"r"(bar), "r"(bytes) : "memory");
-}
-
-// 2-D tiled TMA load from this GPU's memory (no multicast); x is the element
-// column (a multiple of 64 here: 128 bytes), y the row.
-__device__ __forceinline__ void tma_load_2d(uint32_t dst, const CUtensorMap* map, int x, int y, uint32_t bar) {
-  asm volatile(
-      "cp.async.bulk.tensor.2d.shared::cluster.global.tile.mbarrier::complete_tx::bytes [%0], [%1, {%2, %3}], [%4];\n" ::"r"(dst),
-      "l"(reinterpret_cast<uint64_t>(map)), "r"(x), "r"(y), "r"(bar)
-      : "memory");
-}
-
-// Shared-memory descriptor of a K-major operand tile in the 128-byte swizzled
-// layout the TMA writes: 8-row groups 1024 bytes apart (stride byte offset),
-// layout type SWIZZLE_128B (2), descriptor version 1.
-__device__ __forceinline__ uint64_t desc_sw128(uint32_t addr) {
-  return (uint64_t)((addr & 0x3FFFFu) >> 4) | ((uint64_t)1 << 16) | ((uint64_t)(1024 >> 4) << 32) |
-         ((uint64_t)1 << 46) | ((uint64_t)2 << 61);
-}
-
-// Instruction descriptor of kind::f16: FP32 accumulator, BF16 A and B, both
-// K-major, dense, M x N.
-__device__ __forceinline__ uint32_t idesc_bf16(int M, int N) {
-  return (1u << 4) | (1u << 7) | (1u << 10) | ((uint32_t)(N >> 3) << 17) | ((uint32_t)(M >> 4) << 24);
-}
-
-__device__ __forceinline__ void mma_bf16(uint32_t d, uint64_t a, uint64_t b, uint32_t idesc, uint32_t acc) {
-  asm volatile(
-      "{\n\t.reg .pred p;\n\t"
-      "setp.ne.b32 p, %4, 0;\n\t"
-      "tcgen05.mma.cta_group::1.kind::f16 [%0], %1, %2, %3, p;\n\t}\n" ::"r"(d),
-      "l"(a), "l"(b), "r"(idesc), "r"(acc)
-      : "memory");
-}
-
-__device__ __forceinline__ void mma_commit(uint32_t bar) {
-  asm volatile("tcgen05.commit.cta_group::1.mbarrier::arrive::one.shared::cluster.b64 [%0];\n" ::"r"(bar) : "memory");
-}
-
-#define TMEM_LD32X32(taddr, r)                                                                                  \
-  asm volatile("tcgen05.ld.sync.aligned.32x32b.x32.b32 "                                                        \
-               "{%0,%1,%2,%3,%4,%5,%6,%7,%8,%9,%10,%11,%12,%13,%14,%15,"                                         \
-               "%16,%17,%18,%19,%20,%21,%22,%23,%24,%25,%26,%27,%28,%29,%30,%31}, [%32];\n"                       \
-               : "=r"(r[0]), "=r"(r[1]), "=r"(r[2]), "=r"(r[3]), "=r"(r[4]), "=r"(r[5]), "=r"(r[6]), "=r"(r[7]),  \
-                 "=r"(r[8]), "=r"(r[9]), "=r"(r[10]), "=r"(r[11]), "=r"(r[12]), "=r"(r[13]), "=r"(r[14]),         \
-                 "=r"(r[15]), "=r"(r[16]), "=r"(r[17]), "=r"(r[18]), "=r"(r[19]), "=r"(r[20]), "=r"(r[21]),       \
-                 "=r"(r[22]), "=r"(r[23]), "=r"(r[24]), "=r"(r[25]), "=r"(r[26]), "=r"(r[27]), "=r"(r[28]),       \
-                 "=r"(r[29]), "=r"(r[30]), "=r"(r[31])                                                            \
-               : "r"(taddr))
-
-__device__ __forceinline__ float gelu_f(float z) { return 0.5f * z * (1.f + erff(z * 0.70710678118654752f)); }
 
 struct TmaGemm {
   int M, N, K;     // M a multiple of 128, N a multiple of 16 (<= 256), K a multiple of 16
@@ -302,9 +220,10 @@ int g_sms = 0;
 
 size_t tma_smem(int N) { return 1024 + (size_t)kStages * (kABytes + (size_t)N * kBK * 2); }
 
-// Row-major BF16 matrix [rows][ld] read in (64 x box_rows) tiles of its
-// first `cols` columns; out-of-range elements read as zero.
-bool encode(CUtensorMap* map, const bf16* base, int rows, int cols, int ld, int box_rows) {
+}  // namespace
+
+bool tma_encode_bf16(CUtensorMap* map, const bf16* base, int rows, int cols, int ld, int box_rows) {
+  if (!g_encode) return false;
   const cuuint64_t dims[2] = {(cuuint64_t)cols, (cuuint64_t)rows};
   const cuuint64_t strides[1] = {(cuuint64_t)ld * 2};
   const cuuint32_t box[2] = {(cuuint32_t)kBK, (cuuint32_t)box_rows};
@@ -314,7 +233,7 @@ bool encode(CUtensorMap* map, const bf16* base, int rows, int cols, int ld, int 
                   CU_TENSOR_MAP_FLOAT_OOB_FILL_NONE) == CUDA_SUCCESS;
 }
 
-}  // namespace
+int gemm_sm_count() { return g_sms; }
 
 cudaError_t gemm_tma_prepare() {
   if (!g_encode) {
@@ -339,7 +258,7 @@ cudaError_t launch_gemm_tma(const GemmArgs& a, cudaStream_t st) {
       (reinterpret_cast<uintptr_t>(a.A) & 15) || (reinterpret_cast<uintptr_t>(a.B) & 15))
     return cudaErrorInvalidValue;
   CUtensorMap ta, tb;
-  if (!encode(&ta, a.A, a.M, a.K, a.lda, kBM) || !encode(&tb, a.B, a.N, a.K, a.ldb, a.N)) return cudaErrorInvalidValue;
+  if (!tma_encode_bf16(&ta, a.A, a.M, a.K, a.lda, kBM) || !tma_encode_bf16(&tb, a.B, a.N, a.K, a.ldb, a.N)) return cudaErrorInvalidValue;
   TmaGemm g;
   g.M = a.M; g.N = a.N; g.K = a.K;
   // two accumulators 32-column aligned (the epilogue reads 32 columns at a

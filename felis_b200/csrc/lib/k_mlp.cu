@@ -3,6 +3,7 @@
 #include <math.h>
 
 #include "mlp.cuh"
+#include "tc.cuh"
 
 namespace felis {
 
@@ -44,8 +45,12 @@ __global__ void __launch_bounds__(128) k_wait_selftest(int limit, int* timed_out
   if (threadIdx.x == 0) *timed_out = all_ran_out;
 }
 
+// Derivative of the tanh-form GELU of tc.cuh: with t = tanh(u),
+// u = c (z + a z^3): 0.5 (1 + t) + 0.5 z (1 - t^2) c (1 + 3 a z^2).
 __device__ __forceinline__ float gelu_grad(float z) {
-  return 0.5f * (1.f + erff(z * 0.70710678118654752f)) + z * 0.39894228040143268f * expf(-0.5f * z * z);
+  const float c = 0.79788456080286536f, a = 0.044715f;
+  const float t = tc::tanh_hw(c * fmaf(a * z, z * z, z));
+  return 0.5f * (1.f + t) + 0.5f * z * (1.f - t * t) * c * fmaf(3.f * a * z, z, 1.f);
 }
 
 __global__ void k_f32_to_bf16(const float* in, bf16* out, int64_t n) {

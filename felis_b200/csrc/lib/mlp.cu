@@ -36,7 +36,8 @@ struct felis_mlp {
   cudaStream_t st = nullptr;
   std::string err;
   int* d_err = nullptr;
-  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the GEMM chain of the last forward chunk
+  cudaEvent_t ev0 = nullptr, ev1 = nullptr;  // around the inference kernels of the last forward chunk
+  bool fused = false;                        // inference by the fused kernel (k_mlp_fused.cu)
   double fwd_ms = 0.0, fwd_flops = 0.0;
   // per layer: rows (outputs) x cols (inputs), padded
   int rows[kLayers], cols[kLayers], rows_real[kLayers], cols_real[kLayers];
@@ -163,6 +164,21 @@ void forward(felis_mlp* m, int M, bool keep_z = true) {
   }
 }
 
+// The inference pass of rows [0, M) of xb as one fused kernel; the output
+// goes where forward() leaves it (z of the last layer).
+void forward_fused(felis_mlp* m, int M) {
+  MlpFusedArgs a;
+  a.x = m->xb;
+  a.M = M; a.width = m->width; a.in_k = m->in_p; a.out_n = m->out_p;
+  for (int l = 0; l < kLayers; ++l) {
+    a.w[l] = m->wb[l];
+    a.bias[l] = m->p + m->b_off[l];
+  }
+  a.y = m->z[kLayers - 1];
+  a.err = m->d_err;
+  if (launch_mlp_fused(a, m->st) != cudaSuccess) cudaMemsetAsync(m->d_err, 0xff, sizeof(int), m->st);
+}
+
 // Gradients of the mean squared error over the first n_real rows of the
 // chunk (targets in tgt) into m->grad; returns the summed squared error.
 felis_status backward(felis_mlp* m, int M, int n_real, double* sse) {
@@ -252,6 +268,7 @@ felis_status felis_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64
   m->in_p = round_up(n_in, 16);
   m->out_p = round_up(n_out, 16);
   m->out_rows = round_up(m->out_p, 128);
+  m->fused = mlp_fused_supported(width, m->in_p, m->out_p);
   const int r[kLayers] = {width, width, width, m->out_p};
   const int c[kLayers] = {m->in_p, width, width, width};
   const int rr[kLayers] = {width, width, width, n_out};
@@ -284,6 +301,7 @@ felis_status felis_mlp_create(int32_t n_in, int32_t width, int32_t n_out, uint64
     if (e == cudaSuccess) e = cudaMalloc(&m->wt[l], (size_t)r[l] * c[l] * sizeof(bf16));
   }
   if (e == cudaSuccess) e = gemm_tma_prepare();
+  if (e == cudaSuccess) e = mlp_fused_prepare();
   if (e == cudaSuccess) e = cudaEventCreate(&m->ev0);
   if (e == cudaSuccess) e = cudaEventCreate(&m->ev1);
   if (e != cudaSuccess) return bad(FELIS_CUDA_ERROR, cudaGetErrorString(e));
@@ -371,7 +389,8 @@ felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y
     if (s != FELIS_OK) return s;
     launch_f32_to_bf16(m->xf, m->xb, (int64_t)M * m->in_p, m->st);
     MCK(cudaEventRecord(m->ev0, m->st));
-    forward(m, M, false);
+    if (m->fused) forward_fused(m, M);
+    else forward(m, M, false);
     MCK(cudaEventRecord(m->ev1, m->st));
     hy.resize((size_t)nr * m->out_p);
     MCK(cudaMemcpyAsync(hy.data(), m->z[kLayers - 1], hy.size() * sizeof(float), cudaMemcpyDeviceToHost, m->st));
@@ -385,6 +404,14 @@ felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y
     m->fwd_flops = fl;
   }
   return check_err(m);
+}
+
+felis_status felis_mlp_set_fused(felis_mlp* m, int32_t enable) {
+  if (!m) return FELIS_BAD_ARG;
+  if (enable && !mlp_fused_supported(m->width, m->in_p, m->out_p))
+    return mfail(m, FELIS_UNSUPPORTED, "the fused inference kernel needs width 256, n_in <= 64, n_out <= 256");
+  m->fused = enable != 0;
+  return FELIS_OK;
 }
 
 felis_status felis_mlp_gradients(felis_mlp* m, const float* x, const float* t, int64_t n, float* grads,

@@ -2,6 +2,7 @@
 // forward pass, backward pass and AdamW update.
 #pragma once
 
+#include <cuda.h>
 #include <cuda_bf16.h>
 #include <cuda_runtime.h>
 #include <stdint.h>
@@ -36,6 +37,30 @@ struct GemmArgs {
 // outside that.  gemm_tma_prepare() once per device before use.
 cudaError_t launch_gemm_tma(const GemmArgs& g, cudaStream_t st);
 cudaError_t gemm_tma_prepare();
+// 2-D tensor map of a row-major BF16 matrix [rows][ld] read in (64 x
+// box_rows) tiles of its first `cols` columns, 128-byte swizzle; elements
+// outside the matrix read as zero.  Valid after gemm_tma_prepare().
+bool tma_encode_bf16(CUtensorMap* map, const bf16* base, int rows, int cols, int ld, int box_rows);
+int gemm_sm_count();
+
+// The whole inference pass x -> W1 -> GELU -> W2 -> GELU -> W3 -> GELU -> W4
+// in one kernel (k_mlp_fused.cu): y[m][n] = (network)(x[m]) in FP32 for M rows
+// (a multiple of 128), hidden width 256; x [M][in_k] BF16; W_l row-major
+// [rows][cols] BF16 (W1 [256][in_k], W2 and W3 [256][256], W4 [out_n][256]);
+// bias_l FP32; in_k and out_n multiples of 16, in_k <= 64, out_n <= 256;
+// 16-byte aligned pointers.  Same rounding points as the layer-by-layer
+// chain (BF16 hidden activations, FP32 accumulation).
+struct MlpFusedArgs {
+  const bf16* x;
+  int M, width, in_k, out_n;
+  const bf16* w[4];
+  const float* bias[4];
+  float* y;
+  int* err;
+};
+bool mlp_fused_supported(int width, int in_k, int out_n);
+cudaError_t mlp_fused_prepare();
+cudaError_t launch_mlp_fused(const MlpFusedArgs& a, cudaStream_t st);
 
 // Elementwise and reduction helpers (row-major [rows][cols] unless stated).
 void launch_f32_to_bf16(const float* in, bf16* out, int64_t n, cudaStream_t st);

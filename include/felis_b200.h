@@ -416,10 +416,18 @@ felis_status felis_mlp_param_count(const felis_mlp* m, int64_t* count);
 felis_status felis_mlp_get_params(felis_mlp* m, float* out);
 /* Sets the parameters and resets the optimiser state. */
 felis_status felis_mlp_set_params(felis_mlp* m, const float* in);
+/* Inference: y [n][n_out] of x [n][n_in].  With hidden width 256, n_in <= 64
+ * and n_out <= 256 the four layers run as one fused tensor-core kernel
+ * (activations kept on chip); otherwise, or after felis_mlp_set_fused(m, 0),
+ * as the layer-by-layer GEMM chain.  Both round at the same places. */
 felis_status felis_mlp_forward(felis_mlp* m, const float* x, int64_t n, float* y);
+/* Chooses the fused inference kernel (enable != 0, the default where the
+ * shape allows it) or the layer-by-layer chain; FELIS_UNSUPPORTED when the
+ * fused kernel is asked for a shape it does not cover. */
+felis_status felis_mlp_set_fused(felis_mlp* m, int32_t enable);
 /* Device time (CUDA events on the network's stream) and floating-point
  * operations (2 M N K summed over the four layers, M the padded rows) of the
- * GEMM chain of the last chunk of the last felis_mlp_forward (chunks are up
+ * inference kernels of the last chunk of the last felis_mlp_forward (chunks are up
  * to 1,048,576 rows). */
 felis_status felis_mlp_last_forward(const felis_mlp* m, double* ms, double* flops);
 /* Gradient of the loss over n <= 65536 samples, in the parameter layout, and

@@ -9,7 +9,6 @@ gradients to a few BF16 ulps in norm.
 """
 import numpy as np
 import pytest
-from scipy.special import erf
 
 pytestmark = pytest.mark.gpu
 
@@ -25,12 +24,17 @@ def bf16(a):
     return u.astype(np.uint32).view(np.float32).astype(np.float64)
 
 
+GELU_C, GELU_A = np.sqrt(2.0 / np.pi), 0.044715
+
+
 def gelu(z):
-    return 0.5 * z * (1.0 + erf(z / np.sqrt(2.0)))
+    """The network's GELU, tanh form."""
+    return 0.5 * z * (1.0 + np.tanh(GELU_C * (z + GELU_A * z ** 3)))
 
 
 def gelu_grad(z):
-    return 0.5 * (1.0 + erf(z / np.sqrt(2.0))) + z * np.exp(-0.5 * z * z) / np.sqrt(2.0 * np.pi)
+    t = np.tanh(GELU_C * (z + GELU_A * z ** 3))
+    return 0.5 * (1.0 + t) + 0.5 * z * (1.0 - t * t) * GELU_C * (1.0 + 3.0 * GELU_A * z * z)
 
 
 def cpu_forward(layers, x):
@@ -144,14 +148,17 @@ def test_training_fits_a_smooth_map(fb):
     m.close()
 
 
-def test_large_batch_forward_and_timing(net):
-    """200,000 rows: 1,563 tiles of 128 rows over the persistent GEMM's CTAs,
-    so every CTA alternates its two tensor-memory accumulators and wraps its
-    shared-memory stage ring many times.  Rows spread over the batch match
-    the CPU product; the GEMM chain's device time is reported."""
+@pytest.mark.parametrize("fused", [True, False])
+def test_large_batch_forward_and_timing(net, fused):
+    """200,000 rows: 1,563 tiles of 128 rows over the persistent kernels'
+    CTAs, so every CTA alternates its two tensor-memory accumulators (tile
+    slots) and wraps its shared-memory stage ring many times.  Rows spread
+    over the batch match the CPU product; the device time of the fused kernel
+    and of the layer-by-layer GEMM chain is reported."""
     rng = np.random.default_rng(15)
     p = random_params(net, rng)
     net.set_params(p)
+    net.set_fused(fused)
     x = rng.normal(0, 1, (200_000, N_IN)).astype(np.float32)
     y = net.forward(x)
     ms, flops = net.last_forward()
@@ -160,4 +167,30 @@ def test_large_batch_forward_and_timing(net):
     zs, _ = cpu_forward(net.unflatten(p), x[pick])
     ref = zs[-1]
     np.testing.assert_allclose(y[pick], ref, rtol=0, atol=FWD_ATOL * np.abs(ref).max())
-    print(f"forward GEMM chain, 200,000 rows: {ms:.3f} ms, {flops / ms / 1e9:.1f} TFLOP/s")
+    what = "fused kernel" if fused else "GEMM chain"
+    print(f"forward {what}, 200,000 rows: {ms:.3f} ms, {flops / ms / 1e9:.1f} TFLOP/s")
+
+
+@pytest.mark.parametrize("rows", [1, 127, 129, 5000, 37_003])
+def test_fused_inference_equals_the_layer_chain(net, rows):
+    """The fused kernel rounds where the chain rounds (BF16 hidden
+    activations, FP32 accumulation over the same K order, the same GELU), so
+    both give the same bits, for ragged batches (the last tile padded) and
+    for batches where CTAs hold an odd number of tiles."""
+    rng = np.random.default_rng(rows)
+    net.set_params(random_params(net, rng))
+    x = rng.normal(0, 1, (rows, N_IN)).astype(np.float32)
+    net.set_fused(True)
+    a = net.forward(x)
+    net.set_fused(False)
+    b = net.forward(x)
+    net.set_fused(True)
+    assert np.array_equal(a, b)
+
+
+def test_fused_rejects_shapes_it_does_not_cover(fb):
+    m = fb.MLP(38, 128, 33, seed=1)
+    with pytest.raises(fb.FelisError):
+        m.set_fused(True)
+    m.set_fused(False)
+    m.close()
