@@ -372,6 +372,7 @@ felis_status check_err(felis_handle* h) {
   else if (e[ERR_NAN]) s = fail(h, FELIS_NAN, "non-finite particle state");
   else if (e[ERR_RADIAL]) s = fail(h, FELIS_UNSUPPORTED, "particle outside the radial Ez grid or the Bessel table");
   else if (e[ERR_DEPOSIT_CAPACITY]) s = fail(h, FELIS_UNSUPPORTED, "slice holds more particles than the deposit sort");
+  else if (e[ERR_TIMEOUT]) s = fail(h, FELIS_TIMEOUT, "a bounded device wait ran out");
   if (e[ERR_EDGE_DEPOSIT] || s != FELIS_OK) CK(cudaMemsetAsync(h->d_err, 0, ERR_SLOTS * sizeof(int), h->st));
   return s;
 }
@@ -490,6 +491,7 @@ felis_status run_adi(felis_handle* h, int use_source) {
   a.energy = h->d_planes;
   a.nxp = h->nxp;
   a.scratch = h->adi_scratch;
+  a.err = h->d_err;
   {
     KernelScope ks(h, FELIS_KERNEL_ADI);
     if (h->adi_scratch) launch_adi_big(a, h->adi_big_grid, h->st);

@@ -33,6 +33,7 @@ struct AdiLaunch {
   double* energy;      // [H][2][S] plane sums of |U|^2 after the solve (may be null)
   int nxp;             // padded row length of the shared-memory plane
   double2* scratch;    // k_adi_big: one plane per CTA
+  int* err;            // [ERR_SLOTS] (ERR_TIMEOUT: a bounded staging wait ran out)
 };
 
 struct DepositLaunch {

@@ -17,6 +17,7 @@
 //    column on that plane and writes U back to HBM coalesced.  The
 //    data-independent recurrence coefficients (CC) are host tables.
 #include "field.cuh"
+#include "bulk.cuh"
 
 namespace felis {
 
@@ -433,7 +434,7 @@ __global__ void __launch_bounds__(512) k_deposit(DepositLaunch a) {
 }
 
 // ---- ADI -------------------------------------------------------------------
-__global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
+__global__ void __launch_bounds__(256, 1) k_adi(AdiLaunch a) {
   extern __shared__ double2 Apl[];  // ny rows of nxp complex, then the recurrence tables
   __shared__ double red[8];
   const DevGeom& G = a.G;
@@ -465,8 +466,17 @@ __global__ void __launch_bounds__(256) k_adi(AdiLaunch a) {
   const int4 bx = a.box[s];
   const bool src = a.use_source != 0;
   const int tid = threadIdx.x;
-  // ---- stage the plane (coalesced) ----
-  for (int k = tid; k < N; k += blockDim.x) Apl[(k / nx) * nxp + (k % nx)] = U[k];
+  // ---- stage the plane: one bulk copy per row (rows of complex FP64 start on
+  // 16-byte boundaries in global and in shared memory) ----
+  __shared__ __align__(8) unsigned long long pbar;
+  if (tid == 0) bar_init_tx(smem_u32(&pbar), (unsigned)((size_t)N * sizeof(double2)));
+  __syncthreads();
+  for (int r = tid; r < ny; r += blockDim.x)
+    bulk_g2s(Apl + (size_t)r * nxp, U + (size_t)r * nx, (unsigned)(nx * sizeof(double2)), smem_u32(&pbar));
+  if (!bar_wait0(smem_u32(&pbar), kBulkWaitTries)) {
+    set_flag(a.err, ERR_TIMEOUT);
+    bar_wait0(smem_u32(&pbar), kBulkWaitTries);  // once more for the copies in flight
+  }
   __syncthreads();
   // ---- x sweep: thread per row j; one barrier per column so that every row
   // has read column i of U before any row overwrites it with DD ----
