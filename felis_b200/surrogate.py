@@ -228,21 +228,28 @@ def propose(model: Surrogate, beam: dict, n_candidates: int, top: int, seed: int
 
 
 def search(model: Surrogate, beam: dict, n_candidates: int = 1_000_000, top: int = 64, tol: float = 0.05,
-           fallback_runs: int = 64, seed: int = 7) -> dict:
-    """Surrogate-guided taper search for one beam.  The proposed winners are
-    re-run by the plain FP64 method; where the surrogate's error on the final
-    power exceeds `tol`, a plain random scan of `fallback_runs` tapers takes
-    over.  Returns the best verified taper and the bookkeeping."""
+           fallback_runs: int = 64, seed: int = 7, verify: int = 8, seeds: int = 8) -> dict:
+    """Surrogate-guided taper search for one beam.  The runs start from shot
+    noise, so one run of a taper is one draw of its final power; the network,
+    trained on single draws, predicts their mean.  The plain FP64 method
+    therefore verifies the `verify` best of the network's `top` proposals
+    with `seeds` noise realisations each (verify x seeds runs) and judges the
+    network by its error against the verified mean; where that error exceeds
+    `tol`, a plain random scan of `fallback_runs` tapers (one FP64 run each)
+    takes over.  Returns the best verified taper and the bookkeeping."""
     t0 = time.perf_counter()
     ks, pred = propose(model, beam, n_candidates, top, seed)
     t_rank = time.perf_counter() - t0
-    verified = np.stack([simulate_plain(beam, k) for k in ks])
+    ks, pred = ks[:verify], pred[:verify]
+    draws = np.array([[10.0 ** simulate_plain(beam, k, seed=1 + j)[SEGMENTS - 1] for j in range(seeds)] for k in ks])
+    p_true = draws.mean(axis=1)
     p_pred = 10.0 ** pred[:, SEGMENTS - 1]
-    p_true = 10.0 ** verified[:, SEGMENTS - 1]
     err = np.abs(p_pred - p_true) / p_true
     best = int(np.argmax(p_true))
-    res = {"best_power": float(p_true[best]), "best_taper": ks[best], "runs": top, "rank_seconds": t_rank,
-           "surrogate_error_max": float(err.max()), "surrogate_error_best": float(err[best]), "fallback": False}
+    spread = draws.std(axis=1, ddof=1) / p_true if seeds > 1 else np.zeros(len(ks))
+    res = {"best_power": float(p_true[best]), "best_taper": ks[best], "runs": verify * seeds, "rank_seconds": t_rank,
+           "surrogate_error_max": float(err.max()), "surrogate_error_best": float(err[best]),
+           "shot_noise_rel_std": float(spread[best]), "fallback": False}
     if err[best] > tol:
         rng = np.random.default_rng(seed + 1)
         scan = list(random_tapers(rng, fallback_runs))
@@ -256,12 +263,15 @@ def search(model: Surrogate, beam: dict, n_candidates: int = 1_000_000, top: int
 
 
 def compare_with_scan(model: Surrogate, beam: dict, n_candidates: int, top: int, scan_runs: int,
-                      seed: int = 7) -> dict:
+                      seed: int = 7, noise_runs: int = 0) -> dict:
     """What the network gains over the method without it, for one beam, in
     full simulations of one simulator (the batched engine): the best final
     power of the network's `top` proposals against the running best of a
     plain random scan of `scan_runs` tapers, and how many scan runs it takes
-    to reach the network's best (None: not within the scan)."""
+    to reach the network's best (None: not within the scan).  With
+    noise_runs > 1, the best taper of each side is re-run with that many
+    noise realisations: their mean final power (the quantity the network
+    predicts) and relative spread."""
     ks, pred = propose(model, beam, n_candidates, top, seed)
     rng = np.random.default_rng(seed + 2)
     scan = random_tapers(rng, scan_runs)
@@ -271,11 +281,24 @@ def compare_with_scan(model: Surrogate, beam: dict, n_candidates: int, top: int,
     running = np.maximum.accumulate(p_scan)
     best = float(p_sur.max())
     reach = np.flatnonzero(running >= best)
-    pred_best = 10.0 ** pred[int(np.argmax(p_sur)), SEGMENTS - 1]
-    return {"surrogate_best": best, "surrogate_runs": top, "scan_best": float(p_scan.max()),
-            "scan_best_at_equal_runs": float(running[min(top, scan_runs) - 1]),
-            "scan_runs_to_reach": int(reach[0]) + 1 if reach.size else None, "scan_runs": scan_runs,
-            "surrogate_error_at_best": float(abs(pred_best - best) / best)}
+    ib = int(np.argmax(p_sur))
+    pred_best = 10.0 ** pred[ib, SEGMENTS - 1]
+    out = {"surrogate_best": best, "surrogate_runs": top, "scan_best": float(p_scan.max()),
+           "scan_best_at_equal_runs": float(running[min(top, scan_runs) - 1]),
+           "scan_runs_to_reach": int(reach[0]) + 1 if reach.size else None, "scan_runs": scan_runs,
+           "surrogate_error_at_best": float(abs(pred_best - best) / best)}
+    if noise_runs > 1:
+        # the shot-noise spread of the network's best taper and of the scan's,
+        # and the network's error against the mean over noise realisations
+        for name, k in (("surrogate", ks[ib]), ("scan", scan[int(np.argmax(p_scan))])):
+            Yn = simulate([(beam, k)] * noise_runs, seed0=7_000_001)
+            pn = 10.0 ** Yn[:, SEGMENTS - 1]
+            out[f"{name}_best_mean_over_noise"] = float(pn.mean())
+            out[f"{name}_best_noise_rel_std"] = float(pn.std(ddof=1) / pn.mean())
+            out[f"{name}_best_bandwidth_mean"] = float(Yn[:, SEGMENTS].mean())
+        mean = out["surrogate_best_mean_over_noise"]
+        out["surrogate_error_vs_noise_mean"] = float(abs(pred_best - mean) / mean)
+    return out
 
 
 def main():
@@ -292,6 +315,7 @@ def main():
     ap.add_argument("--top", type=int, default=64)
     ap.add_argument("--scan", type=int, default=1280, help="random-scan runs per beam")
     ap.add_argument("--beams", type=int, default=4)
+    ap.add_argument("--noise-runs", type=int, default=32, help="noise realisations of each side's best taper")
     args = ap.parse_args()
     out = {}
     t0 = time.perf_counter()
@@ -317,11 +341,12 @@ def main():
     out["beams"] = []
     for _ in range(args.beams):
         beam = random_beam(rng)
-        r = compare_with_scan(model, beam, args.candidates, args.top, args.scan)
+        r = compare_with_scan(model, beam, args.candidates, args.top, args.scan, noise_runs=args.noise_runs)
         s = search(model, beam, args.candidates, args.top)
         r.update({"beam": beam, "plain_best_power": s["best_power"], "plain_runs": s["runs"],
                   "plain_fallback": s["fallback"], "plain_error_at_best": s["surrogate_error_best"],
-                  "plain_error_max": s["surrogate_error_max"], "rank_seconds": s["rank_seconds"]})
+                  "plain_error_max": s["surrogate_error_max"], "plain_shot_noise_rel_std": s["shot_noise_rel_std"],
+                  "rank_seconds": s["rank_seconds"]})
         out["beams"].append(r)
     model.close()
     print(json.dumps(out, indent=1), flush=True)

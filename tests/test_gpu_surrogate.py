@@ -4,7 +4,8 @@ The network is trained on runs of the batched engine, ranks candidate tapers
 for a beam it has not seen, and its proposals are compared, in full
 simulations, with a plain random scan of the same number of runs: the test
 shows what the trained network gains over the method without it.  The plain
-FP64 method re-runs the best proposals and judges the network's error.
+FP64 method re-runs the best proposals over several shot-noise realisations
+and judges the network's error against their mean.
 """
 import numpy as np
 import pytest
@@ -45,8 +46,8 @@ def test_network_beats_random_scan(trained):
 def test_plain_verification_and_fallback(trained):
     sg, model, _ = trained
     beam = sg.random_beam(np.random.default_rng(7))
-    r = sg.search(model, beam, n_candidates=20000, top=4, tol=0.05, fallback_runs=4)
-    assert r["best_power"] > 0
-    # the fallback scan runs exactly when the verified error exceeds 5 %
+    r = sg.search(model, beam, n_candidates=20000, top=4, tol=0.05, fallback_runs=4, verify=2, seeds=2)
+    assert r["best_power"] > 0 and r["shot_noise_rel_std"] >= 0
+    # the fallback scan runs exactly when the error against the verified mean exceeds 5 %
     assert r["fallback"] == (r["surrogate_error_best"] > 0.05)
-    assert r["runs"] == 4 + (4 if r["fallback"] else 0)
+    assert r["runs"] == 2 * 2 + (4 if r["fallback"] else 0)
