@@ -64,37 +64,51 @@ def tensor_peak() -> tuple[float, str]:
         return 1590.0, "fallback"
 
 
-def run_surrogate_gemm(rows: int) -> dict:
-    """The taper surrogate ranking `rows` candidate tapers: the forward GEMM
-    chain (38 -> 256 -> 256 -> 256 -> 33, BF16 operands, FP32 accumulation on
-    the tensor cores) timed with CUDA events on the network's stream, after
-    one untimed pass."""
+def run_surrogate_gemm(rows: int, chain_too: bool = True, fused: bool = True) -> dict:
+    """The taper surrogate ranking `rows` candidate tapers: the inference pass
+    38 -> 256 -> 256 -> 256 -> 33 (BF16 operands, FP32 accumulation on the
+    tensor cores) as one fused kernel (activations on chip) and, for
+    comparison, as the layer-by-layer GEMM chain; each timed with CUDA events
+    on the network's stream, best of three after one untimed pass."""
     import numpy as np
 
     import felis_b200 as fb
 
     m = fb.MLP(38, 256, 33, seed=3)
     x = np.random.default_rng(1).standard_normal((rows, 38)).astype(np.float32)
-    m.forward(x)
-    best = None
-    for _ in range(3):
+
+    def timed(use_fused):
+        m.set_fused(use_fused)
         m.forward(x)
-        ms, flops = m.last_forward()
-        best = ms if best is None else min(best, ms)
+        best = None
+        for _ in range(3):
+            m.forward(x)
+            ms, flops = m.last_forward()
+            best = ms if best is None else min(best, ms)
+        return best, flops
+
+    best, flops = timed(fused)
+    chain = timed(False)[0] if (chain_too and fused) else None
     m.close()
     peak, kind = tensor_peak()
     tf = flops / (best / 1e3) / 1e12
-    # HBM bytes of the chain: each layer reads its BF16 input and writes its
-    # output (BF16 for hidden layers, FP32 for the last); padded widths 48/256
     M = (rows + 127) // 128 * 128
-    hbm = M * (48 * 2 + 256 * 2) + 2 * M * (256 * 2 + 256 * 2) + M * (256 * 2 + 48 * 4)
+    # HBM bytes: the fused kernel reads the BF16 input and writes the FP32
+    # output; the chain also writes and re-reads every BF16 hidden activation
+    fused_bytes = M * (48 * 2 + 48 * 4)
+    chain_bytes = M * (48 * 2 + 256 * 2) + 2 * M * (256 * 2 + 256 * 2) + M * (256 * 2 + 48 * 4)
+    hbm = fused_bytes if fused else chain_bytes
     hpeak, hkind = peaks()
-    return {"workload": f"surrogate ranking: {rows} candidates through 38-256-256-256-33 (padded 48 / 48)",
-            "ms": best, "flops": flops, "tflops": tf,
-            "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
-                         "peak_source": kind},
-            "hbm": {"algorithmic_bytes": hbm, "achieved_gbs": hbm / (best / 1e3) / 1e9,
-                    "frac": hbm / (best / 1e3) / 1e9 / hpeak}}
+    out = {"workload": f"surrogate ranking: {rows} candidates through 38-256-256-256-33 (padded 48 / 48)",
+           "kernel": "fused four-layer kernel" if fused else "layer-by-layer GEMM chain",
+           "ms": best, "flops": flops, "tflops": tf,
+           "roofline": {"bound": "tensor", "achieved": tf, "peak": peak, "unit": "TFLOP/s", "frac": tf / peak,
+                        "peak_source": kind},
+           "hbm": {"algorithmic_bytes": hbm, "achieved_gbs": hbm / (best / 1e3) / 1e9,
+                   "frac": hbm / (best / 1e3) / 1e9 / hpeak}}
+    if chain is not None:
+        out["layer_chain"] = {"ms": chain, "tflops": flops / (chain / 1e3) / 1e12, "speedup_fused": chain / best}
+    return out
 
 
 class ClockSampler:
@@ -872,6 +886,8 @@ def main():
     ap.add_argument("--fp64-only", action="store_true", help="the FP64 plain path alone (profiling captures)")
     ap.add_argument("--sharded", action="store_true",
                     help="one FP64 run with its slices split over the ranks (strong scaling, device halo exchange)")
+    ap.add_argument("--surrogate-chain", action="store_true",
+                    help="with --surrogate-only: the layer-by-layer GEMM chain instead of the fused kernel")
     ap.add_argument("--surrogate-only", action="store_true",
                     help="the surrogate ranking GEMM chain alone (profiling captures)")
     args = ap.parse_args()
@@ -894,7 +910,8 @@ def main():
         return
 
     if args.surrogate_only:
-        print(json.dumps(run_surrogate_gemm(args.surrogate_rows)), flush=True)
+        print(json.dumps(run_surrogate_gemm(args.surrogate_rows, chain_too=False, fused=not args.surrogate_chain)),
+              flush=True)
         return
     dist, rank, world = dist_init()
     if args.sharded:
