@@ -2,10 +2,11 @@
 network.
 
 The GPU computes with BF16 weights and activations on the tensor cores and
-accumulates in FP32.  The CPU side (numpy, FP64) rounds to BF16 at the same
-places -- inputs, weights, hidden activations, and the backward operands dz
--- so the forward outputs agree to accumulation-order rounding and the
-gradients to a few BF16 ulps in norm.
+accumulates in FP32; its GELU (tanh form) uses the hardware tanh.  The CPU
+side (numpy, FP64, exact tanh) rounds to BF16 at the same places -- inputs,
+weights, hidden activations, and the backward operands dz -- so the forward
+outputs agree up to the BF16 roundings that accumulation order and the
+hardware tanh flip, and the gradients to a few BF16 ulps in norm.
 """
 import numpy as np
 import pytest
@@ -13,7 +14,8 @@ import pytest
 pytestmark = pytest.mark.gpu
 
 N_IN, WIDTH, N_OUT = 38, 256, 33
-FWD_ATOL = 2e-3      # forward, relative to the largest |output|
+FWD_ATOL = 3e-3      # forward, relative to the largest |output| (BF16 roundings flipped by
+                     # accumulation order and by the hardware tanh's ~2^-11 error)
 GRAD_RTOL = 1e-2     # gradient blocks, relative in norm
 
 
