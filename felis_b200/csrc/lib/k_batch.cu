@@ -21,6 +21,8 @@
 // atomics), so the sums do not depend on the order of the atomics: a run is
 // reproducible bit for bit and independent of the launch shape and of the
 // other instances.
+#include <type_traits>
+
 #include "batch.cuh"
 #include "bulk.cuh"
 
@@ -537,6 +539,29 @@ __device__ __forceinline__ void ffac_t(const BesselTab& B, int H, float xi, floa
   }
 }
 
+// The push's fx, fy of an odd harmonic H (real) at xi0 and their slopes
+// d/dxi, from the table cell that holds H xi0: the table interpolant is linear
+// in xi inside a cell, and a particle's xi = xi0 / (1 + d)^2 moves off xi0 by
+// about 2 |d| xi0 (|d| = |gamma / gamR - 1| <~ 1e-3), a small fraction of a
+// cell, so fx = fx0 + dfx (xi - xi0) is the interpolant itself up to the
+// cell edges.
+__device__ __forceinline__ void odd_factors(const BesselTab& B, int H, float xi0, float K0a, float* fx0, float* fy0,
+                                            float* dfx, float* dfy) {
+  const float x = (float)H * xi0 * B.idb;
+  const int idx = (int)x;
+  const float w1 = x - (float)idx, w0 = 1.f - w1;
+  const float sign = (((H - 1) / 2) % 2 == 0) ? 1.f : -1.f;
+  const float a1 = bjt(B, idx, (H - 1) / 2), b1 = bjt(B, idx + 1, (H - 1) / 2);
+  const float a2 = bjt(B, idx, (H + 1) / 2), b2 = bjt(B, idx + 1, (H + 1) / 2);
+  const float J1 = a1 * w0 + b1 * w1, J2 = a2 * w0 + b2 * w1;
+  const float sl = (float)H * B.idb;  // d(x) / d(xi)
+  const float dJ1 = (b1 - a1) * sl, dJ2 = (b2 - a2) * sl;
+  *fx0 = sign * (K0a * J1 - J2);
+  *fy0 = sign * (K0a * J1 + J2);
+  *dfx = sign * (K0a * dJ1 - dJ2);
+  *dfy = sign * (K0a * dJ1 + dJ2);
+}
+
 // Shrinks [i0, i1] x [j0, j1] to its central window of at most `cap` cells
 // (about the same aspect); empty (i1 < i0) when no 2 x 2 window fits.  The
 // same for every thread of a CTA.
@@ -559,7 +584,12 @@ __device__ __forceinline__ void shrink_window(int& i0, int& i1, int& j0, int& j1
 // Fixed-point adds without a return value: shared-memory accumulators by
 // their 32-bit shared address, global ones by pointer.
 __device__ __forceinline__ void red_s(unsigned saddr, acc_t v) {
-  if (v != 0) asm volatile("red.shared.add.s32 [%0], %1;\n" ::"r"(saddr), "r"(v) : "memory");
+  asm volatile(
+      "{\n\t.reg .pred p;\n\t"
+      "setp.ne.s32 p, %1, 0;\n\t"
+      "@p red.shared.add.s32 [%0], %1;\n\t}\n" ::"r"(saddr),
+      "r"(v)
+      : "memory");
 }
 // SH: every accumulator in shared memory, at idx.  Otherwise the box's
 // accumulators are in global memory (idx) and those of its central window in
@@ -581,7 +611,25 @@ struct DepConst {
 // particles into the fixed-point accumulators (2D: shared, or global with the
 // window [wi0, wi1] x [wj0, wj1] of wcells cells in shared memory; radial:
 // shared).
-template <int HM, bool SH>
+// With SUMS, the pass also accumulates the twiss and bunching partial sums of
+// the (pushed) particles (twiss.cpp, saveFile.cpp): acc7 = x^2, y^2, x'^2,
+// y'^2, x x', y y', count; bre / bim = sum of e^{i H theta} per harmonic.
+template <int HM>
+__device__ __forceinline__ void beam_sums(float (&acc7)[7], float (&bre)[HM], float (&bim)[HM], const int (&hh)[HM],
+                                          int H, float x, float y, float px, float py, float g, float thn) {
+  const float ig = 1.f / g, xp = px * ig, yp = py * ig;
+  acc7[0] += x * x; acc7[1] += y * y; acc7[2] += xp * xp;
+  acc7[3] += yp * yp; acc7[4] += x * xp; acc7[5] += y * yp; acc7[6] += 1.f;
+#pragma unroll
+  for (int h = 0; h < HM; ++h) {
+    if (h >= H) break;
+    const float2 e = expif((float)hh[h] * thn);
+    bre[h] += e.x;
+    bim[h] += e.y;
+  }
+}
+
+template <int HM, bool SH, bool SUMS>
 __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const float* __restrict__ ys,
                                              const float* __restrict__ pxs, const float* __restrict__ pys,
                                              const float* __restrict__ dgs, const double* __restrict__ ths,
@@ -591,7 +639,7 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
                                              int ny, int bi0, int bi1, int bj0, int bj1, int bw, int cells,
                                              int wi0, int wi1, int wj0, int wj1, int wcells, float iq2, float iqr,
                                              acc_t* gacc, unsigned sacc, unsigned sR, float dr, float idr2, int nr,
-                                             int L, int F) {
+                                             int L, int F, float (&acc7)[7], float (&bre)[HM], float (&bim)[HM]) {
   const int ww = wi1 - wi0 + 1;
   // the next particle's state is loaded one iteration ahead: the accumulator
   // adds below are compiler memory barriers, so no load moves above them
@@ -600,7 +648,7 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
   if ((int)threadIdx.x < P) {
     const int64_t n = p0 + threadIdx.x;
     nxv = xs[n]; nyv = ys[n]; ndg = dgs[n]; nth = ths[n];
-    if (has_even) { npx = pxs[n]; npy = pys[n]; }
+    if (SUMS || has_even) { npx = pxs[n]; npy = pys[n]; }
   }
   for (int q = threadIdx.x; q < P; q += blockDim.x) {
     const float x = nxv, y = nyv, g = gRf + ndg, px = npx, py = npy;
@@ -608,9 +656,10 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
     if (q + (int)blockDim.x < P) {
       const int64_t m = p0 + q + blockDim.x;
       nxv = xs[m]; nyv = ys[m]; ndg = dgs[m]; nth = ths[m];
-      if (has_even) { npx = pxs[m]; npy = pys[m]; }
+      if (SUMS || has_even) { npx = pxs[m]; npy = pys[m]; }
     }
     const float thr = theta_red(th);
+    if (SUMS) beam_sums<HM>(acc7, bre, bim, hh, H, x, y, px, py, g, thr);
     const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
     const int ii = (int)gx, jj = (int)gy;
     if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
@@ -620,14 +669,30 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
       if (has_even) pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
       int cidx[4], widx[4];
       float wv[4];
+      if constexpr (SH) {
+        // the whole box in shared memory: a corner outside it (an edge cell of
+        // the grid; the particle may sit in the last column or row, beyond
+        // bi1 / bj1) gets weight 0, and a zero term adds nothing
+        const int base = (jj - bj0) * bw + (ii - bi0);
+        const bool vx0 = ii >= bi0 && ii <= bi1, vx1 = ii + 1 >= bi0 && ii + 1 <= bi1;
+        const bool vy0 = jj >= bj0 && jj <= bj1, vy1 = jj + 1 >= bj0 && jj + 1 <= bj1;
 #pragma unroll
-      for (int cb = 0; cb < 4; ++cb) {
-        const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
-        const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
-        cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
-        const bool inw = !SH && ti >= wi0 && ti <= wi1 && tj >= wj0 && tj <= wj1;
-        widx[cb] = inw ? (tj - wj0) * ww + (ti - wi0) : -1;
-        wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
+        for (int cb = 0; cb < 4; ++cb) {
+          const bool in = ((cb & 1) ? vx1 : vx0) && ((cb >> 1) ? vy1 : vy0);
+          cidx[cb] = in ? base + (cb & 1) + (cb >> 1) * bw : 0;
+          widx[cb] = -1;
+          wv[cb] = in ? ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1) : 0.f;
+        }
+      } else {
+#pragma unroll
+        for (int cb = 0; cb < 4; ++cb) {
+          const int ti = ii + (cb & 1), tj = jj + (cb >> 1);
+          const bool in = ti >= bi0 && ti <= bi1 && tj >= bj0 && tj <= bj1;
+          cidx[cb] = in ? (tj - bj0) * bw + (ti - bi0) : -1;
+          const bool inw = ti >= wi0 && ti <= wi1 && tj >= wj0 && tj <= wj1;
+          widx[cb] = inw ? (tj - wj0) * ww + (ti - wi0) : -1;
+          wv[cb] = ((cb & 1) ? wx1 : 1.f - wx1) * ((cb >> 1) ? wy1 : 1.f - wy1);
+        }
       }
       const float ig = 1.f / g;
 #pragma unroll
@@ -640,7 +705,7 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
         if (Hh & 1) {
 #pragma unroll
           for (int cb = 0; cb < 4; ++cb) {
-            if (cidx[cb] < 0) continue;
+            if (!SH && cidx[cb] < 0) continue;
             const int wk = widx[cb] < 0 ? -1 : wbase + 2 * widx[cb];
             acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], wk, fix(mc.x * wv[cb], iq2));
             acc_to<SH>(gacc, sacc, base + 2 * cidx[cb] + 1, wk < 0 ? -1 : wk + 1, fix(mc.y * wv[cb], iq2));
@@ -651,7 +716,7 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
           const float2 ax = cm(cm(D.etaX, fx), mc), ay = cm(cm(D.etaY, fy), mc);
 #pragma unroll
           for (int cb = 0; cb < 4; ++cb) {
-            if (cidx[cb] < 0) continue;
+            if (!SH && cidx[cb] < 0) continue;
             const int wk = widx[cb] < 0 ? -1 : wbase + 2 * widx[cb];
             const int wky = widx[cb] < 0 ? -1 : wbase + 2 * (wcells + widx[cb]);
             acc_to<SH>(gacc, sacc, base + 2 * cidx[cb], wk, fix(-ax.x * wv[cb], iq2));
@@ -753,26 +818,24 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   const size_t area_bytes = (size_t)a.smem_bytes - o2;
   // deposit statistics of the (pushed) beam: cell box and fixed-point bounds.
   // The bounds are conservative and free of per-particle divisions: the 2-D
-  // term |w mc| / weight <= max(wm fb) / min|g| per thread; the radial term
+  // term |w mc| / weight <= max(fb) / min|g| per thread (w <= 1); the radial term
   // (1 + |wr1|) / max(ir, 1) <= 1.625 (|wr1| <= 5/8 for ir >= 1), counted when
   // a particle may lie inside the radial grid.
   int ci0 = 1 << 30, ci1 = -(1 << 30), cj0 = 1 << 30, cj1 = -(1 << 30);
   float wfmax = 0.f, gmin = 3.0e38f;
   int rin = 0;
   const float rlim2 = ((float)nr + 0.5f) * dr * ((float)nr + 0.5f) * dr;
-  auto stats = [&](float gx, float gy, int ii, int jj, float x, float y, float px, float py, float g) {
+  auto stats = [&](auto even_c, int ii, int jj, float x, float y, float px, float py, float g) {
     if (ii >= 0 && ii < nx && jj >= 0 && jj < ny) {
       ci0 = min(ci0, ii); ci1 = max(ci1, ii); cj0 = min(cj0, jj); cj1 = max(cj1, jj);
-      const float w1 = gx - ii, v1 = gy - jj;
-      const float wm = fmaxf(fabsf(w1), fabsf(1.f - w1)) * fmaxf(fabsf(v1), fabsf(1.f - v1));
-      float fb = 1.f;  // odd harmonics accumulate w mc (|f| applied later)
-      if (has_even) {
+      float fb = 1.f;  // odd harmonics accumulate w mc (|f| applied later); bilinear w <= 1
+      if constexpr (decltype(even_c)::value) {
         float xi2;
         float2 eP;
         pol_phase(D.K0, D.ue, D.K0a, D.Phi_half, px, py, &xi2, &eP);
         fb = fmaxf(fb, 2.f * xi2 * Hmax);
       }
-      wfmax = fmaxf(wfmax, wm * fb);
+      wfmax = fmaxf(wfmax, fb);
       gmin = fminf(gmin, fabsf(g));
     }
     rin |= (x * x + y * y < rlim2) ? 1 : 0;
@@ -784,13 +847,7 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
       const int l = k / (F * nr), rest = k % (F * nr);
       sEz[k] = I.Ez[((size_t)l * S + s) * F * nr + rest];
     }
-    const float R0 = T.R0, A0 = T.A0, AQ0 = T.AQ0, c12 = T.c1 * T.c2, K0 = T.K0, ue = T.ue, K0a = T.K0a;
-    const float Phi_half = T.Phi_half, cxi = T.cxi, K0sq = T.K0 * T.sq, ksK0sq = T.ksK0 * T.sq, e_mc2 = T.e_mc2;
-    const float dPhi = T.dPhi;
-    const float2 etaX = T.etaX, etaY = T.etaY;
-    const int drift = T.drift, shift = T.shift;
-    const double ku = T.ku, A0d = T.A0d;
-    const int stride = 7 + 2 * H + 1;
+    const int shift = T.shift;
     const double wakeE = I.wakeOn ? I.wakeE[s + I.minI] / (K_MC2 * 1.0e6) : 0.0;
     const double dz = I.dz;
     const float dwake = (float)(dz * wakeE);
@@ -856,187 +913,189 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
     }
     __syncthreads();
     const float4* m4 = reinterpret_cast<const float4*>(smap);
-    // twiss / bunching partial sums: FP32 over a thread's particles (64 per
-    // thread on the 8192-particle slices), FP64 across threads
-    float acc7[7] = {0, 0, 0, 0, 0, 0, 0};
-    float bre[HM], bim[HM];
-#pragma unroll
-    for (int h = 0; h < HM; ++h) { bre[h] = 0.f; bim[h] = 0.f; }
-    double wsum = 0.0;
-    int bad_over = 0, bad_range = 0, bad_nan = 0, bad_radial = 0;
-    // the next particle's state is loaded one iteration ahead
-    float nxv = 0.f, nyv = 0.f, npx = 0.f, npy = 0.f, ndg = 0.f;
-    double nth = 0.0;
-    if (tid < P) {
-      const int64_t n = p0 + tid;
-      nxv = xs[n]; nyv = ys[n]; npx = pxs[n]; npy = pys[n]; ndg = dgs[n]; nth = ths[n];
-    }
-    for (int q = tid; q < P; q += nt) {
-      const int64_t n = p0 + q;
-      float x = nxv, y = nyv, px = npx, py = npy, dg = ndg;
-      double th = nth;
-      if (q + nt < P) {
-        const int64_t m = n + nt;
-        nxv = xs[m]; nyv = ys[m]; npx = pxs[m]; npy = pys[m]; ndg = dgs[m]; nth = ths[m];
-      }
-      const float g = gRf + dg;
-      {  // both transverse half-pushes as one linear map (see BStep)
-        const float da = -dg * igR / g;
-        float o[4];
-#pragma unroll
-        for (int r = 0; r < 4; ++r) {
-          const float4 Dr = m4[r], Ar = m4[4 + r], Br = m4[8 + r];
-          const float m2 = Br.x * x + Br.y * y + Br.z * px + Br.w * py;
-          const float m1 = Ar.x * x + Ar.y * y + Ar.z * px + Ar.w * py + da * m2;
-          o[r] = Dr.x * x + Dr.y * y + Dr.z * px + Dr.w * py + da * m1;
-        }
-        x += o[0]; y += o[1]; px += o[2]; py += o[3];
-      }
-      const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
-      const int ii = (int)gx, jj = (int)gy;
-      if (ii >= 0 && ii < nx - 1 && jj >= 0 && jj < ny - 1) {
-        const float wx1 = gx - ii, wy1 = gy - jj, wx0 = 1.f - wx1, wy0 = 1.f - wy1;
-        float2 Ux[HM], Uy[HM];
-        float sumU2 = 0.f;
-        const bool staged = ii >= fi0 && ii < fi1 && jj >= fj0 && jj < fj1;
-        const float2* fb = staged ? sF + (jj - fj0) * fbw + (ii - fi0) : Ubase + jj * nx + ii;
-        const size_t fps = staged ? (size_t)fcells : hpstride;
-        const int frs = staged ? fbw : nx;
+    // error flags of this thread's particles, one bit each
+    constexpr int kBadOver = 1, kBadRange = 2, kBadNan = 4, kBadRadial = 8;
+    int bad = 0;
+    // The push loop, specialised on the drift / undulator mode and on even
+    // harmonics (uniform per CTA), so that each copy holds only the constants
+    // its mode reads.
+    auto push_loop = [&](auto drift_c, auto even_c) {
+      constexpr bool DRIFT = decltype(drift_c)::value, EVEN = decltype(even_c)::value;
+      // odd harmonics: the Bessel factors as a linear function of xi (odd_factors)
+      float fx0[HM], fy0[HM], dfx[HM], dfy[HM];
+      float xi0 = 0.f;
+      if constexpr (!DRIFT) {
+        xi0 = T.cxi * igR * igR;
 #pragma unroll
         for (int h = 0; h < HM; ++h) {
-          if (h >= H) break;
-          const float2* Px = fb + (2 * h) * fps;
-          const float2* Py = Px + fps;
-          Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[frs], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[frs + 1], wx1 * wy1)));
-          Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[frs], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[frs + 1], wx1 * wy1)));
-          const float Hh = (float)hh[h];
-          sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
+          fx0[h] = fy0[h] = dfx[h] = dfy[h] = 0.f;
+          if (h < H && (hh[h] & 1)) odd_factors(B, hh[h], xi0, T.K0a, &fx0[h], &fy0[h], &dfx[h], &dfy[h]);
         }
-        if (!drift) {
-          const float r2 = x * x + y * y;
-          const float k2 = px * px + py * py + c12 * r2;  // K2 - Q0
-          const float xi = cxi * igR * igR / ((1.f + dg * igR) * (1.f + dg * igR));
-          float xi2 = 0.f;
-          float2 eP = make_float2(1.f, 0.f);
-          if (has_even) pol_phase(K0, ue, K0a, Phi_half, px, py, &xi2, &eP);
+      }
+      // the next particle's state is loaded one iteration ahead
+      float nxv = 0.f, nyv = 0.f, npx = 0.f, npy = 0.f, ndg = 0.f;
+      double nth = 0.0;
+      if (tid < P) {
+        const int64_t n = p0 + tid;
+        nxv = xs[n]; nyv = ys[n]; npx = pxs[n]; npy = pys[n]; ndg = dgs[n]; nth = ths[n];
+      }
+      for (int q = tid; q < P; q += nt) {
+        const int64_t n = p0 + q;
+        float x = nxv, y = nyv, px = npx, py = npy, dg = ndg;
+        double th = nth;
+        if (q + nt < P) {
+          const int64_t m = n + nt;
+          nxv = xs[m]; nyv = ys[m]; npx = pxs[m]; npy = pys[m]; ndg = dgs[m]; nth = ths[m];
+        }
+        const float g = gRf + dg;
+        {  // both transverse half-pushes as one linear map (see BStep)
+          const float da = -dg * igR / g;
+          float o[4];
 #pragma unroll
-          for (int h = 0; h < HM; ++h) {  // fold the polarisation factors into the field
+          for (int r = 0; r < 4; ++r) {
+            const float4 Dr = m4[r], Ar = m4[4 + r], Br = m4[8 + r];
+            const float m2 = Br.x * x + Br.y * y + Br.z * px + Br.w * py;
+            const float m1 = Ar.x * x + Ar.y * y + Ar.z * px + Ar.w * py + da * m2;
+            o[r] = Dr.x * x + Dr.y * y + Dr.z * px + Dr.w * py + da * m1;
+          }
+          x += o[0]; y += o[1]; px += o[2]; py += o[3];
+        }
+        const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
+        const int ii = (int)gx, jj = (int)gy;
+        if (ii >= 0 && ii < nx - 1 && jj >= 0 && jj < ny - 1) {
+          const float wx1 = gx - ii, wy1 = gy - jj, wx0 = 1.f - wx1, wy0 = 1.f - wy1;
+          float2 Ux[HM], Uy[HM];
+          float sumU2 = 0.f;
+          const bool staged = ii >= fi0 && ii < fi1 && jj >= fj0 && jj < fj1;
+          const float2* fb = staged ? sF + (jj - fj0) * fbw + (ii - fi0) : Ubase + jj * nx + ii;
+          const size_t fps = staged ? (size_t)fcells : hpstride;
+          const int frs = staged ? fbw : nx;
+#pragma unroll
+          for (int h = 0; h < HM; ++h) {
             if (h >= H) break;
-            float2 fx, fy;
-            ffac_t(B, hh[h], xi, xi2, K0a, eP, false, &fx, &fy);
-            Ux[h] = cm(cm(etaX, fx), Ux[h]);
-            Uy[h] = cm(cm(etaY, fy), Uy[h]);
+            const float2* Px = fb + (2 * h) * fps;
+            const float2* Py = Px + fps;
+            Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[frs], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[frs + 1], wx1 * wy1)));
+            Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[frs], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[frs + 1], wx1 * wy1)));
+            const float Hh = (float)hh[h];
+            sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
           }
-          const float r = sqrtf(r2);
-          const int ir = (int)(r / dr + 0.5f);
-          float2 Em[LM];
+          if constexpr (!DRIFT) {
+            const float R0 = T.R0, A0 = T.A0, AQ0 = T.AQ0, c12 = T.c1 * T.c2, K0 = T.K0, ue = T.ue, K0a = T.K0a;
+            const float Phi_half = T.Phi_half, K0sq = T.K0 * T.sq, ksK0sq = T.ksK0 * T.sq;
+            const float e_mc2 = T.e_mc2, dPhi = T.dPhi;
+            const float2 etaX = T.etaX, etaY = T.etaY;
+            const float r2 = x * x + y * y;
+            const float k2 = px * px + py * py + c12 * r2;  // K2 - Q0
+            const float i10 = 1.f / (1.f + dg * igR), i20 = i10 * i10;
+            const float dxi = xi0 * (i20 - 1.f);  // xi - xi0, xi = cxi / gamma^2
+            float xi2 = 0.f;
+            float2 eP = make_float2(1.f, 0.f);
+            if constexpr (EVEN) pol_phase(K0, ue, K0a, Phi_half, px, py, &xi2, &eP);
 #pragma unroll
-          for (int l = 0; l < LM; ++l) Em[l] = make_float2(0.f, 0.f);
-          if (ir >= 0 && ir < nr) {
-            const float wr1 = ir > 0 ? (r2 * idr2 - (float)(ir * ir)) / (2.f * ir) : 1.f;
-            const float wr0 = ir > 0 ? 1.f - wr1 : 1.f;
-#pragma unroll
-            for (int l = 0; l < LM; ++l) {
-              if (l >= L) break;
-              for (int f = 0; f < F; ++f) {
-                const float2 a0 = sEz[(l * F + f) * nr + ir];
-                const float2 a1 = (ir + 1 < nr) ? sEz[(l * F + f) * nr + ir + 1] : make_float2(0.f, 0.f);
-                Em[l] = cad(Em[l], cad(cs(a0, wr0), cs(a1, wr1)));
-              }
-            }
-          } else {
-            // beyond the radial Ez grid: the reference reuses the previous
-            // particle's Em there (particlePush.cpp:286-304); flagged
-            bad_radial = 1;
-          }
-          // RK4 in z of (theta, gamma); the theta slope in FP32 relative to
-          // the resonance (BStep), theta itself accumulated in FP64
-          const float thr = theta_red(th);
-          float kth_prev = 0.f, kth_sum = 0.f, kg_prev = 0.f, kg_sum = 0.f;
-#pragma unroll
-          for (int m = 1; m < 5; ++m) {
-            const float clm = (m == 1) ? 0.f : (m == 4 ? 1.f : 0.5f);
-            const float tm = thr + dzf * kth_prev * clm;
-            const float dgm = dg + dzf * kg_prev * clm;
-            const float d = dgm * igR;
-            const float inv2 = 1.f / ((1.f + d) * (1.f + d));
-            float sumEz = 0.f, sumTh = 0.f, sumG = 0.f;
-#pragma unroll
-            for (int l = 0; l < LM; ++l) {
-              if (l >= L) break;
-              const float2 e = expif((l + 1.f) * tm);
-              sumEz += 2.f * (Em[l].x * e.x - Em[l].y * e.y);
-            }
-#pragma unroll
-            for (int h = 0; h < HM; ++h) {
+            for (int h = 0; h < HM; ++h) {  // fold the polarisation factors into the field
               if (h >= H) break;
-              const float Hh = (float)hh[h];
-              const float2 e = expif(Hh * (tm + Phi_half));
-              const float2 tc = cm(e, csb(Ux[h], Uy[h]));
-              sumTh += -tc.y / Hh;
-              sumG += tc.x;
+              float2 fx, fy;
+              if (hh[h] & 1) {
+                fx = make_float2(fx0[h] + dfx[h] * dxi, 0.f);
+                fy = make_float2(fy0[h] + dfy[h] * dxi, 0.f);
+              } else {
+                ffac_t(B, hh[h], xi0 * i20, xi2, K0a, eP, false, &fx, &fy);
+              }
+              Ux[h] = cm(cm(etaX, fx), Ux[h]);
+              Uy[h] = cm(cm(etaY, fy), Uy[h]);
             }
-            sumG *= 0.5f / (gRf + dgm);
-            kth_prev = R0 + AQ0 * (d * (2.f + d) * inv2) - A0 * inv2 * (k2 + sumU2 + K0sq * sumTh);
-            kg_prev = ksK0sq * sumG + e_mc2 * sumEz;
-            const float wgt = (m == 1 || m == 4) ? 1.f : 2.f;
-            kth_sum += wgt * kth_prev;
-            kg_sum += wgt * kg_prev;
+            const float r = sqrtf(r2);
+            const int ir = (int)(r / dr + 0.5f);
+            float2 Em[LM];
+#pragma unroll
+            for (int l = 0; l < LM; ++l) Em[l] = make_float2(0.f, 0.f);
+            if (ir >= 0 && ir < nr) {
+              const float wr1 = ir > 0 ? (r2 * idr2 - (float)(ir * ir)) / (2.f * ir) : 1.f;
+              const float wr0 = ir > 0 ? 1.f - wr1 : 1.f;
+#pragma unroll
+              for (int l = 0; l < LM; ++l) {
+                if (l >= L) break;
+                for (int f = 0; f < F; ++f) {
+                  const float2 a0 = sEz[(l * F + f) * nr + ir];
+                  const float2 a1 = (ir + 1 < nr) ? sEz[(l * F + f) * nr + ir + 1] : make_float2(0.f, 0.f);
+                  Em[l] = cad(Em[l], cad(cs(a0, wr0), cs(a1, wr1)));
+                }
+              }
+            } else {
+              // beyond the radial Ez grid: the reference reuses the previous
+              // particle's Em there (particlePush.cpp:286-304); flagged
+              bad |= kBadRadial;
+            }
+            // RK4 in z of (theta, gamma); the theta slope in FP32 relative to
+            // the resonance (BStep), theta itself accumulated in FP64
+            const float thr = theta_red(th);
+            float kth_prev = 0.f, kth_sum = 0.f, kg_prev = 0.f, kg_sum = 0.f;
+#pragma unroll
+            for (int m = 1; m < 5; ++m) {
+              const float clm = (m == 1) ? 0.f : (m == 4 ? 1.f : 0.5f);
+              const float tm = thr + dzf * kth_prev * clm;
+              const float dgm = dg + dzf * kg_prev * clm;
+              const float d = dgm * igR;
+              const float inv1 = 1.f / (1.f + d), inv2 = inv1 * inv1;
+              float sumEz = 0.f, sumTh = 0.f, sumG = 0.f;
+#pragma unroll
+              for (int l = 0; l < LM; ++l) {
+                if (l >= L) break;
+                const float2 e = expif((l + 1.f) * tm);
+                sumEz += 2.f * (Em[l].x * e.x - Em[l].y * e.y);
+              }
+#pragma unroll
+              for (int h = 0; h < HM; ++h) {
+                if (h >= H) break;
+                const float Hh = (float)hh[h];
+                const float2 e = expif(Hh * (tm + Phi_half));
+                const float2 tc = cm(e, csb(Ux[h], Uy[h]));
+                sumTh += -tc.y / Hh;
+                sumG += tc.x;
+              }
+              sumG *= 0.5f * igR * inv1;  // 1 / (gR + dg) = (1 / gR) / (1 + d)
+              kth_prev = R0 + AQ0 * (d * (2.f + d) * inv2) - A0 * inv2 * (k2 + sumU2 + K0sq * sumTh);
+              kg_prev = ksK0sq * sumG + e_mc2 * sumEz;
+              const float wgt = (m == 1 || m == 4) ? 1.f : 2.f;
+              kth_sum += wgt * kth_prev;
+              kg_sum += wgt * kg_prev;
+            }
+            const float dth = dzf / 6.f * kth_sum;
+            if (dth > dPhi || dth < -dPhi) bad |= kBadOver;
+            th += (double)dth;
+            dg += dzf / 6.f * kg_sum - dwake;
+          } else {
+            const double K2 = 1.0 + (double)px * px + (double)py * py;
+            const double tmp = T.ku - T.A0d * (K2 + sumU2);
+            th += tmp * dz;
+            th -= dz * wakeE;
           }
-          const float dth = dzf / 6.f * kth_sum;
-          if (dth > dPhi || dth < -dPhi) bad_over = 1;
-          th += (double)dth;
-          dg += dzf / 6.f * kg_sum - dwake;
-        } else {
-          const double K2 = 1.0 + (double)px * px + (double)py * py;
-          const double tmp = ku - A0d * (K2 + sumU2);
-          th += tmp * dz;
-          th -= dz * wakeE;
         }
+        th += thshift;  // [Phase_shifter] (0 when no shifter sits in this step)
+        // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
+        if (th >= dTh || th < 0) {
+          th -= dTh * floor(th * idTh);
+          if (th >= dTh) th -= dTh;
+          else if (th < 0) th += dTh;
+        }
+        if (th > dTh || th < 0) bad |= kBadRange;
+        if (!(dg - dg == 0.f) || !(th - th == 0.0) || !(x - x == 0.f)) bad |= kBadNan;
+        xs[n] = x; ys[n] = y; pxs[n] = px; pys[n] = py; dgs[n] = dg; ths[n] = th;
+        if (dep) stats(even_c, ii, jj, x, y, px, py, gRf + dg);
       }
-      th += thshift;  // [Phase_shifter] (0 when no shifter sits in this step)
-      // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
-      if (th >= dTh || th < 0) {
-        th -= dTh * floor(th * idTh);
-        if (th >= dTh) th -= dTh;
-        else if (th < 0) th += dTh;
-      }
-      if (th > dTh || th < 0) bad_range = 1;
-      if (!(dg - dg == 0.f) || !(th - th == 0.0) || !(x - x == 0.f)) bad_nan = 1;
-      xs[n] = x; ys[n] = y; pxs[n] = px; pys[n] = py; dgs[n] = dg; ths[n] = th;
-      // twiss / bFactor partial sums of the new state (twiss.cpp, saveFile.cpp)
-      const float ig = 1.f / (gRf + dg), xp = px * ig, yp = py * ig;
-      acc7[0] += x * x; acc7[1] += y * y; acc7[2] += xp * xp;
-      acc7[3] += yp * yp; acc7[4] += x * xp; acc7[5] += y * yp; acc7[6] += 1.f;
-      const float thn = theta_red(th);
-#pragma unroll
-      for (int h = 0; h < HM; ++h) {
-        if (h >= H) break;
-        const float2 e = expif((float)hh[h] * thn);
-        bre[h] += e.x;
-        bim[h] += e.y;
-      }
-      if (dep) stats(gx, gy, ii, jj, x, y, px, py, gRf + dg);
+    };
+    if (T.drift) {
+      if (has_even) push_loop(std::true_type{}, std::true_type{});
+      else push_loop(std::true_type{}, std::false_type{});
+    } else {
+      if (has_even) push_loop(std::false_type{}, std::true_type{});
+      else push_loop(std::false_type{}, std::false_type{});
     }
-    wsum = (double)weight * (double)max(0, (P - tid + nt - 1) / nt);
-    if (bad_over) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
-    if (bad_range) atomicOr(I.err + ERR_OUT_OF_RANGE, 1);
-    if (bad_nan) atomicOr(I.err + ERR_NAN, 1);
-    if (bad_radial) atomicOr(I.err + ERR_RADIAL, 1);
-    double* out = I.part_b + (size_t)s * stride;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const double t = block_sum_d((double)acc7[k], redd);
-      if (tid == 0) out[k] = t;
-    }
-#pragma unroll
-    for (int h = 0; h < HM; ++h) {
-      if (h >= H) break;
-      const double tr = block_sum_d((double)bre[h], redd), ti = block_sum_d((double)bim[h], redd);
-      if (tid == 0) { out[7 + 2 * h] = tr * weight; out[8 + 2 * h] = ti * weight; }
-    }
-    const double tw = block_sum_d(wsum, redd);
-    if (tid == 0) out[7 + 2 * H] = tw;
+    if (bad & kBadOver) atomicOr(I.err + ERR_THETA_OVERFLOW, 1);
+    if (bad & kBadRange) atomicOr(I.err + ERR_OUT_OF_RANGE, 1);
+    if (bad & kBadNan) atomicOr(I.err + ERR_NAN, 1);
+    if (bad & kBadRadial) atomicOr(I.err + ERR_RADIAL, 1);
     // slippage shift: the plane of the last slice becomes the new first slice
     if (shift && s == S - 1) {
       __syncthreads();
@@ -1049,8 +1108,42 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
     for (int q = tid; q < P; q += nt) {
       const int64_t n = p0 + q;
       const float x = xs[n], y = ys[n], gx = (x - minX) * idx_, gy = (y - minY) * idy_;
-      stats(gx, gy, (int)gx, (int)gy, x, y, has_even ? pxs[n] : 0.f, has_even ? pys[n] : 0.f, gRf + dgs[n]);
+      const float px = has_even ? pxs[n] : 0.f, py = has_even ? pys[n] : 0.f;
+      if (has_even) stats(std::true_type{}, (int)gx, (int)gy, x, y, px, py, gRf + dgs[n]);
+      else stats(std::false_type{}, (int)gx, (int)gy, x, y, px, py, gRf + dgs[n]);
     }
+  }
+  // twiss / bunching partial sums of the pushed beam: FP32 over a thread's
+  // particles (64 per thread on the 8192-particle slices), FP64 across
+  // threads; taken in the deposit pass below when there is one, else here
+  float acc7[7] = {0, 0, 0, 0, 0, 0, 0};
+  float bre[HM], bim[HM];
+#pragma unroll
+  for (int h = 0; h < HM; ++h) { bre[h] = 0.f; bim[h] = 0.f; }
+  auto write_sums = [&]() {
+    const int stride = 7 + 2 * H + 1;
+    double* out = I.part_b + (size_t)s * stride;
+#pragma unroll
+    for (int k = 0; k < 7; ++k) {
+      const double t = block_sum_d((double)acc7[k], redd);
+      if (tid == 0) out[k] = t;
+    }
+#pragma unroll
+    for (int h = 0; h < HM; ++h) {
+      if (h >= H) break;
+      const double tr = block_sum_d((double)bre[h], redd), ti = block_sum_d((double)bim[h], redd);
+      if (tid == 0) { out[7 + 2 * h] = tr * weight; out[8 + 2 * h] = ti * weight; }
+    }
+    const double wsum = (double)weight * (double)max(0, (P - tid + nt - 1) / nt);
+    const double tw = block_sum_d(wsum, redd);
+    if (tid == 0) out[7 + 2 * H] = tw;
+  };
+  if (push && !dep) {
+    for (int q = tid; q < P; q += nt) {
+      const int64_t n = p0 + q;
+      beam_sums<HM>(acc7, bre, bim, hh, H, xs[n], ys[n], pxs[n], pys[n], gRf + dgs[n], theta_red(ths[n]));
+    }
+    write_sums();
   }
   if (!dep) return;
   // ================= pass 2: deposit of the next solveField =================
@@ -1087,14 +1180,25 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   __syncthreads();
   const unsigned sacc = (unsigned)__cvta_generic_to_shared(area);
   const unsigned sRa = (unsigned)__cvta_generic_to_shared(sR);
-  if (in_smem)
-    deposit_pass<HM, true>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
-                           idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, 1, 0, 1, 0, 0, iq2, iqr, nullptr, sacc,
-                           sRa, dr, idr2, nr, L, F);
-  else
-    deposit_pass<HM, false>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX, minY,
-                            idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, wi0, wi1, wj0, wj1, wcells, iq2, iqr,
-                            acc, sacc, sRa, dr, idr2, nr, L, F);
+  auto dep_pass = [&](auto sh_c, auto sums_c) {
+    constexpr bool SHc = decltype(sh_c)::value, SUMSc = decltype(sums_c)::value;
+    if constexpr (SHc)
+      deposit_pass<HM, SHc, SUMSc>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX,
+                                   minY, idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, 1, 0, 1, 0, 0, iq2, iqr,
+                                   nullptr, sacc, sRa, dr, idr2, nr, L, F, acc7, bre, bim);
+    else
+      deposit_pass<HM, SHc, SUMSc>(xs, ys, pxs, pys, dgs, ths, p0, P, hh, sp, H, has_even, D, B, weight, gRf, minX,
+                                   minY, idx_, idy_, nx, ny, bi0, bi1, bj0, bj1, bw, cells, wi0, wi1, wj0, wj1, wcells,
+                                   iq2, iqr, acc, sacc, sRa, dr, idr2, nr, L, F, acc7, bre, bim);
+  };
+  if (in_smem) {
+    if (push) dep_pass(std::true_type{}, std::true_type{});
+    else dep_pass(std::true_type{}, std::false_type{});
+  } else {
+    if (push) dep_pass(std::false_type{}, std::true_type{});
+    else dep_pass(std::false_type{}, std::false_type{});
+  }
+  if (push) write_sums();
   __syncthreads();
   if (wcells > 0) {
     // the window's sums into the box's

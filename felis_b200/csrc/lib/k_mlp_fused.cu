@@ -19,8 +19,8 @@
 //              the slot's accumulator has been read, commits each weight
 //              stage back to the producer and each finished accumulator to
 //              the epilogue
-//   warps 2-17 the epilogue: warp w reads lanes 32 (w % 4) .. + 31 of the
-//              accumulator (one row per thread), four warps per lane quarter
+//   warps 2-9  the epilogue: warp w reads lanes 32 (w % 4) .. + 31 of the
+//              accumulator (one row per thread), two warps per lane quarter
 //              splitting the columns; bias and GELU, BF16 into the slot's
 //              activation buffer in the swizzled layout (hidden layers), or
 //              bias and FP32 rows to global memory (last layer)
@@ -47,7 +47,7 @@ constexpr uint32_t kActChunk = kBM * 128;         // one 64-column K chunk of a 
 constexpr uint32_t kAct = 4 * kActChunk;          // a slot's activation buffer: 64 KB
 constexpr uint32_t kWStage = kWidth * 128;        // one K chunk of a 256-row weight: 32 KB
 constexpr int kWStages = 3;
-constexpr int kEpiWarps = 16;
+constexpr int kEpiWarps = 8;
 constexpr int kThreads = 32 * (2 + kEpiWarps);
 constexpr int kTmemCols = 2 * kWidth;
 constexpr size_t kSmem = 1024 + 2 * (size_t)kAct + (size_t)kWStages * kWStage;
@@ -193,9 +193,9 @@ __global__ void __launch_bounds__(kThreads, 1)
     }
     __syncwarp();
   } else {
-    const int q = warp & 3;             // tensor-memory lane quarter this warp may read
-    const int part = (warp - 2) >> 2;   // which of the four warps of that quarter
-    const int r = q * 32 + lane;        // this thread's row of the tile
+    const int q = warp & 3;            // tensor-memory lane quarter this warp may read
+    const int half = (warp - 2) >> 2;  // which of the two warps of that quarter
+    const int r = q * 32 + lane;       // this thread's row of the tile
     bool ok = true;
     for (int p = 0; 2 * p < nt && ok; ++p)
       for (int l = 0; l < 4 && ok; ++l)
@@ -210,21 +210,17 @@ __global__ void __launch_bounds__(kThreads, 1)
           if (l < 3) {
             unsigned char* a_s = act + (size_t)s * kAct;
 #pragma unroll 1
-            for (int i = 0; i < 2; ++i) {
-              const int c0 = part * 64 + i * 32;
-              // the chunk's biases are loaded while the tensor-memory load is in flight
-              float4 b4[8];
-#pragma unroll
-              for (int j = 0; j < 8; ++j) b4[j] = __ldg(reinterpret_cast<const float4*>(bias + c0) + j);
+            for (int i = 0; i < 4; ++i) {
+              const int c0 = half * 128 + i * 32;
               uint32_t v[32];
               TMEM_LD32X32(tbase + (uint32_t)c0, v);
               asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");
-              const float* bv = reinterpret_cast<const float*>(b4);
               uint32_t w[16];
 #pragma unroll
               for (int j = 0; j < 16; ++j) {
-                const float x0 = gelu_f(__uint_as_float(v[2 * j]) + bv[2 * j]);
-                const float x1 = gelu_f(__uint_as_float(v[2 * j + 1]) + bv[2 * j + 1]);
+                const float2 b2 = __ldg(reinterpret_cast<const float2*>(bias + c0) + j);
+                const float x0 = gelu_f(__uint_as_float(v[2 * j]) + b2.x);
+                const float x1 = gelu_f(__uint_as_float(v[2 * j + 1]) + b2.y);
                 const __nv_bfloat162 h2 = __floats2bfloat162_rn(x0, x1);
                 w[j] = *reinterpret_cast<const uint32_t*>(&h2);
               }
@@ -241,7 +237,7 @@ __global__ void __launch_bounds__(kThreads, 1)
           } else {
             const int tile = blockIdx.x + k * gridDim.x;
             float* yrow = f.y + ((size_t)tile * kBM + r) * (size_t)f.out_n;
-            for (int c0 = part * 32; c0 < f.out_n; c0 += 128) {
+            for (int c0 = half * 32; c0 < f.out_n; c0 += 64) {
               uint32_t v[32];
               TMEM_LD32X32(tbase + (uint32_t)c0, v);
               asm volatile("tcgen05.wait::ld.sync.aligned;\n" ::: "memory");

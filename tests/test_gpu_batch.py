@@ -251,6 +251,33 @@ def test_download_into_caller_buffers(fb, seeded):
     b.close()
 
 
+@pytest.mark.parametrize("nx", [41, 42])
+def test_particles_in_the_edge_cells(fb, tmp_path, nx):
+    """Particles in the last grid column and row (cell index nx - 1, outside
+    the interior box the deposit accumulates) on odd and even grids: the run
+    completes, and its power follows the FP64 path's, which leaves those
+    cells' sources out too (the ADI solves interior cells only)."""
+    cfg, beam, fields = make_case(fb, tmp_path, kind="sase", slices=6, beamlets=64, nx=nx, total_length=0.5,
+                                  seed_power=1e5, energy_mev=1000.0)
+    p = cfg.params
+    beam = {k: np.array(v) for k, v in beam.items()}
+    last_x = p.min_x + (p.nx - 0.5) * p.dx
+    last_y = p.min_y + (p.ny - 0.5) * p.dy
+    for k in range(0, len(beam["x"]), 7):  # one particle in seven on the edge
+        if k % 2:
+            beam["x"][k] = last_x
+        beam["y"][k] = last_y
+    steps = 6
+    g = _fp64(fb, cfg, beam, fields, steps)
+    b = fb.Batch([p])
+    _upload(fb, b, 0, cfg, beam, fields)
+    b.run(0, steps)
+    P32 = b.diagnostics(0, 0, steps + 1)[0].sum(axis=1)
+    P64 = g.diagnostics(0, steps + 1)[0].sum(axis=1)
+    assert np.all(np.isfinite(P32))
+    assert np.max(np.abs(P32 - P64) / P64) < POWER_RTOL
+
+
 def test_errors_are_reported(fb, seeded):
     cfg, beam, fields = seeded
     b = fb.Batch([cfg.params])
