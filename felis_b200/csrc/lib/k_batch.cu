@@ -843,6 +843,18 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   // ================= pass 1: push (particlePush.cpp) =================
   if (push) {
     for (int k = tid; k < 48; k += nt) smap[k] = k < 16 ? T.tD0[k] : (k < 32 ? T.tM1[k - 16] : T.tM2[k - 32]);
+    // The push's step constants and the odd harmonics' linearised Bessel
+    // factors in shared memory, read (volatile) where the loop uses them:
+    // held in registers across the loop they would spill at the 72-register
+    // budget, and as reloads from the step structure they would be global
+    // loads (the particle stores may alias it).  Same values, same results.
+    __shared__ float pcst[16 + 4 * HM];
+    if (tid == 0) {
+      pcst[0] = T.R0; pcst[1] = T.A0; pcst[2] = T.AQ0; pcst[3] = T.c1 * T.c2; pcst[4] = T.K0; pcst[5] = T.ue;
+      pcst[6] = T.K0a; pcst[7] = T.Phi_half; pcst[8] = T.K0 * T.sq; pcst[9] = T.ksK0 * T.sq; pcst[10] = T.e_mc2;
+      pcst[11] = T.dPhi; pcst[12] = T.etaX.x; pcst[13] = T.etaX.y; pcst[14] = T.etaY.x; pcst[15] = T.etaY.y;
+    }
+    const volatile float* vc = pcst;
     for (int k = tid; k < LF * nr; k += nt) {
       const int l = k / (F * nr), rest = k % (F * nr);
       sEz[k] = I.Ez[((size_t)l * S + s) * F * nr + rest];
@@ -931,6 +943,11 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
           fx0[h] = fy0[h] = dfx[h] = dfy[h] = 0.f;
           if (h < H && (hh[h] & 1)) odd_factors(B, hh[h], xi0, T.K0a, &fx0[h], &fy0[h], &dfx[h], &dfy[h]);
         }
+        if (tid == 0)
+          for (int h = 0; h < HM; ++h) {
+            pcst[16 + 4 * h] = fx0[h]; pcst[17 + 4 * h] = fy0[h]; pcst[18 + 4 * h] = dfx[h]; pcst[19 + 4 * h] = dfy[h];
+          }
+        __syncthreads();
       }
       // the next particle's state is loaded one iteration ahead
       float nxv = 0.f, nyv = 0.f, npx = 0.f, npy = 0.f, ndg = 0.f;
@@ -981,10 +998,10 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
             sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
           }
           if constexpr (!DRIFT) {
-            const float R0 = T.R0, A0 = T.A0, AQ0 = T.AQ0, c12 = T.c1 * T.c2, K0 = T.K0, ue = T.ue, K0a = T.K0a;
-            const float Phi_half = T.Phi_half, K0sq = T.K0 * T.sq, ksK0sq = T.ksK0 * T.sq;
-            const float e_mc2 = T.e_mc2, dPhi = T.dPhi;
-            const float2 etaX = T.etaX, etaY = T.etaY;
+            const float R0 = vc[0], A0 = vc[1], AQ0 = vc[2], c12 = vc[3], K0 = vc[4], ue = vc[5], K0a = vc[6];
+            const float Phi_half = vc[7], K0sq = vc[8], ksK0sq = vc[9];
+            const float e_mc2 = vc[10], dPhi = vc[11];
+            const float2 etaX = make_float2(vc[12], vc[13]), etaY = make_float2(vc[14], vc[15]);
             const float r2 = x * x + y * y;
             const float k2 = px * px + py * py + c12 * r2;  // K2 - Q0
             const float i10 = 1.f / (1.f + dg * igR), i20 = i10 * i10;
@@ -997,8 +1014,8 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
               if (h >= H) break;
               float2 fx, fy;
               if (hh[h] & 1) {
-                fx = make_float2(fx0[h] + dfx[h] * dxi, 0.f);
-                fy = make_float2(fy0[h] + dfy[h] * dxi, 0.f);
+                fx = make_float2(vc[16 + 4 * h] + vc[18 + 4 * h] * dxi, 0.f);
+                fy = make_float2(vc[17 + 4 * h] + vc[19 + 4 * h] * dxi, 0.f);
               } else {
                 ffac_t(B, hh[h], xi0 * i20, xi2, K0a, eP, false, &fx, &fy);
               }
