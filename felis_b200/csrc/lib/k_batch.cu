@@ -129,9 +129,13 @@ __device__ __forceinline__ float quantum(float bound) {
 // Each sweep is a forward and a backward first-order linear recurrence along
 // every interior row (x) or column (y), with data-independent coefficients.
 // Each line is split into four chunks.  Thread (q, l) runs chunk q of line l:
-// q = tid / NL and l = tid % NL with NL a multiple of 32, so all lanes of a
-// warp work on the same chunk of 32 neighbouring lines, run the same trip
-// counts and take the same branches.  A thread runs the recurrence over its
+// q = tid / NL and l = tid % NL with NL = max(mx, my), the threads rounded up
+// to whole warps, so the lanes of a warp work on the same chunk of 32
+// neighbouring lines (all but the one warp at each chunk boundary, which
+// holds the last lines of chunk q and the first of chunk q + 1) and, the
+// chunks being equal, run the same trip counts.  No lane is idle for lack of
+// a line, as a line count rounded up to 32 per chunk would leave them (28 of
+// 128 lanes on a 102-point grid).  A thread runs the recurrence over its
 // chunk from a zero start and publishes the chunk's end value; after a
 // barrier, chunk q composes the carry of the chunks before it (forward) or
 // after it (backward) with the chunk products at their ends, at most three
@@ -266,8 +270,11 @@ __global__ void __launch_bounds__(1024) k_batch_adi(BatchLaunch a) {
   const int S = I.S, nx = I.nx, ny = I.ny, P = I.pitch, Mx = nx > ny ? nx : ny;
   const int mx = nx - 2, my = ny - 2;
   const int tid = threadIdx.x, nt = blockDim.x;
-  const int NL = nt >> 2;  // lines per chunk: a multiple of 32, >= max(mx, my)
-  const int q = tid / NL, l = tid - q * NL;
+  const int NL = Mx - 2;  // lines per chunk: max(mx, my)
+  // thread (chunk q, line l), q = tid / NL; the threads that round the block up
+  // to whole warps get no line (l = NL fails every line test below)
+  int q = tid / NL, l = tid - q * NL;
+  if (q > 3) { q = 3; l = NL; }
   float2* U = I.U + ((size_t)hp * S + (s + T.ring_base) % S) * I.N;
   const float2* ad = I.adi_c + (size_t)h * 16 * Mx;
   float2* pl = reinterpret_cast<float2*>(sm);  // interior cells, [my][P]
@@ -1401,13 +1408,13 @@ PushKernel push_kernel(int H, int L) { return L <= 1 ? push_kernel_l<1>(H) : pus
 
 size_t batch_adi_smem(int nx_max, int ny_max, int src_cells) {
   const int M = nx_max > ny_max ? nx_max : ny_max;
-  const size_t NL = (size_t)batch_adi_threads(nx_max, ny_max) / 4;
+  const size_t NL = (size_t)M - 2;  // lines per chunk (the kernel's NL)
   return ((size_t)(ny_max - 2) * ((nx_max - 2) | 1) + 16 * (size_t)M + 9 * NL + (size_t)src_cells) * sizeof(float2);
 }
 
 int batch_adi_threads(int nx, int ny) {
   const int m = (nx > ny ? nx : ny) - 2;
-  return 4 * (((m + 31) / 32) * 32);
+  return ((4 * m + 31) / 32) * 32;  // four chunks of m lines, whole warps
 }
 
 size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
