@@ -6,12 +6,12 @@
 //                 source box in shared memory, four threads per line
 //                 (partitioned recurrences); emits the plane's |U|^2 sum.
 //   k_batch_push  one CTA per (instance, slice): both transverse half-pushes,
-//                 push_theta_gamma or the drift, the theta wrap, the beam
-//                 partial sums (particlePush.cpp, rearrangeParticles.cpp,
-//                 twiss.cpp, saveFile.cpp), then the source deposit and the
-//                 radial Ez solve of the next iteration's solveField
-//                 (solveField.cpp:233-399) from the pushed particles, which the
-//                 CTA reads back from L2.
+//                 push_theta_gamma or the drift and the theta wrap
+//                 (particlePush.cpp, rearrangeParticles.cpp) in a loop
+//                 specialised on the mode, then, reading the pushed particles
+//                 back, the source deposit and the radial Ez solve of the next
+//                 iteration's solveField (solveField.cpp:233-399) together with
+//                 the beam partial sums (twiss.cpp, saveFile.cpp).
 //
 // Every (instance, slice) of an iteration is independent of the others: the
 // slippage shift only renames planes (ring buffer), and the CTA of the last
