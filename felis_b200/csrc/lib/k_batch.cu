@@ -1326,27 +1326,40 @@ __global__ void __launch_bounds__(256) k_batch_measure(const BInst* inst, const 
 // ring) and the twiss / bFactor of the pushed beam, summed in slice order.
 __global__ void __launch_bounds__(256) k_batch_reduce(const BInst* inst, const BStep* step, double* hist_e,
                                                       double* hist_t, double* hist_b, int se, int st_, int sb) {
-  __shared__ double red[8];
+  // every component (2 H plane energies, then the beam sums) reduced in the
+  // same order as block_sum_d (warp trees, then the warps in order), with one
+  // barrier for all of them
+  constexpr int kMaxV = 2 * FELIS_MAX_HARMONY + 7 + 2 * FELIS_MAX_HARMONY + 1;
+  __shared__ double part[8][kMaxV];
+  __shared__ double tot[kMaxV];
   const BInst& I = inst[blockIdx.x];
   const BStep& T = step[blockIdx.x];
-  const int H = I.H, S = I.S, stride = 7 + 2 * H + 1;
+  const int H = I.H, S = I.S, stride = 7 + 2 * H + 1, ne = 2 * H, nv = ne + stride;
   double* he = hist_e + (size_t)blockIdx.x * se;
   double* ht = hist_t + (size_t)blockIdx.x * st_;
   double* hb = hist_b + (size_t)blockIdx.x * sb;
   const int last = T.shift ? S - 1 : S;
-  for (int hp = 0; hp < 2 * H; ++hp) {
+  const int w = threadIdx.x >> 5, ln = threadIdx.x & 31, nw = (int)((blockDim.x + 31) >> 5);
+  for (int k = 0; k < nv; ++k) {
     double v = 0.0;
-    for (int s = threadIdx.x; s < last; s += blockDim.x) v += I.part_e[(size_t)s * 2 * H + hp];
-    const double t = block_sum_d(v, red);
-    if (threadIdx.x == 0) he[hp] = t;
+    if (k < ne) {
+      for (int s = threadIdx.x; s < last; s += blockDim.x) v += I.part_e[(size_t)s * 2 * H + k];
+    } else {
+      for (int s = threadIdx.x; s < S; s += blockDim.x) v += I.part_b[(size_t)s * stride + (k - ne)];
+    }
+    for (int o = 16; o > 0; o >>= 1) v += __shfl_down_sync(0xffffffffu, v, o);
+    if (ln == 0) part[w][k] = v;
   }
-  double acc[7 + 2 * FELIS_MAX_HARMONY + 1];
-  for (int k = 0; k < stride; ++k) {
-    double v = 0.0;
-    for (int s = threadIdx.x; s < S; s += blockDim.x) v += I.part_b[(size_t)s * stride + k];
-    acc[k] = block_sum_d(v, red);
+  __syncthreads();
+  if ((int)threadIdx.x < nv) {
+    double t = 0.0;
+    for (int k = 0; k < nw; ++k) t += part[k][threadIdx.x];
+    tot[threadIdx.x] = t;
   }
+  __syncthreads();
   if (threadIdx.x == 0) {
+    for (int hp = 0; hp < ne; ++hp) he[hp] = tot[hp];
+    const double* acc = tot + ne;
     for (int k = 0; k < 6; ++k) ht[k] = 0.0;
     const double cnt = acc[6];
     if (cnt > 0) {
