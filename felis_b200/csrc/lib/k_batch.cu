@@ -622,18 +622,23 @@ struct DepConst {
 // the (pushed) particles (twiss.cpp, saveFile.cpp): acc7 = x^2, y^2, x'^2,
 // y'^2, x x', y y', count; bre / bim = sum of e^{i H theta} per harmonic.
 template <int HM>
-__device__ __forceinline__ void beam_sums(float (&acc7)[7], float (&bre)[HM], float (&bim)[HM], const int (&hh)[HM],
-                                          int H, float x, float y, float px, float py, float g, float thn) {
+__device__ __forceinline__ void beam_sums(float (&acc7)[7], float (&bre)[HM], float (&bim)[HM], const float2 (&eb)[HM],
+                                          int H, float x, float y, float px, float py, float g) {
   const float ig = 1.f / g, xp = px * ig, yp = py * ig;
   acc7[0] += x * x; acc7[1] += y * y; acc7[2] += xp * xp;
   acc7[3] += yp * yp; acc7[4] += x * xp; acc7[5] += y * yp; acc7[6] += 1.f;
 #pragma unroll
   for (int h = 0; h < HM; ++h) {
     if (h >= H) break;
-    const float2 e = expif((float)hh[h] * thn);
-    bre[h] += e.x;
-    bim[h] += e.y;
+    bre[h] += eb[h].x;
+    bim[h] += eb[h].y;
   }
+}
+// e^{i H theta} of every harmonic from the reduced phase
+template <int HM>
+__device__ __forceinline__ void harmonic_phases(float2 (&eb)[HM], const int (&hh)[HM], int H, float thn) {
+#pragma unroll
+  for (int h = 0; h < HM; ++h) eb[h] = h < H ? expif((float)hh[h] * thn) : make_float2(1.f, 0.f);
 }
 
 template <int HM, bool SH, bool SUMS>
@@ -648,6 +653,9 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
                                              acc_t* gacc, unsigned sacc, unsigned sR, float dr, float idr2, int nr,
                                              int L, int F, float (&acc7)[7], float (&bre)[HM], float (&bim)[HM]) {
   const int ww = wi1 - wi0 + 1;
+  float2 ePhi[HM];  // e^{-i H Phi/2} of the deposit's lattice
+#pragma unroll
+  for (int h = 0; h < HM; ++h) ePhi[h] = expif(-(float)hh[h] * D.Phi_half);
   // the next particle's state is loaded one iteration ahead: the accumulator
   // adds below are compiler memory barriers, so no load moves above them
   float nxv = 0.f, nyv = 0.f, ndg = 0.f, npx = 0.f, npy = 0.f;
@@ -666,7 +674,11 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
       if (SUMS || has_even) { npx = pxs[m]; npy = pys[m]; }
     }
     const float thr = theta_red(th);
-    if (SUMS) beam_sums<HM>(acc7, bre, bim, hh, H, x, y, px, py, g, thr);
+    // e^{i H theta}: the bunching sums' phases, and (conjugated, times the
+    // per-launch e^{-i H Phi/2}) the deposit's
+    float2 eb[HM];
+    harmonic_phases<HM>(eb, hh, H, thr);
+    if (SUMS) beam_sums<HM>(acc7, bre, bim, eb, H, x, y, px, py, g);
     const float gx = (x - minX) * idx_, gy = (y - minY) * idy_;
     const int ii = (int)gx, jj = (int)gy;
     if (ii >= 0 && ii < nx && jj >= 0 && jj < ny && cells > 0) {
@@ -706,7 +718,7 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
       for (int h = 0; h < HM; ++h) {
         if (h >= H) break;
         const int Hh = hh[h];
-        const float2 e = expif(-(float)Hh * (thr + D.Phi_half));
+        const float2 e = cm(make_float2(eb[h].x, -eb[h].y), ePhi[h]);  // e^{-i H (theta + Phi/2)}
         const float2 mc = cs(e, (float)Hh * weight * D.coef_U * ig);
         const int base = sp[h] * cells * 2, wbase = sp[h] * wcells * 2;
         if (Hh & 1) {
@@ -746,7 +758,10 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
       for (int l = 0; l < L; ++l)
         for (int f = 0; f < F; ++f) {
           if (ir == 0 && f > 0) continue;
-          const float2 e = expif(-((float)(l + 1) * thr + (float)f * phi));
+          // e^{-i ((l + 1) theta + f phi)}: the conjugate of the first harmonic's
+          // phase for the lowest mode when the first harmonic is the fundamental
+          const float2 e = (l == 0 && f == 0 && hh[0] == 1) ? make_float2(eb[0].x, -eb[0].y)
+                                                            : expif(-((float)(l + 1) * thr + (float)f * phi));
           const float mag = mag0 * (l + 1.f);
           const float2 cc = make_float2(-e.y * mag, e.x * mag);  // i * coef * e^{-i..}
           const unsigned b0 = sR + 8u * (unsigned)((l * F + f) * nr + ir);
@@ -1097,14 +1112,16 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
           }
         }
         th += thshift;  // [Phase_shifter] (0 when no shifter sits in this step)
-        // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh)
-        if (th >= dTh || th < 0) {
+        // theta wrap (rearrangeParticles.cpp:301-320) into [0, dTh); a theta
+        // that needs no wrap is in range, so the range and NaN checks of theta
+        // run only after a wrap (a NaN theta takes the wrap branch too)
+        if (!(th >= 0.0 && th < dTh)) {
           th -= dTh * floor(th * idTh);
           if (th >= dTh) th -= dTh;
           else if (th < 0) th += dTh;
+          if (!(th >= 0.0 && th <= dTh)) bad |= (th - th == 0.0) ? kBadRange : kBadNan;
         }
-        if (th > dTh || th < 0) bad |= kBadRange;
-        if (!(dg - dg == 0.f) || !(th - th == 0.0) || !(x - x == 0.f)) bad |= kBadNan;
+        if (!(dg - dg == 0.f) || !(x - x == 0.f)) bad |= kBadNan;
         xs[n] = x; ys[n] = y; pxs[n] = px; pys[n] = py; dgs[n] = dg; ths[n] = th;
         if (dep) stats(even_c, ii, jj, x, y, px, py, gRf + dg);
       }
@@ -1165,7 +1182,9 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   if (push && !dep) {
     for (int q = tid; q < P; q += nt) {
       const int64_t n = p0 + q;
-      beam_sums<HM>(acc7, bre, bim, hh, H, xs[n], ys[n], pxs[n], pys[n], gRf + dgs[n], theta_red(ths[n]));
+      float2 eb[HM];
+      harmonic_phases<HM>(eb, hh, H, theta_red(ths[n]));
+      beam_sums<HM>(acc7, bre, bim, eb, H, xs[n], ys[n], pxs[n], pys[n], gRf + dgs[n]);
     }
     write_sums();
   }
