@@ -1267,7 +1267,8 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   }
   if (tid == 0) I.sbox[s] = make_int4(bi0, cells > 0 ? bi1 : bi0 - 1, bj0, bj1);
   __syncthreads();
-  // radial Thomas solve in FP64 (solveField.cpp:361-397), one thread per (l, f)
+  // radial Thomas solve in FP64 (solveField.cpp:361-397): the elimination one
+  // thread per (l, f), then the divisions of every point by the whole CTA
   if (tid < LF) {
     const int l = tid / F, f = tid % F;
     double bprev, dre, dim;
@@ -1294,10 +1295,14 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
       dbuf[j * 3] = djr; dbuf[j * 3 + 1] = dji; dbuf[j * 3 + 2] = bj_;
       dre = djr; dim = dji; bprev = bj_; aprev = aj;
     }
-    for (int j = nr - 2; j >= 0; --j) {
-      const float2 v = make_float2((float)(dbuf[j * 3] / dbuf[j * 3 + 2]), (float)(dbuf[j * 3 + 1] / dbuf[j * 3 + 2]));
-      I.Ez[((size_t)l * S + s) * F * nr + (size_t)f * nr + j] = v;
-    }
+  }
+  __syncthreads();
+  // the solution d_j / b_j, j < nr - 1: independent divisions, spread over the CTA
+  for (int k = tid; k < LF * (nr - 1); k += nt) {
+    const int lf = k / (nr - 1), j = k - lf * (nr - 1), l = lf / F, f = lf - l * F;
+    const double* dbuf = reinterpret_cast<const double*>(area) + (size_t)lf * nr * 3;
+    const float2 v = make_float2((float)(dbuf[j * 3] / dbuf[j * 3 + 2]), (float)(dbuf[j * 3 + 1] / dbuf[j * 3 + 2]));
+    I.Ez[((size_t)l * S + s) * F * nr + (size_t)f * nr + j] = v;
   }
 }
 
