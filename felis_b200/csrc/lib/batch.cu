@@ -330,6 +330,7 @@ struct felis_batch {
   int4* d_push_work = nullptr;
   int n_adi = 0, n_push = 0;
   BStep* d_steps = nullptr;
+  double* d_rad = nullptr;  // radial elimination tables of the run's steps (BStep::rad_off)
   int steps_cap = 0;
   double *d_he = nullptr, *d_ht = nullptr, *d_hb = nullptr;
   int hist_n = 0;
@@ -461,11 +462,41 @@ void make_sfac(const Inst& I, const BDep& d, float2 sfac[FELIS_MAX_HARMONY][2]) 
   }
 }
 
+// The radial Ez elimination of solveField.cpp:361-397 for one deposit's
+// coefficient A: per (l, f) mode and point j the multiplier w_j = c_j / b_{j-1}
+// and the pivot b_j, in the order and FP64 arithmetic of the device solve,
+// which then runs only the right-hand side's recurrence and the divisions.
+void radial_elimination(const Inst& I, double depA, double* out) {
+  const int L = I.p.scl_mode, F = I.p.scf_mode, nr = I.p.nr;
+  for (int l = 0; l < L; ++l)
+    for (int f = 0; f < F; ++f) {
+      double* t = out + ((size_t)l * F + f) * nr * 2;
+      double bprev = f == 0 ? -(1.0 + (l + 1.0) * (l + 1.0) * depA / 8.0) : 1.0;
+      double aprev = f == 0 ? 1.0 : 0.0;
+      t[0] = 0.0;
+      t[1] = bprev;
+      for (int j = 1; j < nr; ++j) {
+        const bool last = j == nr - 1;
+        const double aj = last ? 0.0 : j + 0.5, cj = last ? 0.0 : j - 0.5;
+        double bj = last ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * depA * j - f * f * log((j + 0.5) / (j - 0.5));
+        const double ww = cj / bprev;
+        bj -= ww * aprev;
+        t[2 * j] = ww;
+        t[2 * j + 1] = bj;
+        bprev = bj;
+        aprev = aj;
+      }
+    }
+}
+
 // Per-iteration scalars of every instance for iterations [it0, it1), plus
-// one row (index it1 - it0) for a deposit-only launch at it0.
-felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& out) {
+// one row (index it1 - it0) for a deposit-only launch at it0; `rad` receives
+// every row's radial elimination table (rad_stride doubles per row).
+felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& out, std::vector<double>& rad) {
   const int n = (int)b->in.size();
   out.assign((size_t)(it1 - it0 + 1) * n, BStep{});
+  const size_t rs = (size_t)b->LF_max * b->nr_max * 2;
+  rad.assign(out.size() * rs, 0.0);
   for (int k = 0; k < n; ++k) {
     Inst& I = b->in[k];
     const felis_params& p = I.p;
@@ -474,6 +505,9 @@ felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& o
       D0.ring_base = I.ring_base;
       D0.deposit = I.lat.current_flag;
       if (!make_dep(I, I.lat, &D0.dep)) return bfail(b, FELIS_BAD_ARG, "invalid K0_alpha");
+      const size_t r = (size_t)(it1 - it0) * n + k;
+      D0.rad_off = (int64_t)(r * rs);
+      radial_elimination(I, D0.dep.A, rad.data() + r * rs);
     }
     for (int it = it0; it < it1; ++it) {
       BStep& T = out[(size_t)(it - it0) * n + k];
@@ -514,6 +548,9 @@ felis_status build_steps(felis_batch* b, int it0, int it1, std::vector<BStep>& o
       T.A0d = A0;
       T.etaX = make_float2((float)eta[0], (float)eta[1]);
       T.etaY = make_float2((float)eta[2], (float)eta[3]);
+      const size_t r = (size_t)(it - it0) * n + k;
+      T.rad_off = (int64_t)(r * rs);
+      radial_elimination(I, T.dep.A, rad.data() + r * rs);
     }
   }
   return FELIS_OK;
@@ -623,7 +660,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
   if (deposit0) {
     BatchLaunch d{};
     d.inst = b->d_inst; d.step = row_d0; d.work = b->d_push_work; d.nwork = b->n_push;
-    d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY;
+    d.smem_bytes = b->push_smem; d.mode = BATCH_DEPOSIT_ONLY; d.rad = b->d_rad;
     BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
     launch_batch_push(d, b->H_max, b->L_max, b->st);
   }
@@ -639,6 +676,7 @@ felis_status enqueue_run(felis_batch* b, int it0, int it1, bool deposit0) {
       BatchLaunch p{};
       p.inst = b->d_inst; p.step = T; p.work = b->d_push_work; p.nwork = b->n_push; p.smem_bytes = b->push_smem;
       p.mode = BATCH_PUSH;
+      p.rad = b->d_rad;
       BatchScope ks(b, FELIS_BATCH_KERNEL_PUSH);
       launch_batch_push(p, b->H_max, b->L_max, b->st);
     }
@@ -806,7 +844,7 @@ void felis_batch_destroy(felis_batch* b) {
                     I.src, I.sbox, I.part_e, I.part_b, I.err};
     for (void* q : ptrs) if (q) cudaFree(q);
   }
-  void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_he, b->d_ht, b->d_hb, b->stage};
+  void* ptrs[] = {b->d_inst, b->d_adi_work, b->d_push_work, b->d_steps, b->d_rad, b->d_he, b->d_ht, b->d_hb, b->stage};
   for (void* q : ptrs) if (q) cudaFree(q);
   if (b->h_err) cudaFreeHost(b->h_err);
   for (cudaEvent_t e : b->ev) cudaEventDestroy(e);
@@ -992,15 +1030,20 @@ felis_status felis_batch_run(felis_batch* b, int32_t it0, int32_t it1) {
     for (size_t k = 0; k < b->in.size(); ++k) { b->in[k].lat = saved[k].first; b->in[k].ring_base = saved[k].second; }
   };
   std::vector<BStep> tab;
-  s = build_steps(b, it0, it1, tab);
+  std::vector<double> rad;
+  s = build_steps(b, it0, it1, tab, rad);
   if (s != FELIS_OK) { restore(); return s; }
   if (steps > b->steps_cap) {
     if (b->d_steps) cudaFree(b->d_steps);
+    if (b->d_rad) cudaFree(b->d_rad);
     b->d_steps = nullptr;
+    b->d_rad = nullptr;
     b->steps_cap = steps;
     BCK(cudaMalloc(&b->d_steps, (size_t)(b->steps_cap + 1) * n * sizeof(BStep)));
+    BCK(cudaMalloc(&b->d_rad, (size_t)(b->steps_cap + 1) * n * b->LF_max * b->nr_max * 2 * sizeof(double)));
   }
   BCK(cudaMemcpy(b->d_steps, tab.data(), tab.size() * sizeof(BStep), cudaMemcpyHostToDevice));
+  BCK(cudaMemcpy(b->d_rad, rad.data(), rad.size() * sizeof(double), cudaMemcpyHostToDevice));
   BCK(cudaStreamSynchronize(b->st));
   const bool deposit0 = b->src_valid_it != it0;
   cudaGraph_t graph = nullptr;

@@ -77,6 +77,10 @@ struct BStep {
   float2 etaX, etaY;
   BDep dep;       // deposit done by this launch
   float2 sfac[FELIS_MAX_HARMONY][2];  // ADI source factor per harmonic and polarisation
+  // the radial Ez elimination of this launch's deposit (data-independent:
+  // it depends on dep.A, l, f and nr only), made on the host: per (l, f) mode
+  // nr pairs (w_j, b_j) at BatchLaunch::rad + rad_off, b_0 in the first pair
+  int64_t rad_off;
 };
 
 constexpr int kPushThreads = 128;  // threads per CTA of the push launch
@@ -88,6 +92,7 @@ struct BatchLaunch {
   int nwork;
   int smem_bytes;     // dynamic shared memory of the launch
   int mode;           // push launch: BATCH_PUSH or BATCH_DEPOSIT_ONLY
+  const double* rad;  // push launch: the radial elimination tables of the run (BStep::rad_off)
 };
 
 enum { BATCH_PUSH = 0, BATCH_DEPOSIT_ONLY = 1 };

@@ -66,30 +66,6 @@ __device__ __forceinline__ double block_sum_d(double v, double* red) {
   return t;
 }
 
-__device__ __forceinline__ float block_max_f(float v, float* red) {
-  for (int o = 16; o > 0; o >>= 1) v = fmaxf(v, __shfl_down_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  float t = 0.f;
-  for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t = fmaxf(t, red[k]);
-  __syncthreads();
-  return t;
-}
-
-__device__ __forceinline__ int block_min_i(int v, int* red) {
-  for (int o = 16; o > 0; o >>= 1) v = min(v, __shfl_down_sync(0xffffffffu, v, o));
-  const int w = threadIdx.x >> 5, l = threadIdx.x & 31;
-  __syncthreads();
-  if (l == 0) red[w] = v;
-  __syncthreads();
-  int t = 1 << 30;
-  for (int k = 0; k < (int)((blockDim.x + 31) >> 5); ++k) t = min(t, red[k]);
-  __syncthreads();
-  return t;
-}
-
 // xi2 and e^{i (B - Phi/2)} of particlePush.cpp:272-279 / solveField.cpp:259-266.
 __device__ __forceinline__ void pol_phase(float K0, float ue, float K0a, float Phi_half, float px, float py,
                                           float* xi2, float2* eP) {
@@ -788,9 +764,6 @@ struct PushBlocks {
 template <int HM, int LM>
 __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_push(BatchLaunch a) {
   extern __shared__ __align__(16) unsigned char sm[];
-  __shared__ double redd[8];
-  __shared__ float redf[8];
-  __shared__ int redi[8];
   __shared__ __align__(16) float smap[48];  // transverse map: D0, M1, M2 (row-major 4x4 each)
   __shared__ __align__(8) unsigned long long fbar;  // bulk staging of the field box
   const int4 wi = a.work[blockIdx.x];
@@ -830,7 +803,6 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   DepConst D;
   D.K0 = T.dep.K0; D.ue = T.dep.ue; D.K0a = T.dep.K0a; D.Phi_half = T.dep.Phi_half; D.coef_U = T.dep.coef_U;
   D.xi = T.dep.xi; D.coef_Ez = T.dep.coef_Ez; D.etaX = T.dep.etaX; D.etaY = T.dep.etaY;
-  const double depA = T.dep.A;
   // shared memory: Ez of the slice | radial accumulators | 2D accumulators
   float2* sEz = reinterpret_cast<float2*>(sm);
   const size_t o1 = ((size_t)LF * nr * sizeof(float2) + 15) & ~(size_t)15;
@@ -1161,23 +1133,38 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   float bre[HM], bim[HM];
 #pragma unroll
   for (int h = 0; h < HM; ++h) { bre[h] = 0.f; bim[h] = 0.f; }
+  // the 7 + 2 H + 1 block sums of the beam, each as block_sum_d forms it (warp
+  // tree, then the warps in order), under one barrier
+  __shared__ double rsum[kPushThreads / 32][7 + 2 * HM + 1];
   auto write_sums = [&]() {
     const int stride = 7 + 2 * H + 1;
     double* out = I.part_b + (size_t)s * stride;
-#pragma unroll
-    for (int k = 0; k < 7; ++k) {
-      const double t = block_sum_d((double)acc7[k], redd);
-      if (tid == 0) out[k] = t;
-    }
-#pragma unroll
-    for (int h = 0; h < HM; ++h) {
-      if (h >= H) break;
-      const double tr = block_sum_d((double)bre[h], redd), ti = block_sum_d((double)bim[h], redd);
-      if (tid == 0) { out[7 + 2 * h] = tr * weight; out[8 + 2 * h] = ti * weight; }
-    }
     const double wsum = (double)weight * (double)max(0, (P - tid + nt - 1) / nt);
-    const double tw = block_sum_d(wsum, redd);
-    if (tid == 0) out[7 + 2 * H] = tw;
+    double v[7 + 2 * HM + 1];
+#pragma unroll
+    for (int k = 0; k < 7; ++k) v[k] = (double)acc7[k];
+#pragma unroll
+    for (int h = 0; h < HM; ++h) { v[7 + 2 * h] = (double)bre[h]; v[8 + 2 * h] = (double)bim[h]; }
+    v[7 + 2 * HM] = wsum;
+    const int w = tid >> 5, ln = tid & 31;
+#pragma unroll
+    for (int k = 0; k < 7 + 2 * HM + 1; ++k) {
+      if (k >= 7 + 2 * H && k < 7 + 2 * HM) continue;  // harmonics beyond H
+      double x = v[k];
+      for (int o = 16; o > 0; o >>= 1) x += __shfl_down_sync(0xffffffffu, x, o);
+      if (ln == 0) rsum[w][k] = x;
+    }
+    __syncthreads();
+    if (tid == 0) {
+      auto total = [&](int k) {
+        double t = 0.0;
+        for (int q = 0; q < (nt + 31) / 32; ++q) t += rsum[q][k];
+        return t;
+      };
+      for (int k = 0; k < 7; ++k) out[k] = total(k);
+      for (int h = 0; h < H; ++h) { out[7 + 2 * h] = total(7 + 2 * h) * weight; out[8 + 2 * h] = total(8 + 2 * h) * weight; }
+      out[7 + 2 * H] = total(7 + 2 * HM);
+    }
   };
   if (push && !dep) {
     for (int q = tid; q < P; q += nt) {
@@ -1190,14 +1177,41 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   }
   if (!dep) return;
   // ================= pass 2: deposit of the next solveField =================
-  const int mi1 = -block_min_i(-ci1, redi), mi0 = block_min_i(ci0, redi);
-  const int mj1 = -block_min_i(-cj1, redi), mj0 = block_min_i(cj0, redi);
   // bounds: |w mc| <= wm H weight coef_U / g for odd harmonics, times |f| <=
   // 2 xi2 H for even ones (|eta| <= 1, |e| = 1); radial |w c| <= coef_Ez L
   // weight (1 + |wr1|) / max(ir, 1)
   const float bmax = wfmax > 0.f ? wfmax / gmin : 0.f, rmax = rin ? 1.625f : 0.f;
-  const float bnd = block_max_f(bmax, redf) * 1.0625f * Hmax * weight * fabsf(D.coef_U) * (float)P;
-  const float rbnd = block_max_f(rmax, redf) * 1.0625f * L * weight * fabsf(D.coef_Ez) * (float)P;
+  // the cell box and both bounds over the CTA: warp trees, then the warps,
+  // one barrier for the six values
+  int mi0, mi1, mj0, mj1;
+  float bmx, rmx;
+  {
+    __shared__ int rbox[kPushThreads / 32][4];
+    __shared__ float rbnd2[kPushThreads / 32][2];
+    int iv[4] = {ci0, -ci1, cj0, -cj1};
+    float fv[2] = {bmax, rmax};
+#pragma unroll
+    for (int k = 0; k < 4; ++k)
+      for (int o = 16; o > 0; o >>= 1) iv[k] = min(iv[k], __shfl_down_sync(0xffffffffu, iv[k], o));
+#pragma unroll
+    for (int k = 0; k < 2; ++k)
+      for (int o = 16; o > 0; o >>= 1) fv[k] = fmaxf(fv[k], __shfl_down_sync(0xffffffffu, fv[k], o));
+    if ((tid & 31) == 0) {
+      for (int k = 0; k < 4; ++k) rbox[tid >> 5][k] = iv[k];
+      for (int k = 0; k < 2; ++k) rbnd2[tid >> 5][k] = fv[k];
+    }
+    __syncthreads();
+    int t[4] = {1 << 30, 1 << 30, 1 << 30, 1 << 30};
+    float u[2] = {0.f, 0.f};
+    for (int q = 0; q < (nt + 31) / 32; ++q) {
+      for (int k = 0; k < 4; ++k) t[k] = min(t[k], rbox[q][k]);
+      for (int k = 0; k < 2; ++k) u[k] = fmaxf(u[k], rbnd2[q][k]);
+    }
+    mi0 = t[0]; mi1 = -t[1]; mj0 = t[2]; mj1 = -t[3];
+    bmx = u[0]; rmx = u[1];
+  }
+  const float bnd = bmx * 1.0625f * Hmax * weight * fabsf(D.coef_U) * (float)P;
+  const float rbnd = rmx * 1.0625f * L * weight * fabsf(D.coef_Ez) * (float)P;
   // interior targets a particle can reach
   const int bi0 = max(1, mi0), bi1 = min(nx - 2, mi1 + 1), bj0 = max(1, mj0), bj1 = min(ny - 2, mj1 + 1);
   const int bw = bi1 - bi0 + 1, bh = bj1 - bj0 + 1;
@@ -1267,33 +1281,29 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   }
   if (tid == 0) I.sbox[s] = make_int4(bi0, cells > 0 ? bi1 : bi0 - 1, bj0, bj1);
   __syncthreads();
-  // radial Thomas solve in FP64 (solveField.cpp:361-397): the elimination one
-  // thread per (l, f), then the divisions of every point by the whole CTA
+  // radial Thomas solve in FP64 (solveField.cpp:361-397): the multipliers and
+  // pivots come from the host's table (they do not depend on the particles),
+  // the right-hand side's recurrence one thread per (l, f), then the divisions
+  // of every point by the whole CTA
   if (tid < LF) {
-    const int l = tid / F, f = tid % F;
-    double bprev, dre, dim;
+    const int f = tid % F;
+    const double* rt = a.rad + T.rad_off + (size_t)tid * nr * 2;  // (w_j, b_j)
+    double dre = 0.0, dim = 0.0;
     if (f == 0) {
-      bprev = -(1.0 + (l + 1.0) * (l + 1.0) * depA / 8.0);
       dre = (double)sR[(tid * nr) * 2] * qr;
       dim = (double)sR[(tid * nr) * 2 + 1] * qr;
-    } else {
-      bprev = 1.0; dre = 0.0; dim = 0.0;
     }
     double* dbuf = reinterpret_cast<double*>(area) + (size_t)tid * nr * 3;  // d re, d im, b
-    dbuf[0] = dre; dbuf[1] = dim; dbuf[2] = bprev;
-    double aprev = (f == 0) ? 1.0 : 0.0;
+    dbuf[0] = dre; dbuf[1] = dim; dbuf[2] = rt[1];
     for (int j = 1; j < nr; ++j) {
       const bool last = j == nr - 1;
-      const double aj = last ? 0.0 : j + 0.5, cj = last ? 0.0 : j - 0.5;
-      double bj_ = last ? 1.0 : -2.0 * j - (l + 1.0) * (l + 1.0) * depA * j - f * f * log((j + 0.5) / (j - 0.5));
-      const double ww = cj / bprev;
-      bj_ -= ww * aprev;
+      const double ww = rt[2 * j];
       double djr = last ? 0.0 : (double)sR[(tid * nr + j) * 2] * qr;
       double dji = last ? 0.0 : (double)sR[(tid * nr + j) * 2 + 1] * qr;
       djr -= ww * dre;
       dji -= ww * dim;
-      dbuf[j * 3] = djr; dbuf[j * 3 + 1] = dji; dbuf[j * 3 + 2] = bj_;
-      dre = djr; dim = dji; bprev = bj_; aprev = aj;
+      dbuf[j * 3] = djr; dbuf[j * 3 + 1] = dji; dbuf[j * 3 + 2] = rt[2 * j + 1];
+      dre = djr; dim = dji;
     }
   }
   __syncthreads();
