@@ -88,14 +88,23 @@ __device__ __forceinline__ void cp_async_wait_all() { asm volatile("cp.async.wai
 // ---- fixed-point accumulation ------------------------------------------------
 constexpr int kAccBits = 31;
 
-// v / q rounded to an integer; q is a power of two, so v * (1/q) is exact in
-// FP32 and only the rounding to an integer is inexact
-__device__ __forceinline__ acc_t fix(float v, float inv_q) { return (acc_t)__float2int_rn(v * inv_q); }
+// v / q rounded to the nearest integer (ties to even), for |v / q| < 2^22,
+// on the FMA pipe: q is a power of two, so v * (1/q) is exact, and adding
+// 1.5 * 2^23 rounds it once to an integer held in the low mantissa bits.  The
+// same value as __float2int_rn(v * inv_q) in that range, without the
+// conversion unit.
+__device__ __forceinline__ acc_t fix(float v, float inv_q) {
+  return (acc_t)(__float_as_int(__fmaf_rn(v, inv_q, 12582912.f)) - 0x4B400000);
+}
 // quantum 2^e with bound / 2^e < 2^(kAccBits - 1): the rounded terms add at
-// most half a quantum each on top of the exact sum, so no sum overflows
-__device__ __forceinline__ float quantum(float bound) {
+// most half a quantum each on top of the exact sum, so no sum overflows; and
+// term / 2^e < 2^22 for fix's range, `term` bounding a single term (it decides
+// only for slices of a few hundred particles or fewer)
+__device__ __forceinline__ float quantum(float bound, float term) {
   if (!(bound > 0.f)) return 1.f;
-  const int e = max(ilogbf(bound) + 2 - kAccBits, -120);  // 1/q stays a finite float
+  int e = ilogbf(bound) + 2 - kAccBits;
+  if (term > 0.f) e = max(e, ilogbf(term) - 21);
+  e = max(e, -120);  // 1/q stays a finite float
   return ldexpf(1.f, e);
 }
 
@@ -632,20 +641,24 @@ __device__ __forceinline__ void deposit_pass(const float* __restrict__ xs, const
   float2 ePhi[HM];  // e^{-i H Phi/2} of the deposit's lattice
 #pragma unroll
   for (int h = 0; h < HM; ++h) ePhi[h] = expif(-(float)hh[h] * D.Phi_half);
-  // the next particle's state is loaded one iteration ahead: the accumulator
-  // adds below are compiler memory barriers, so no load moves above them
+  // The particles are visited in the reverse of the push's order, so that the
+  // first reads find the push's latest stores still in L2.  The next
+  // particle's state is loaded one iteration ahead: the accumulator adds below
+  // are compiler memory barriers, so no load moves above them.
+  const int nt = blockDim.x, t0 = threadIdx.x;
   float nxv = 0.f, nyv = 0.f, ndg = 0.f, npx = 0.f, npy = 0.f;
   double nth = 0.0;
-  if ((int)threadIdx.x < P) {
-    const int64_t n = p0 + threadIdx.x;
+  const int qlast = t0 < P ? t0 + (P - 1 - t0) / nt * nt : -1;  // this thread's last particle
+  if (qlast >= 0) {
+    const int64_t n = p0 + qlast;
     nxv = xs[n]; nyv = ys[n]; ndg = dgs[n]; nth = ths[n];
     if (SUMS || has_even) { npx = pxs[n]; npy = pys[n]; }
   }
-  for (int q = threadIdx.x; q < P; q += blockDim.x) {
+  for (int q = qlast; q >= 0; q -= nt) {
     const float x = nxv, y = nyv, g = gRf + ndg, px = npx, py = npy;
     const double th = nth;
-    if (q + (int)blockDim.x < P) {
-      const int64_t m = p0 + q + blockDim.x;
+    if (q >= nt) {
+      const int64_t m = p0 + q - nt;
       nxv = xs[m]; nyv = ys[m]; ndg = dgs[m]; nth = ths[m];
       if (SUMS || has_even) { npx = pxs[m]; npy = pys[m]; }
     }
@@ -1210,13 +1223,13 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
     mi0 = t[0]; mi1 = -t[1]; mj0 = t[2]; mj1 = -t[3];
     bmx = u[0]; rmx = u[1];
   }
-  const float bnd = bmx * 1.0625f * Hmax * weight * fabsf(D.coef_U) * (float)P;
-  const float rbnd = rmx * 1.0625f * L * weight * fabsf(D.coef_Ez) * (float)P;
+  const float tb = bmx * 1.0625f * Hmax * weight * fabsf(D.coef_U), bnd = tb * (float)P;
+  const float rtb = rmx * 1.0625f * L * weight * fabsf(D.coef_Ez), rbnd = rtb * (float)P;
   // interior targets a particle can reach
   const int bi0 = max(1, mi0), bi1 = min(nx - 2, mi1 + 1), bj0 = max(1, mj0), bj1 = min(ny - 2, mj1 + 1);
   const int bw = bi1 - bi0 + 1, bh = bj1 - bj0 + 1;
   const int cells = (bw > 0 && bh > 0) ? bw * bh : 0;
-  const float q2 = quantum(bnd), qr = quantum(rbnd);
+  const float q2 = quantum(bnd, tb), qr = quantum(rbnd, rtb);
   const float iq2 = 1.f / q2, iqr = 1.f / qr;
   // accumulators: one interleaved (re, im) pair per cell of each source plane
   const int nsrc = I.nsrc;
@@ -1282,27 +1295,31 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   if (tid == 0) I.sbox[s] = make_int4(bi0, cells > 0 ? bi1 : bi0 - 1, bj0, bj1);
   __syncthreads();
   // radial Thomas solve in FP64 (solveField.cpp:361-397): the multipliers and
-  // pivots come from the host's table (they do not depend on the particles),
-  // the right-hand side's recurrence one thread per (l, f), then the divisions
-  // of every point by the whole CTA
+  // pivots come from the host's table (they do not depend on the particles).
+  // The whole CTA lays out, per (l, f) and point j, the right-hand side
+  // (d re, d im), the pivot b_j and the multiplier w_j in shared memory; one
+  // thread per (l, f) then runs the recurrence d_j -= w_j d_{j-1}, which
+  // waits on no global load; the divisions of every point by the whole CTA.
+  for (int k = tid; k < LF * nr; k += nt) {
+    const int lf = k / nr, j = k - lf * nr, f = lf % F;
+    const double* rt = a.rad + T.rad_off + (size_t)lf * nr * 2;  // (w_j, b_j)
+    double* db = reinterpret_cast<double*>(area) + (size_t)k * 4;
+    const bool zero = j == nr - 1 || (j == 0 && f != 0);
+    db[0] = zero ? 0.0 : (double)sR[k * 2] * qr;
+    db[1] = zero ? 0.0 : (double)sR[k * 2 + 1] * qr;
+    db[2] = rt[2 * j + 1];
+    db[3] = rt[2 * j];
+  }
+  __syncthreads();
   if (tid < LF) {
-    const int f = tid % F;
-    const double* rt = a.rad + T.rad_off + (size_t)tid * nr * 2;  // (w_j, b_j)
-    double dre = 0.0, dim = 0.0;
-    if (f == 0) {
-      dre = (double)sR[(tid * nr) * 2] * qr;
-      dim = (double)sR[(tid * nr) * 2 + 1] * qr;
-    }
-    double* dbuf = reinterpret_cast<double*>(area) + (size_t)tid * nr * 3;  // d re, d im, b
-    dbuf[0] = dre; dbuf[1] = dim; dbuf[2] = rt[1];
+    double* dbuf = reinterpret_cast<double*>(area) + (size_t)tid * nr * 4;  // d re, d im, b, w
+    double dre = dbuf[0], dim = dbuf[1];
     for (int j = 1; j < nr; ++j) {
-      const bool last = j == nr - 1;
-      const double ww = rt[2 * j];
-      double djr = last ? 0.0 : (double)sR[(tid * nr + j) * 2] * qr;
-      double dji = last ? 0.0 : (double)sR[(tid * nr + j) * 2 + 1] * qr;
+      const double ww = dbuf[j * 4 + 3];
+      double djr = dbuf[j * 4], dji = dbuf[j * 4 + 1];
       djr -= ww * dre;
       dji -= ww * dim;
-      dbuf[j * 3] = djr; dbuf[j * 3 + 1] = dji; dbuf[j * 3 + 2] = rt[2 * j + 1];
+      dbuf[j * 4] = djr; dbuf[j * 4 + 1] = dji;
       dre = djr; dim = dji;
     }
   }
@@ -1310,8 +1327,8 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
   // the solution d_j / b_j, j < nr - 1: independent divisions, spread over the CTA
   for (int k = tid; k < LF * (nr - 1); k += nt) {
     const int lf = k / (nr - 1), j = k - lf * (nr - 1), l = lf / F, f = lf - l * F;
-    const double* dbuf = reinterpret_cast<const double*>(area) + (size_t)lf * nr * 3;
-    const float2 v = make_float2((float)(dbuf[j * 3] / dbuf[j * 3 + 2]), (float)(dbuf[j * 3 + 1] / dbuf[j * 3 + 2]));
+    const double* dbuf = reinterpret_cast<const double*>(area) + (size_t)lf * nr * 4;
+    const float2 v = make_float2((float)(dbuf[j * 4] / dbuf[j * 4 + 2]), (float)(dbuf[j * 4 + 1] / dbuf[j * 4 + 2]));
     I.Ez[((size_t)l * S + s) * F * nr + (size_t)f * nr + j] = v;
   }
 }
@@ -1468,7 +1485,7 @@ size_t batch_push_smem(int nsrc_max, int LF_max, int nr_max, int box_cells) {
   const size_t head = (((size_t)LF_max * nr_max * sizeof(float2) + 15) & ~(size_t)15) +
                       (((size_t)LF_max * nr_max * 2 * sizeof(acc_t) + 15) & ~(size_t)15);
   size_t area = (size_t)nsrc_max * box_cells * 2 * sizeof(acc_t);  // a (re, im) pair per cell and plane
-  const size_t thomas = (size_t)LF_max * nr_max * 3 * sizeof(double);
+  const size_t thomas = (size_t)LF_max * nr_max * 4 * sizeof(double);  // d re, d im, b, w per point
   if (thomas > area) area = thomas;
   return head + area;
 }
