@@ -990,17 +990,26 @@ __global__ void __launch_bounds__(kPushThreads, PushBlocks<HM>::value) k_batch_p
           const float wx1 = gx - ii, wy1 = gy - jj, wx0 = 1.f - wx1, wy0 = 1.f - wy1;
           float2 Ux[HM], Uy[HM];
           float sumU2 = 0.f;
+          // the bilinear gather of both polarisations of every harmonic: from
+          // the staged box or from the plane in global memory, as two
+          // explicit paths, so that the staged one reads shared memory
+          // directly instead of through generic addresses
           const bool staged = ii >= fi0 && ii < fi1 && jj >= fj0 && jj < fj1;
-          const float2* fb = staged ? sF + (jj - fj0) * fbw + (ii - fi0) : Ubase + jj * nx + ii;
-          const size_t fps = staged ? (size_t)fcells : hpstride;
-          const int frs = staged ? fbw : nx;
+          auto gather = [&](const float2* __restrict__ fb, auto fps, int frs) {
+#pragma unroll
+            for (int h = 0; h < HM; ++h) {
+              if (h >= H) break;
+              const float2* Px = fb + (2 * h) * fps;
+              const float2* Py = Px + fps;
+              Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[frs], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[frs + 1], wx1 * wy1)));
+              Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[frs], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[frs + 1], wx1 * wy1)));
+            }
+          };
+          if (staged) gather(sF + (jj - fj0) * fbw + (ii - fi0), fcells, fbw);
+          else gather(Ubase + jj * nx + ii, hpstride, nx);
 #pragma unroll
           for (int h = 0; h < HM; ++h) {
             if (h >= H) break;
-            const float2* Px = fb + (2 * h) * fps;
-            const float2* Py = Px + fps;
-            Ux[h] = cad(cad(cs(Px[0], wx0 * wy0), cs(Px[frs], wx0 * wy1)), cad(cs(Px[1], wx1 * wy0), cs(Px[frs + 1], wx1 * wy1)));
-            Uy[h] = cad(cad(cs(Py[0], wx0 * wy0), cs(Py[frs], wx0 * wy1)), cad(cs(Py[1], wx1 * wy0), cs(Py[frs + 1], wx1 * wy1)));
             const float Hh = (float)hh[h];
             sumU2 += (Ux[h].x * Ux[h].x + Ux[h].y * Ux[h].y + Uy[h].x * Uy[h].x + Uy[h].y * Uy[h].y) / (2.f * Hh * Hh);
           }
